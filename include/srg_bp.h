@@ -1,0 +1,175 @@
+/*
+ * srg_bp.h -- C ABI of the B200 (sm_100a) time-domain backprojection library
+ * (libsrg_bp.so), a drop-in for the azimuth-compression entry of ASFHyP3/SRG.
+ *
+ * Plain C: pointers, sizes and scalars only.  Complex samples are complex64,
+ * stored as interleaved float pairs (re, im), exactly the layout of Fortran
+ * `complex` and C `float _Complex`.
+ *
+ * Error convention of the status-returning entries: 0 on success, a negative
+ * SRG_E* code otherwise; srg_last_error() returns a one-line message for the
+ * calling thread.
+ */
+#ifndef SRG_BP_H
+#define SRG_BP_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SRG_OK            0
+#define SRG_E_ARG        -1   /* invalid argument or size */
+#define SRG_E_CUDA       -2   /* a CUDA runtime call failed */
+#define SRG_E_IO         -3   /* DEM read or .geo read/write failed */
+#define SRG_E_TIMEOUT    -4   /* a bounded device-side wait gave up */
+#define SRG_E_NOMEM      -5   /* device or host allocation failed */
+#define SRG_E_UNSUPPORTED -6  /* configuration not supported by this build */
+
+/* Arithmetic of the per-term sum. */
+#define SRG_FORM_FP64   0  /* geometry, phase, sincos and accumulation in FP64,
+                              FP32 range interpolation: the arithmetic of
+                              sentinel/azimuth_compress.cu:59-79 */
+#define SRG_FORM_SPLIT  1  /* FP64 only for orbit, pixel ECEF and one reference
+                              range per tile and pulse; compensated FP32 for the
+                              per-term differential range and phase */
+
+typedef struct srg_bp_options {
+    int form;          /* SRG_FORM_FP64 or SRG_FORM_SPLIT */
+    int tile_cfg;      /* kernel shape index (srg_tile_config_count()); -1: tuned default */
+    int device;        /* CUDA device ordinal; -1: current device */
+    int centres_on_host; /* 1: per-line azimuth centres solved on the host CPU,
+                            0: on the GPU (default) */
+    int verbose;       /* 1: print the reference's "Burst line limits" line */
+} srg_bp_options;
+
+/* Fill *o with the defaults (split form, tuned tile, current device,
+ * centres on the GPU, quiet). */
+void srg_bp_default_options(srg_bp_options *o);
+
+/* Message of the last failing call on this thread ("" if none). */
+const char *srg_last_error(void);
+
+/* ------------------------------------------------------------------------
+ * Drop-in entry.  Replaces
+ *     extern "C" void azimuth_compress_(...)   sentinel/azimuth_compress.cu:181-214
+ * called by reference from sentinel/backprojectgpusub.f90:244-247
+ * (gfortran implicit interface: lower-case name + '_', every argument by
+ * reference, no hidden lengths).  Same 33 arguments, same meaning, same file
+ * side effects: reads DEM rows [firstline, firstline+nlines) from *fddem and
+ * read-modify-writes the same rows of the complex64 raster on *fdout,
+ * replacing a pixel where |Re(new)| > 1e-18 (azimuth_compress.cu:510-537).
+ * Like the reference it returns nothing; failures are reported on stderr and
+ * in srg_last_error().  Uses the options of srg_set_default_options()
+ * (split form unless changed).  tstart, tend, t, dtaz and iaperture are
+ * accepted and unused, as in the reference.
+ * ------------------------------------------------------------------------ */
+void azimuth_compress_(
+    float *burstdata,      /* [rawdatalines][samplesPerBurst] complex64 */
+    double *satloc,        /* [rawdatalines][3] ECEF m */
+    int *rawdatalines, int *samplesPerBurst, int *demwidth, int *demlength,
+    int *fdout, int *fddem,
+    double *deltalat, double *deltalon, double *firstlat, double *firstlon,
+    double *latlons,       /* [4] min lat, max lat, min lon, max lon (deg) */
+    double *timeorbit,     /* [numstatevec] s */
+    double *xx, double *vv,/* [numstatevec][3] ECEF m, m/s */
+    int *numstatevec,
+    double *rngstart, double *rngend, double *tstart, double *tend,
+    double *tmid, double *xyz_mid, double *vel_mid, double *t, double *dtaz,
+    double *dmrg, double *wvl, int *aperture, int *iaperture,
+    double *angc0, double *angc1, double *prf);
+
+/* Same call with a status and explicit options (opts may be NULL). */
+int srg_azimuth_compress(
+    const float *burstdata, const double *satloc, int rawdatalines,
+    int samplesPerBurst, int demwidth, int demlength, int fdout, int fddem,
+    double deltalat, double deltalon, double firstlat, double firstlon,
+    const double *latlons, const double *timeorbit, const double *xx,
+    const double *vv, int numstatevec, double rngstart, double rngend,
+    double tmid, const double *xyz_mid, const double *vel_mid, double dmrg,
+    double wvl, int aperture, double angc0, double angc1, double prf,
+    const srg_bp_options *opts);
+
+/* Options used by azimuth_compress_ (process-wide). */
+void srg_set_default_options(const srg_bp_options *o);
+
+/* ------------------------------------------------------------------------
+ * Device-resident bursts (no file I/O; all pointers are device pointers
+ * unless noted).  The unit of the batched scene launch.
+ * ------------------------------------------------------------------------ */
+typedef struct srg_burst_desc {
+    const float *burst;      /* [P][ldb] complex64 range lines (device) */
+    const double *satloc;    /* [P][3] (device) */
+    const int16_t *dem;      /* DEM row `firstline` of the grid, row stride dem_ld elements (device) */
+    float *out;              /* output row 0 (= grid line firstline), row stride out_ld complex64,
+                                column c = grid pixel c + out_pix0 (device) */
+    const double *coef;      /* optional [nlines][3] azimuth-centre parabolas (device);
+                                NULL: solved on the device from the orbit below */
+    int64_t ldb, dem_ld, out_ld;
+    int P, S;
+    int demwidth;            /* W */
+    int firstline, nlines, firstpix, lastpix; /* as derived by the reference from latlons */
+    int out_pix0;
+    int aperture;
+    double firstlat, deltalat, firstlon, deltalon;
+    double rngstart, rngend, dmrg, wvl;
+    /* azimuth-centre inputs (host pointers; used when coef == NULL) */
+    const double *timeorbit, *xx, *vv;
+    int numstatevec;
+    double tmid, xyz_mid[3], vel_mid[3], angc0, angc1, prf;
+} srg_burst_desc;
+
+/* Backproject `n` bursts in one persistent launch on `stream` (a
+ * cudaStream_t; NULL = default stream).  Each burst writes its pixels
+ * [firstpix, min(lastpix, W-1)] x [0, nlines) of `out` (formed pixels get the
+ * scaled complex64 sum, the others 0); bursts must not share output pixels
+ * (see srg_merge_device for the ordered merge).  Asynchronous: returns after
+ * enqueueing; srg_sync_check() reports device-side errors. */
+int srg_bp_bursts_device(const srg_burst_desc *bursts, int n,
+                         const srg_bp_options *opts, void *stream);
+
+/* Exact count of executed terms (pixel, pulse pairs inside the aperture
+ * window that pass the reference's range test) of the given bursts, computed
+ * on the device with the reference's FP64 arithmetic.  Blocking. */
+int srg_count_terms_device(const srg_burst_desc *bursts, int n, int64_t *terms,
+                           void *stream);
+
+/* Ordered merge of a burst output into a raster: dst[l][c] = src[l][c] where
+ * |Re(src)| > 1e-18 (azimuth_compress.cu:527-531).  Device pointers. */
+int srg_merge_device(float *dst, int64_t dst_ld, const float *src, int64_t src_ld,
+                     int rows, int cols, void *stream);
+
+/* Per-line azimuth-centre parabolas (azimuth_compress.cu:438-481) computed
+ * on the device into coef_out ([nlines][3], device).  Blocking. */
+int srg_line_centres_device(const srg_burst_desc *b, double *coef_out, void *stream);
+
+/* Per-pulse ECEF position and velocity by 4-point Hermite interpolation of
+ * the state vectors (sentinel/sentineltimingsub.f90:55-66, orbithermite.f),
+ * one thread per pulse.  times/pos/vel: device; timeorbit/xx/vv: host. */
+int srg_pulse_orbit_device(const double *times, int P, const double *timeorbit,
+                           const double *xx, const double *vv, int numstatevec,
+                           double *pos, double *vel, void *stream);
+
+/* Synchronise `stream` and report any device-side error flag raised by the
+ * library's kernels since the last check (SRG_E_TIMEOUT) or CUDA error. */
+int srg_sync_check(void *stream);
+
+/* Number of compiled kernel shapes, and the shape of one of them. */
+int srg_tile_config_count(void);
+int srg_tile_config(int idx, int *tile_x, int *tile_y, int *threads, int *chunk,
+                    int *window);
+
+/* Synthetic-scene support: forward-project a per-pixel reflectivity field
+ * (complex64, [nlines][dem_ld-aligned W] of the burst's grid, device) into
+ * the burst's range lines (accumulates into burst, device), with a
+ * sinc^2 azimuth antenna pattern of length `antenna_m`, a linear range
+ * response and FP64 geometry.  Atomic accumulation: not bit-reproducible. */
+int srg_forward_project_device(const srg_burst_desc *b, const float *refl,
+                               int64_t refl_ld, const double *satvel,
+                               double antenna_m, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SRG_BP_H */

@@ -1,0 +1,212 @@
+"""Python entry points of the backprojection library.
+
+* ``azimuth_compress_files``: the reference-facing call -- the 33-argument
+  by-reference ``azimuth_compress_`` of libsrg_bp.so, exactly as
+  sentinel/backprojectgpusub.f90:244-247 makes it, on a DEM file and a .geo
+  file.
+* ``DeviceBurst`` / ``backproject``: device-resident bursts (torch tensors
+  for memory and streams) through ``srg_bp_bursts_device``, one persistent
+  launch for any number of bursts.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import FORM_FP64, FORM_SPLIT, BurstDesc, check, default_options, lib
+from .scene import Burst
+
+_dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
+
+
+def _d(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def limits(b: Burst):
+    """Reference line/pixel limits (sentinel/azimuth_compress.cu:295-301, 378-379)."""
+    ll = int((b.latlons[0] - b.firstlat) / b.deltalat)
+    fl = int((b.latlons[1] - b.firstlat) / b.deltalat)
+    fl = min(max(fl, 0), b.demlength - 1)
+    ll = min(max(ll, 0), b.demlength - 1)
+    fp = max(int((b.latlons[2] - b.firstlon) / b.deltalon), 0)
+    lp = min(int((b.latlons[3] - b.firstlon) / b.deltalon), b.demwidth)
+    return fl, ll, fp, lp
+
+
+def azimuth_compress_files(b: Burst, fdout: int, fddem: int, burst: Optional[np.ndarray] = None):
+    """Call the drop-in ``azimuth_compress_`` (33 by-reference arguments)."""
+    L = lib()
+    burst = np.ascontiguousarray(b.burst if burst is None else burst, np.complex64)
+    keep = {k: _d(getattr(b, k)) for k in
+            ("satloc", "latlons", "timeorbit", "xx", "vv", "xyz_mid", "vel_mid", "pulse_time")}
+    i = {k: C.c_int(v) for k, v in dict(P=b.rawdatalines, S=b.samples, W=b.demwidth,
+                                        L=b.demlength, fo=fdout, fd=fddem, n=b.numstatevec,
+                                        ap=b.aperture, iap=b.iaperture).items()}
+    d = {k: C.c_double(getattr(b, k)) for k in
+         ("deltalat", "deltalon", "firstlat", "firstlon", "rngstart", "rngend", "tstart", "tend",
+          "tmid", "dtaz", "dmrg", "wvl", "angc0", "angc1", "prf")}
+    r = C.byref
+    p = lambda a: a.ctypes.data_as(_dp)  # noqa: E731
+    L.azimuth_compress_(
+        burst.ctypes.data_as(_fp), p(keep["satloc"]), r(i["P"]), r(i["S"]), r(i["W"]), r(i["L"]),
+        r(i["fo"]), r(i["fd"]), r(d["deltalat"]), r(d["deltalon"]), r(d["firstlat"]),
+        r(d["firstlon"]), p(keep["latlons"]), p(keep["timeorbit"]), p(keep["xx"]), p(keep["vv"]),
+        r(i["n"]), r(d["rngstart"]), r(d["rngend"]), r(d["tstart"]), r(d["tend"]), r(d["tmid"]),
+        p(keep["xyz_mid"]), p(keep["vel_mid"]), p(keep["pulse_time"]), r(d["dtaz"]), r(d["dmrg"]),
+        r(d["wvl"]), r(i["ap"]), r(i["iap"]), r(d["angc0"]), r(d["angc1"]), r(d["prf"]))
+
+
+def azimuth_compress_status(b: Burst, fdout: int, fddem: int, form: int = FORM_SPLIT,
+                            tile_cfg: int = -1, burst: Optional[np.ndarray] = None) -> int:
+    """The status-returning twin of the drop-in entry (raises on error)."""
+    L = lib()
+    burst = np.ascontiguousarray(b.burst if burst is None else burst, np.complex64)
+    keep = {k: _d(getattr(b, k)) for k in
+            ("satloc", "latlons", "timeorbit", "xx", "vv", "xyz_mid", "vel_mid")}
+    p = lambda a: a.ctypes.data_as(_dp)  # noqa: E731
+    o = default_options(form, tile_cfg)
+    rc = L.srg_azimuth_compress(
+        burst.ctypes.data_as(_fp), p(keep["satloc"]), b.rawdatalines, b.samples, b.demwidth,
+        b.demlength, fdout, fddem, b.deltalat, b.deltalon, b.firstlat, b.firstlon,
+        p(keep["latlons"]), p(keep["timeorbit"]), p(keep["xx"]), p(keep["vv"]), b.numstatevec,
+        b.rngstart, b.rngend, b.tmid, p(keep["xyz_mid"]), p(keep["vel_mid"]), b.dmrg, b.wvl,
+        b.aperture, b.angc0, b.angc1, b.prf, C.byref(o))
+    check(rc)
+    return rc
+
+
+def set_default_form(form: int, tile_cfg: int = -1) -> None:
+    o = default_options(form, tile_cfg)
+    lib().srg_set_default_options(C.byref(o))
+
+
+@dataclasses.dataclass
+class DeviceBurst:
+    """A burst resident in device memory (torch tensors) plus its descriptor."""
+
+    b: Burst
+    burst: "object"        # torch complex64 [P][S] (or a view with row stride ldb)
+    satloc: "object"       # torch float64 [P][3]
+    dem: "object"          # torch int16 [nlines][W] (rows firstline.. of the grid)
+    out: "object"          # torch complex64 [nlines][W]
+    firstline: int
+    nlines: int
+    firstpix: int
+    lastpix: int
+    keep: dict = dataclasses.field(default_factory=dict)
+
+    def desc(self, coef_ptr: int = 0) -> BurstDesc:
+        b = self.b
+        d = BurstDesc()
+        d.burst = self.burst.data_ptr()
+        d.satloc = self.satloc.data_ptr()
+        d.dem = self.dem.data_ptr()
+        d.out = self.out.data_ptr()
+        d.coef = coef_ptr or None
+        d.ldb = self.burst.stride(0)
+        d.dem_ld = self.dem.stride(0)
+        d.out_ld = self.out.stride(0)
+        d.P = b.rawdatalines
+        d.S = b.samples
+        d.demwidth = b.demwidth
+        d.firstline, d.nlines, d.firstpix, d.lastpix = (self.firstline, self.nlines, self.firstpix,
+                                                        self.lastpix)
+        d.out_pix0 = 0
+        d.aperture = b.aperture
+        d.firstlat, d.deltalat, d.firstlon, d.deltalon = b.firstlat, b.deltalat, b.firstlon, b.deltalon
+        d.rngstart, d.rngend, d.dmrg, d.wvl = b.rngstart, b.rngend, b.dmrg, b.wvl
+        for k in ("timeorbit", "xx", "vv"):
+            self.keep[k] = _d(getattr(b, k))
+            setattr(d, k, self.keep[k].ctypes.data_as(_dp))
+        d.numstatevec = b.numstatevec
+        d.tmid = b.tmid
+        for i in range(3):
+            d.xyz_mid[i] = float(b.xyz_mid[i])
+            d.vel_mid[i] = float(b.vel_mid[i])
+        d.angc0, d.angc1, d.prf = b.angc0, b.angc1, b.prf
+        return d
+
+
+def to_device(b: Burst, device="cuda", burst_tensor=None) -> DeviceBurst:
+    import torch
+
+    fl, ll, fp, lp = limits(b)
+    nl = ll - fl + 1
+    if burst_tensor is None:
+        burst_tensor = torch.from_numpy(np.ascontiguousarray(b.burst, np.complex64)).to(device)
+    sat = torch.from_numpy(_d(b.satloc)).to(device)
+    dem = torch.from_numpy(np.ascontiguousarray(b.dem[fl:fl + nl], np.int16)).to(device)
+    out = torch.zeros((nl, b.demwidth), dtype=torch.complex64, device=device)
+    return DeviceBurst(b=b, burst=burst_tensor, satloc=sat, dem=dem, out=out, firstline=fl,
+                       nlines=nl, firstpix=fp, lastpix=lp)
+
+
+def _stream_ptr(stream) -> Optional[int]:
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    return int(stream)
+
+
+def backproject(bursts: Sequence[DeviceBurst], form: int = FORM_SPLIT, tile_cfg: int = -1,
+                stream=None, sync: bool = True) -> None:
+    """Backproject device bursts into their `out` tensors (one launch)."""
+    arr = (BurstDesc * len(bursts))(*[db.desc() for db in bursts])
+    o = default_options(form, tile_cfg)
+    st = _stream_ptr(stream)
+    check(lib().srg_bp_bursts_device(arr, len(bursts), C.byref(o), C.c_void_p(st)))
+    if sync:
+        check(lib().srg_sync_check(C.c_void_p(st)))
+
+
+def count_terms(bursts: Sequence[DeviceBurst], stream=None) -> int:
+    arr = (BurstDesc * len(bursts))(*[db.desc() for db in bursts])
+    n = C.c_int64()
+    check(lib().srg_count_terms_device(arr, len(bursts), C.byref(n), C.c_void_p(_stream_ptr(stream))))
+    return int(n.value)
+
+
+def line_centres(db: DeviceBurst, stream=None):
+    import torch
+    coef = torch.zeros((db.nlines, 3), dtype=torch.float64, device=db.out.device)
+    d = db.desc()
+    st = _stream_ptr(stream)
+    check(lib().srg_line_centres_device(C.byref(d), C.c_void_p(coef.data_ptr()), C.c_void_p(st)))
+    check(lib().srg_sync_check(C.c_void_p(st)))
+    return coef
+
+
+def pulse_orbit(times, b: Burst, stream=None):
+    """Per-pulse Hermite orbit on the device; times: torch float64 [P] (device)."""
+    import torch
+    P = times.shape[0]
+    pos = torch.empty((P, 3), dtype=torch.float64, device=times.device)
+    vel = torch.empty_like(pos)
+    to, xx, vv = _d(b.timeorbit), _d(b.xx), _d(b.vv)
+    check(lib().srg_pulse_orbit_device(
+        C.c_void_p(times.data_ptr()), P, to.ctypes.data_as(_dp), xx.ctypes.data_as(_dp),
+        vv.ctypes.data_as(_dp), len(to), C.c_void_p(pos.data_ptr()), C.c_void_p(vel.data_ptr()),
+        C.c_void_p(_stream_ptr(stream))))
+    return pos, vel
+
+
+def merge(dst, src, stream=None) -> None:
+    """dst[r][c] = src[r][c] where |Re(src)| > 1e-18 (the reference merge rule)."""
+    rows, cols = src.shape
+    check(lib().srg_merge_device(C.c_void_p(dst.data_ptr()), dst.stride(0),
+                                 C.c_void_p(src.data_ptr()), src.stride(0), rows, cols,
+                                 C.c_void_p(_stream_ptr(stream))))
+
+
+def forward_project(db: DeviceBurst, refl, satvel, antenna: float = 10.0, stream=None) -> None:
+    """Accumulate the echo of a per-pixel reflectivity field into db.burst."""
+    d = db.desc()
+    check(lib().srg_forward_project_device(C.byref(d), C.c_void_p(refl.data_ptr()), refl.stride(0),
+                                           C.c_void_p(satvel.data_ptr()), antenna,
+                                           C.c_void_p(_stream_ptr(stream))))

@@ -1,0 +1,641 @@
+// capi.cu -- the C ABI of libsrg_bp.so (declared in include/srg_bp.h).
+//
+// Host orchestration of one burst mirrors sentinel/azimuth_compress.cu:
+// line/pixel limits from latlons (295-301, 378-379), DEM slab read from the
+// caller's descriptor (399-408), per-line azimuth centres (438-481), the
+// per-pixel sum (500), and the read-modify-write merge of the output rows
+// into the .geo raster (510-537).  Differences: every CUDA call is checked
+// and reported; device scratch is cached per device and reused across calls
+// instead of being allocated and freed on every burst; the merge uses
+// pread/pwrite on the descriptor instead of an fdopen() stream that is never
+// flushed or closed.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/srg_bp.h"
+#include "kernels.h"
+
+using namespace srg;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(call)                                                                       \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess)                                                         \
+            return fail(SRG_E_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));   \
+    } while (0)
+
+srg_bp_options g_default_opts = {SRG_FORM_SPLIT, -1, -1, 0, 0};
+std::mutex g_opts_mu;
+
+// Grow-only device buffer.
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    int ensure(size_t bytes) {
+        if (bytes <= cap) return SRG_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = std::max(bytes, (size_t)256);
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(SRG_E_NOMEM, "cudaMalloc(%zu) failed: %s", want, cudaGetErrorString(e));
+        }
+        cap = want;
+        return SRG_OK;
+    }
+};
+
+// Per-device scratch, reused by every call on that device.
+struct DevCtx {
+    int dev = -1;
+    int sms = 0;
+    std::mutex mu;
+    DevBuf flags;     // [0] work counter, [1] error word, [2..3] term counter (u64)
+    DevBuf bursts;    // BurstDev[]
+    DevBuf tmaps;     // CUtensorMap[]
+    DevBuf coef;      // doubles
+    DevBuf orbit;     // state vectors
+    DevBuf in_burst, in_sat, in_dem, out;  // drop-in staging
+    bool attrs_done[64] = {};
+};
+
+DevCtx g_ctx[64];
+std::mutex g_ctx_mu;
+
+int get_ctx(int device, DevCtx **out) {
+    int dev = device;
+    if (dev < 0) CK(cudaGetDevice(&dev));
+    if (dev >= 64) return fail(SRG_E_ARG, "device ordinal %d out of range", dev);
+    CK(cudaSetDevice(dev));
+    std::lock_guard<std::mutex> g(g_ctx_mu);
+    DevCtx &c = g_ctx[dev];
+    if (c.dev < 0) {
+        CK(cudaDeviceGetAttribute(&c.sms, cudaDevAttrMultiProcessorCount, dev));
+        c.dev = dev;
+    }
+    *out = &c;
+    return SRG_OK;
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaDriverEntryPointQueryResult q;
+        void *p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        else
+            cudaGetLastError();
+    });
+    return fn;
+}
+
+// Kernel entry for a form and shape index (-1: the default of that form).
+const KernelEntry *pick_kernel(int form, int cfg) {
+    if (cfg >= 0) {
+        if (cfg >= kNumKernels || kKernels[cfg].form != form) return nullptr;
+        return &kKernels[cfg];
+    }
+    for (int i = 0; i < kNumKernels; ++i)
+        if (kKernels[i].form == form) return &kKernels[i];
+    return nullptr;
+}
+
+// Reference line/pixel limits (azimuth_compress.cu:295-301, 378-379).
+void ref_limits(const double *latlons, double firstlat, double deltalat, double firstlon,
+                double deltalon, int W, int L, int *fl, int *ll, int *fp, int *lp) {
+    int lastline = (int)((latlons[0] - firstlat) / deltalat);
+    int firstline = (int)((latlons[1] - firstlat) / deltalat);
+    if (firstline < 0) firstline = 0;
+    if (lastline < 0) lastline = 0;
+    if (firstline > L - 1) firstline = L - 1;
+    if (lastline > L - 1) lastline = L - 1;
+    int firstpix = (int)((latlons[2] - firstlon) / deltalon);
+    if (firstpix < 0) firstpix = 0;
+    int lastpix = (int)((latlons[3] - firstlon) / deltalon);
+    if (lastpix > W) lastpix = W;
+    *fl = firstline;
+    *ll = lastline;
+    *fp = firstpix;
+    *lp = lastpix;
+}
+
+double ref_pi() { return 4.0 * atan2(1.0, 1.0); }
+
+int validate_desc(const srg_burst_desc &d) {
+    if (!d.burst || !d.satloc || !d.dem || !d.out)
+        return fail(SRG_E_ARG, "null device pointer in burst descriptor");
+    if (d.P < 1 || d.S < 2 || d.ldb < d.S || d.demwidth < 1 || d.nlines < 1)
+        return fail(SRG_E_ARG, "bad sizes: P=%d S=%d ldb=%lld W=%d nlines=%d", d.P, d.S,
+                    (long long)d.ldb, d.demwidth, d.nlines);
+    if (d.P > 100000000 || d.S > (1 << 28))
+        return fail(SRG_E_ARG, "burst too large: P=%d S=%d", d.P, d.S);
+    if (!(d.dmrg > 0) || !(d.wvl > 0) || d.aperture < 0)
+        return fail(SRG_E_ARG, "bad radar scalars: dmrg=%g wvl=%g aperture=%d", d.dmrg, d.wvl,
+                    d.aperture);
+    if (!d.coef && (!d.timeorbit || !d.xx || !d.vv || d.numstatevec < 4))
+        return fail(SRG_E_ARG, "no coef and no orbit (numstatevec=%d, need >= 4)", d.numstatevec);
+    if (d.firstpix < 0 || d.out_pix0 > d.firstpix)
+        return fail(SRG_E_ARG, "bad pixel window firstpix=%d out_pix0=%d", d.firstpix, d.out_pix0);
+    return SRG_OK;
+}
+
+BurstDev make_burst_dev(const srg_burst_desc &d, const double *coef) {
+    BurstDev B{};
+    B.burst = reinterpret_cast<const float2 *>(d.burst);
+    B.satloc = d.satloc;
+    B.dem = reinterpret_cast<const short *>(d.dem);
+    B.out = reinterpret_cast<float2 *>(d.out);
+    B.coef = coef;
+    B.ldb = d.ldb;
+    B.dem_ld = d.dem_ld;
+    B.out_ld = d.out_ld;
+    B.P = d.P;
+    B.S = d.S;
+    B.W = d.demwidth;
+    B.firstline = d.firstline;
+    B.nlines = d.nlines;
+    B.firstpix = d.firstpix;
+    B.lastpix = d.lastpix;
+    B.lastpix_eff = std::min(d.lastpix, d.demwidth - 1);
+    B.out_pix0 = d.out_pix0;
+    B.aperture = d.aperture;
+    B.ap2 = d.aperture / 2;
+    B.tmap = -1;
+    const double pi = ref_pi();
+    B.firstlat = d.firstlat;
+    B.deltalat = d.deltalat;
+    B.firstlon = d.firstlon;
+    B.deltalon = d.deltalon;
+    B.deg2rad = pi / 180.;
+    B.rngstart = d.rngstart;
+    B.rmax = d.rngend - d.dmrg;
+    B.dmrg = d.dmrg;
+    B.k4pi = 4. * pi / d.wvl;
+    B.K = 2.0 / d.wvl;
+    B.inv_dmrg = 1.0 / d.dmrg;
+    B.K_hi = (float)B.K;
+    B.K_lo = (float)(B.K - (double)B.K_hi);
+    B.K_f = B.K_hi;
+    B.inv_dmrg_f = (float)B.inv_dmrg;
+    return B;
+}
+
+int make_tmap(const BurstDev &B, int box_x, int box_y, CUtensorMap *out) {
+    auto enc = get_encode();
+    if (!enc) return -1;
+    const uintptr_t base = reinterpret_cast<uintptr_t>(B.burst);
+    if ((base & 15) || ((B.ldb * 8) & 15) || (box_x & 1)) return -1;
+    cuuint64_t dims[2] = {(cuuint64_t)B.S, (cuuint64_t)B.P};
+    cuuint64_t strides[1] = {(cuuint64_t)(B.ldb * 8)};
+    cuuint32_t box[2] = {(cuuint32_t)box_x, (cuuint32_t)box_y};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(out, CU_TENSOR_MAP_DATA_TYPE_UINT64, 2, (void *)B.burst, dims, strides, box,
+                     estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? 0 : -1;
+}
+
+// Device line centres for one descriptor into `coef` (device).
+int centres_device(DevCtx &c, const srg_burst_desc &d, const BurstDev &B, double *coef,
+                   cudaStream_t st) {
+    const int n = d.numstatevec;
+    int rc = c.orbit.ensure(sizeof(double) * 7 * (size_t)n);
+    if (rc) return rc;
+    double *ob = static_cast<double *>(c.orbit.p);
+    std::vector<double> host(7 * (size_t)n);
+    std::memcpy(host.data(), d.timeorbit, sizeof(double) * n);
+    std::memcpy(host.data() + n, d.xx, sizeof(double) * 3 * n);
+    std::memcpy(host.data() + 4 * n, d.vv, sizeof(double) * 3 * n);
+    CK(cudaMemcpyAsync(ob, host.data(), sizeof(double) * 7 * n, cudaMemcpyHostToDevice, st));
+    Orbit o{ob, ob + n, ob + 4 * n, n};
+    CentreParams cp{};
+    cp.tmid = d.tmid;
+    for (int i = 0; i < 3; ++i) {
+        cp.xm[i] = d.xyz_mid[i];
+        cp.vm[i] = d.vel_mid[i];
+    }
+    cp.wvl = d.wvl;
+    cp.angc0 = d.angc0;
+    cp.angc1 = d.angc1;
+    cp.prf = d.prf;
+    cp.pi = ref_pi();
+    // a pageable source is staged before cudaMemcpyAsync returns, so `host`
+    // may go out of scope now
+    CK(launch_line_centres(B, o, cp, coef, st));
+    return SRG_OK;
+}
+
+void ensure_attrs(DevCtx &c, int idx) {
+    if (c.attrs_done[idx]) return;
+    const KernelEntry &e = kKernels[idx];
+    cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, shared_bytes(e));
+    c.attrs_done[idx] = true;
+}
+
+int kernel_index(const KernelEntry *e) { return (int)(e - kKernels); }
+
+// Core: launch the tiled kernel over n prepared bursts.
+int run_bursts(DevCtx &c, const srg_burst_desc *descs, int n, const srg_bp_options &o,
+               cudaStream_t st) {
+    const KernelEntry *ke = pick_kernel(o.form, o.tile_cfg);
+    if (!ke) return fail(SRG_E_ARG, "no kernel for form %d shape %d", o.form, o.tile_cfg);
+    const int TX = ke->shape.tx, TY = ke->shape.ty;
+    // coefficient scratch
+    size_t coef_total = 0;
+    for (int i = 0; i < n; ++i) {
+        int rc = validate_desc(descs[i]);
+        if (rc) return rc;
+        if (!descs[i].coef) coef_total += 3 * (size_t)descs[i].nlines;
+    }
+    int rc = c.coef.ensure(sizeof(double) * std::max<size_t>(coef_total, 3));
+    if (rc) return rc;
+    rc = c.bursts.ensure(sizeof(BurstDev) * n);
+    if (rc) return rc;
+    rc = c.tmaps.ensure(sizeof(CUtensorMap) * n);
+    if (rc) return rc;
+    rc = c.flags.ensure(64);
+    if (rc) return rc;
+    std::vector<BurstDev> hb(n);
+    std::vector<CUtensorMap> hm(n);
+    double *coef_base = static_cast<double *>(c.coef.p);
+    size_t coef_off = 0;
+    int total = 0;
+    for (int i = 0; i < n; ++i) {
+        const srg_burst_desc &d = descs[i];
+        const double *coef = d.coef;
+        if (!coef) {
+            double *dst = coef_base + coef_off;
+            coef_off += 3 * (size_t)d.nlines;
+            BurstDev tmp = make_burst_dev(d, dst);
+            if (o.centres_on_host)
+                return fail(SRG_E_UNSUPPORTED, "host centres need host DEM (use the file entry)");
+            rc = centres_device(c, d, tmp, dst, st);
+            if (rc) return rc;
+            coef = dst;
+        }
+        BurstDev B = make_burst_dev(d, coef);
+        const int nx = B.lastpix_eff - B.firstpix + 1;
+        B.tiles_x = nx > 0 ? (nx + TX - 1) / TX : 0;
+        B.tiles_y = (B.nlines + TY - 1) / TY;
+        B.tile_base = total;
+        total += B.tiles_x * B.tiles_y;
+        if (make_tmap(B, ke->shape.window, ke->shape.chunk, &hm[i]) == 0) B.tmap = i;
+        hb[i] = B;
+    }
+    if (total == 0) return SRG_OK;
+    CK(cudaMemcpyAsync(c.bursts.p, hb.data(), sizeof(BurstDev) * n, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(c.tmaps.p, hm.data(), sizeof(CUtensorMap) * n, cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(c.flags.p, 0, sizeof(int), st));  // work counter only
+    const int idx = kernel_index(ke);
+    ensure_attrs(c, idx);
+    const int smem = shared_bytes(*ke);
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ke->fn, ke->shape.threads, smem));
+    if (per_sm < 1) return fail(SRG_E_UNSUPPORTED, "kernel shape %d does not fit an SM", idx);
+    const int grid = std::min(total, per_sm * c.sms);
+    int *flags = static_cast<int *>(c.flags.p);
+    CK(launch_tiles(*ke, grid, smem, st, static_cast<const BurstDev *>(c.bursts.p), n, total,
+                    static_cast<const CUtensorMap *>(c.tmaps.p), flags, flags + 1));
+    // host vectors hb/hm were copied from pageable memory: the copies are
+    // complete (staged) when cudaMemcpyAsync returns for pageable sources.
+    return SRG_OK;
+}
+
+int check_flags(DevCtx &c, cudaStream_t st) {
+    int h[2] = {0, 0};
+    CK(cudaMemcpyAsync(h, c.flags.p, sizeof h, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (h[1]) {
+        cudaMemsetAsync(static_cast<int *>(c.flags.p) + 1, 0, sizeof(int), st);
+        return fail(SRG_E_TIMEOUT, "device error word 0x%x (TMA wait timed out)", h[1]);
+    }
+    return SRG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void srg_bp_default_options(srg_bp_options *o) {
+    if (!o) return;
+    o->form = SRG_FORM_SPLIT;
+    o->tile_cfg = -1;
+    o->device = -1;
+    o->centres_on_host = 0;
+    o->verbose = 0;
+}
+
+const char *srg_last_error(void) { return g_err.c_str(); }
+
+void srg_set_default_options(const srg_bp_options *o) {
+    std::lock_guard<std::mutex> g(g_opts_mu);
+    if (o) g_default_opts = *o;
+    else srg_bp_default_options(&g_default_opts);
+}
+
+int srg_tile_config_count(void) { return kNumKernels; }
+
+int srg_tile_config(int idx, int *tile_x, int *tile_y, int *threads, int *chunk, int *window) {
+    if (idx < 0 || idx >= kNumKernels) return fail(SRG_E_ARG, "shape index %d", idx);
+    const TileShape &s = kKernels[idx].shape;
+    if (tile_x) *tile_x = s.tx;
+    if (tile_y) *tile_y = s.ty;
+    if (threads) *threads = s.threads;
+    if (chunk) *chunk = s.chunk;
+    if (window) *window = s.window;
+    return kKernels[idx].form;
+}
+
+int srg_bp_bursts_device(const srg_burst_desc *bursts, int n, const srg_bp_options *opts,
+                         void *stream) {
+    if (!bursts || n < 1) return fail(SRG_E_ARG, "no bursts");
+    srg_bp_options o;
+    srg_bp_default_options(&o);
+    if (opts) o = *opts;
+    DevCtx *c = nullptr;
+    int rc = get_ctx(o.device, &c);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> g(c->mu);
+    return run_bursts(*c, bursts, n, o, static_cast<cudaStream_t>(stream));
+}
+
+int srg_sync_check(void *stream) {
+    DevCtx *c = nullptr;
+    int rc = get_ctx(-1, &c);
+    if (rc) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    CK(cudaStreamSynchronize(st));
+    CK(cudaGetLastError());
+    if (!c->flags.p) return SRG_OK;
+    return check_flags(*c, st);
+}
+
+int srg_count_terms_device(const srg_burst_desc *bursts, int n, int64_t *terms, void *stream) {
+    if (!bursts || n < 1 || !terms) return fail(SRG_E_ARG, "bad arguments");
+    DevCtx *c = nullptr;
+    int rc = get_ctx(-1, &c);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> g(c->mu);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    rc = c->flags.ensure(64);
+    if (rc) return rc;
+    unsigned long long *cnt = reinterpret_cast<unsigned long long *>(static_cast<int *>(c->flags.p) + 2);
+    CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), st));
+    size_t coef_total = 0;
+    for (int i = 0; i < n; ++i) {
+        rc = validate_desc(bursts[i]);
+        if (rc) return rc;
+        if (!bursts[i].coef) coef_total += 3 * (size_t)bursts[i].nlines;
+    }
+    rc = c->coef.ensure(sizeof(double) * std::max<size_t>(coef_total, 3));
+    if (rc) return rc;
+    double *coef_base = static_cast<double *>(c->coef.p);
+    size_t off = 0;
+    for (int i = 0; i < n; ++i) {
+        const double *coef = bursts[i].coef;
+        if (!coef) {
+            double *dst = coef_base + off;
+            off += 3 * (size_t)bursts[i].nlines;
+            rc = centres_device(*c, bursts[i], make_burst_dev(bursts[i], dst), dst, st);
+            if (rc) return rc;
+            coef = dst;
+        }
+        BurstDev B = make_burst_dev(bursts[i], coef);
+        CK(launch_count_terms(B, cnt, c->sms, st));
+    }
+    unsigned long long h = 0;
+    CK(cudaMemcpyAsync(&h, cnt, sizeof h, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    *terms = (int64_t)h;
+    return SRG_OK;
+}
+
+int srg_merge_device(float *dst, int64_t dst_ld, const float *src, int64_t src_ld, int rows,
+                     int cols, void *stream) {
+    if (!dst || !src || rows < 0 || cols < 0) return fail(SRG_E_ARG, "bad merge arguments");
+    DevCtx *c = nullptr;
+    int rc = get_ctx(-1, &c);
+    if (rc) return rc;
+    CK(launch_merge(reinterpret_cast<float2 *>(dst), dst_ld, reinterpret_cast<const float2 *>(src),
+                    src_ld, rows, cols, c->sms, static_cast<cudaStream_t>(stream)));
+    return SRG_OK;
+}
+
+int srg_line_centres_device(const srg_burst_desc *b, double *coef_out, void *stream) {
+    if (!b || !coef_out) return fail(SRG_E_ARG, "bad arguments");
+    int rc = validate_desc(*b);
+    if (rc) return rc;
+    DevCtx *c = nullptr;
+    rc = get_ctx(-1, &c);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> g(c->mu);
+    return centres_device(*c, *b, make_burst_dev(*b, coef_out), coef_out,
+                          static_cast<cudaStream_t>(stream));
+}
+
+int srg_pulse_orbit_device(const double *times, int P, const double *timeorbit, const double *xx,
+                           const double *vv, int numstatevec, double *pos, double *vel,
+                           void *stream) {
+    if (!times || !timeorbit || !xx || !vv || !pos || !vel || P < 0 || numstatevec < 4)
+        return fail(SRG_E_ARG, "bad arguments");
+    DevCtx *c = nullptr;
+    int rc = get_ctx(-1, &c);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> g(c->mu);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int n = numstatevec;
+    rc = c->orbit.ensure(sizeof(double) * 7 * (size_t)n);
+    if (rc) return rc;
+    double *ob = static_cast<double *>(c->orbit.p);
+    std::vector<double> host(7 * (size_t)n);
+    std::memcpy(host.data(), timeorbit, sizeof(double) * n);
+    std::memcpy(host.data() + n, xx, sizeof(double) * 3 * n);
+    std::memcpy(host.data() + 4 * n, vv, sizeof(double) * 3 * n);
+    CK(cudaMemcpyAsync(ob, host.data(), sizeof(double) * 7 * n, cudaMemcpyHostToDevice, st));
+    Orbit o{ob, ob + n, ob + 4 * n, n};
+    CK(launch_pulse_orbit(times, P, o, pos, vel, st));
+    CK(cudaStreamSynchronize(st));
+    return SRG_OK;
+}
+
+int srg_forward_project_device(const srg_burst_desc *b, const float *refl, int64_t refl_ld,
+                               const double *satvel, double antenna_m, void *stream) {
+    if (!b || !refl || !satvel) return fail(SRG_E_ARG, "bad arguments");
+    int rc = validate_desc(*b);
+    if (rc) return rc;
+    DevCtx *c = nullptr;
+    rc = get_ctx(-1, &c);
+    if (rc) return rc;
+    BurstDev B = make_burst_dev(*b, nullptr);
+    CK(launch_forward_project(B, reinterpret_cast<const float2 *>(refl), refl_ld, satvel,
+                              antenna_m, static_cast<cudaStream_t>(stream)));
+    return SRG_OK;
+}
+
+int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawdatalines,
+                         int samplesPerBurst, int demwidth, int demlength, int fdout, int fddem,
+                         double deltalat, double deltalon, double firstlat, double firstlon,
+                         const double *latlons, const double *timeorbit, const double *xx,
+                         const double *vv, int numstatevec, double rngstart, double rngend,
+                         double tmid, const double *xyz_mid, const double *vel_mid, double dmrg,
+                         double wvl, int aperture, double angc0, double angc1, double prf,
+                         const srg_bp_options *opts) {
+    if (!burstdata || !satloc || !latlons || !timeorbit || !xx || !vv || !xyz_mid || !vel_mid)
+        return fail(SRG_E_ARG, "null argument");
+    if (rawdatalines < 1 || samplesPerBurst < 2 || demwidth < 1 || demlength < 1 ||
+        numstatevec < 4 || !(dmrg > 0) || !(wvl > 0) || aperture < 0)
+        return fail(SRG_E_ARG, "bad sizes or scalars (P=%d S=%d W=%d L=%d n=%d)", rawdatalines,
+                    samplesPerBurst, demwidth, demlength, numstatevec);
+    srg_bp_options o;
+    if (opts) o = *opts;
+    else {
+        std::lock_guard<std::mutex> g(g_opts_mu);
+        o = g_default_opts;
+    }
+    int fl, ll, fp, lp;
+    ref_limits(latlons, firstlat, deltalat, firstlon, deltalon, demwidth, demlength, &fl, &ll, &fp,
+               &lp);
+    const int nl = ll - fl + 1;
+    if (o.verbose) printf("Burst line limits, size (first,last,nlines) %d %d %d\n", fl, ll, nl);
+    const int W = demwidth;
+    const size_t npix = (size_t)nl * W;
+
+    // DEM slab (azimuth_compress.cu:399-408); a short read leaves zeros.
+    std::vector<int16_t> slab(npix, 0);
+    {
+        const ssize_t want = (ssize_t)(npix * 2);
+        const ssize_t got = pread(fddem, slab.data(), want, (off_t)fl * W * 2);
+        if (got < 0) return fail(SRG_E_IO, "DEM read failed (fd %d, offset %lld)", fddem,
+                                 (long long)fl * W * 2);
+    }
+    DevCtx *c = nullptr;
+    int rc = get_ctx(o.device, &c);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> g(c->mu);
+    cudaStream_t st = 0;
+    const size_t bbytes = (size_t)rawdatalines * samplesPerBurst * 8;
+    if ((rc = c->in_burst.ensure(bbytes)) || (rc = c->in_sat.ensure(24 * (size_t)rawdatalines)) ||
+        (rc = c->in_dem.ensure(npix * 2)) || (rc = c->out.ensure(npix * 8)))
+        return rc;
+    CK(cudaMemcpyAsync(c->in_burst.p, burstdata, bbytes, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(c->in_sat.p, satloc, 24 * (size_t)rawdatalines, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(c->in_dem.p, slab.data(), npix * 2, cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(c->out.p, 0, npix * 8, st));
+
+    srg_burst_desc d{};
+    d.burst = static_cast<const float *>(c->in_burst.p);
+    d.satloc = static_cast<const double *>(c->in_sat.p);
+    d.dem = static_cast<const int16_t *>(c->in_dem.p);
+    d.out = static_cast<float *>(c->out.p);
+    d.coef = nullptr;
+    d.ldb = samplesPerBurst;
+    d.dem_ld = W;
+    d.out_ld = W;
+    d.P = rawdatalines;
+    d.S = samplesPerBurst;
+    d.demwidth = W;
+    d.firstline = fl;
+    d.nlines = nl;
+    d.firstpix = fp;
+    d.lastpix = lp;
+    d.out_pix0 = 0;
+    d.aperture = aperture;
+    d.firstlat = firstlat;
+    d.deltalat = deltalat;
+    d.firstlon = firstlon;
+    d.deltalon = deltalon;
+    d.rngstart = rngstart;
+    d.rngend = rngend;
+    d.dmrg = dmrg;
+    d.wvl = wvl;
+    d.timeorbit = timeorbit;
+    d.xx = xx;
+    d.vv = vv;
+    d.numstatevec = numstatevec;
+    d.tmid = tmid;
+    for (int i = 0; i < 3; ++i) {
+        d.xyz_mid[i] = xyz_mid[i];
+        d.vel_mid[i] = vel_mid[i];
+    }
+    d.angc0 = angc0;
+    d.angc1 = angc1;
+    d.prf = prf;
+    if (fp <= std::min(lp, W - 1)) {
+        rc = run_bursts(*c, &d, 1, o, st);
+        if (rc) return rc;
+    }
+    std::vector<float> out(2 * npix), cur(2 * npix, 0.f);
+    CK(cudaMemcpyAsync(out.data(), c->out.p, npix * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    CK(cudaGetLastError());
+    rc = check_flags(*c, st);
+    if (rc) return rc;
+
+    // merge into the .geo rows (azimuth_compress.cu:510-537)
+    const off_t off = (off_t)fl * W * 8;
+    if (pread(fdout, cur.data(), npix * 8, off) < 0)
+        return fail(SRG_E_IO, "output read failed (fd %d)", fdout);
+    for (size_t i = 0; i < npix; ++i) {
+        if (std::fabs((double)out[2 * i]) > 1.e-18) {
+            cur[2 * i] = out[2 * i];
+            cur[2 * i + 1] = out[2 * i + 1];
+        }
+    }
+    const ssize_t wr = pwrite(fdout, cur.data(), npix * 8, off);
+    if (wr != (ssize_t)(npix * 8)) return fail(SRG_E_IO, "output write failed (fd %d)", fdout);
+    return SRG_OK;
+}
+
+void azimuth_compress_(float *burstdata, double *satloc, int *rawdatalines, int *samplesPerBurst,
+                       int *demwidth, int *demlength, int *fdout, int *fddem, double *deltalat,
+                       double *deltalon, double *firstlat, double *firstlon, double *latlons,
+                       double *timeorbit, double *xx, double *vv, int *numstatevec,
+                       double *rngstart, double *rngend, double *tstart, double *tend, double *tmid,
+                       double *xyz_mid, double *vel_mid, double *t, double *dtaz, double *dmrg,
+                       double *wvl, int *aperture, int *iaperture, double *angc0, double *angc1,
+                       double *prf) {
+    (void)tstart;
+    (void)tend;
+    (void)t;
+    (void)dtaz;
+    (void)iaperture;
+    const int rc = srg_azimuth_compress(
+        burstdata, satloc, *rawdatalines, *samplesPerBurst, *demwidth, *demlength, *fdout, *fddem,
+        *deltalat, *deltalon, *firstlat, *firstlon, latlons, timeorbit, xx, vv, *numstatevec,
+        *rngstart, *rngend, *tmid, xyz_mid, vel_mid, *dmrg, *wvl, *aperture, *angc0, *angc1, *prf,
+        nullptr);
+    if (rc) fprintf(stderr, "azimuth_compress_: error %d: %s\n", rc, g_err.c_str());
+}
+
+}  // extern "C"

@@ -1,0 +1,45 @@
+// common.cuh -- device-side descriptors shared by the backprojection kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace srg {
+
+// Error bits raised by kernels into the device error word.
+enum : int {
+    ERR_TMA_TIMEOUT = 1,   // a bounded mbarrier wait for a TMA tile gave up
+    ERR_BAD_BURST = 2,     // a work item referenced an inconsistent burst
+};
+
+// Everything a kernel needs about one burst, prepared on the host.  Field
+// names follow the reference's (sentinel/azimuth_compress.cu).
+struct BurstDev {
+    const float2 *burst;      // [P][ldb] complex64
+    const double *satloc;     // [P][3]
+    const short *dem;         // row 0 = grid line firstline; stride dem_ld
+    float2 *out;              // row 0 = grid line firstline; stride out_ld
+    const double *coef;       // [nlines][3]
+    long long ldb, dem_ld, out_ld;
+    int P, S, W;
+    int firstline, nlines, firstpix, lastpix;  // lastpix as the reference (may be W)
+    int lastpix_eff;          // min(lastpix, W-1)
+    int out_pix0;
+    int aperture, ap2;        // ap2 = aperture / 2 (integer division, as the reference)
+    int tiles_x, tiles_y, tile_base;
+    int tmap;                 // index of this burst's TMA descriptor, -1 = none
+    int pad0;
+    double firstlat, deltalat, firstlon, deltalon, deg2rad;
+    double rngstart, rmax;    // rmax = rngend - dmrg (the reference's upper range test)
+    double dmrg, k4pi;        // k4pi = 4*pi/wvl, grouped as the reference
+    double K;                 // 2 / wvl: cycles of two-way phase per metre
+    double inv_dmrg;
+    float K_hi, K_lo;         // K as an unevaluated float sum
+    float K_f, inv_dmrg_f;
+};
+
+// Kernel shape of the tiled backprojection.
+struct TileShape {
+    int tx, ty, threads, chunk, window;
+};
+
+}  // namespace srg

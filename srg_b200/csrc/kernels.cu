@@ -1,0 +1,227 @@
+// kernels.cu -- auxiliary device kernels and the compiled shapes of the
+// tiled backprojection.
+#include "bp_kernel.cuh"
+#include "kernels.h"
+
+namespace srg {
+
+// ---------------------------------------------------------------------------
+// Per-line azimuth-centre parabola (sentinel/azimuth_compress.cu:438-481),
+// one thread per grid line.  The reference runs this loop serially on the
+// host; the arithmetic here is the same operation for operation.  Lines
+// firstline .. lastline-1 get a parabola; the last line keeps zeros (the
+// reference leaves it unset), so it is never formed.
+__global__ void line_centres_kernel(BurstDev B, Orbit o, CentreParams cp, double *coef) {
+    const int line = blockIdx.x * blockDim.x + threadIdx.x;
+    if (line >= B.nlines) return;
+    double *cl = coef + 3 * line;
+    if (line == B.nlines - 1) {
+        cl[0] = cl[1] = cl[2] = 0.0;
+        return;
+    }
+    const int half = (B.lastpix - B.firstpix) / 2 - 1;
+    int y[3];
+    for (int s = 0; s < 3; ++s) {
+        const int pix = B.firstpix + s * half;
+        double g[3] = {0.0, 0.0, 0.0};
+        if (pix >= B.firstpix && pix <= B.lastpix && pix >= 0 && pix < B.W) {
+            const double h = (double)B.dem[(long long)line * B.dem_ld + pix];
+            pixel_ecef(B, line, pix, h, g[0], g[1], g[2]);
+        }
+        const double rngpix = zero_doppler_range(o, g, cp.tmid, cp.xm, cp.vm);
+        double u0 = dsub(g[0], cp.xm[0]), u1 = dsub(g[1], cp.xm[1]), u2 = dsub(g[2], cp.xm[2]);
+        const double umag = __dsqrt_rn(dadd(dadd(dmul(u0, u0), dmul(u1, u1)), dmul(u2, u2)));
+        u0 = ddiv(u0, umag);
+        u1 = ddiv(u1, umag);
+        u2 = ddiv(u2, umag);
+        const double udotv = dadd(dadd(dmul(cp.vm[0], u0), dmul(cp.vm[1], u1)), dmul(cp.vm[2], u2));
+        const double fd = dmul(ddiv(2.0, cp.wvl), udotv);
+        const double veff = __dsqrt_rn(
+            dadd(dadd(dmul(cp.vm[0], cp.vm[0]), dmul(cp.vm[1], cp.vm[1])), dmul(cp.vm[2], cp.vm[2])));
+        const double num = dsub(dmul(ddiv(ddiv(ddiv(dmul(rngpix, cp.wvl), 2.0), veff), veff), fd),
+                                ddiv(ddiv(dmul(dmul(rngpix, cp.angc0), cp.pi), 180.0), veff));
+        const double den = dadd(1.0, ddiv(ddiv(dmul(dmul(rngpix, cp.angc1), cp.pi), 180.0), veff));
+        const double td = ddiv(num, den);
+        y[s] = (int)dadd(dmul(td, cp.prf), (double)(B.P / 2));
+    }
+    cl[0] = dmul(0.5, dsub((double)(y[0] + y[2]), dmul(2.0, (double)y[1])));
+    cl[1] = dmul(0.5, (double)(y[2] - y[0]));
+    cl[2] = (double)y[1];
+}
+
+// ---------------------------------------------------------------------------
+// Exact executed-term count with the reference's FP64 predicate
+// (azimuth_compress.cu:54-64), one thread per pixel.
+__global__ void count_terms_kernel(BurstDev B, unsigned long long *terms) {
+    const int nx = B.lastpix_eff - B.firstpix + 1;
+    const long long npix = (long long)nx * B.nlines;
+    unsigned long long cnt = 0;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < npix;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int line = (int)(idx / nx);
+        const int px = B.firstpix + (int)(idx - (long long)line * nx);
+        double X[3];
+        const double h = (double)B.dem[(long long)line * B.dem_ld + px];
+        pixel_ecef(B, line, px, h, X[0], X[1], X[2]);
+        int azs, aze;
+        pixel_window(B, pixel_azoff(B, B.coef + 3 * line, px), azs, aze);
+        for (int k = azs; k < aze; ++k) {
+            const double *s = B.satloc + 3 * k;
+            const double vx = dsub(X[0], s[0]), vy = dsub(X[1], s[1]), vz = dsub(X[2], s[2]);
+            const double R = __dsqrt_rn(dadd(dadd(dmul(vx, vx), dmul(vy, vy)), dmul(vz, vz)));
+            cnt += (R >= B.rngstart && R <= B.rmax) ? 1 : 0;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(terms, cnt);
+}
+
+// ---------------------------------------------------------------------------
+// Ordered merge (azimuth_compress.cu:527-531): replace where |Re(src)| > 1e-18.
+__global__ void merge_kernel(float2 *dst, long long dst_ld, const float2 *src, long long src_ld,
+                             int rows, int cols) {
+    const long long n = (long long)rows * cols;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(i / cols);
+        const int c = (int)(i - (long long)r * cols);
+        const float2 v = src[(long long)r * src_ld + c];
+        if (fabs((double)v.x) > 1.e-18) dst[(long long)r * dst_ld + c] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Per-pulse orbit (sentinel/sentineltimingsub.f90:55-66 with
+// orbithermite.f), one thread per pulse.  Window start int((t-t1)/dt) - 1
+// (1-based) as the reference; clamped to the vector array, where the
+// reference would read outside it.
+__global__ void pulse_orbit_kernel(const double *times, int P, Orbit o, double *pos, double *vel) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= P) return;
+    const double t = times[k];
+    int loc = (int)ddiv(dsub(t, o.t[0]), dsub(o.t[1], o.t[0]));
+    int s = min(max(loc - 2, 0), o.n - 4);
+    hermite4(o.x + 3 * s, o.v + 3 * s, o.t + s, t, pos + 3 * k, vel + 3 * k);
+}
+
+// ---------------------------------------------------------------------------
+// Synthetic-scene forward projection: every pixel of the burst window with a
+// non-zero reflectivity adds a * sinc^2(L sin(psi)/lambda) * exp(-j 4 pi R / lambda)
+// to the two range bins around R of every pulse (the adjoint of linear
+// interpolation).  FP64 geometry; atomic accumulation.
+__global__ void forward_project_kernel(BurstDev B, const float2 *refl, long long refl_ld,
+                                       const double *satvel, double antenna) {
+    const int nx = B.lastpix_eff - B.firstpix + 1;
+    const long long npix = (long long)nx * B.nlines;
+    const double pi = 3.141592653589793;
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= npix) return;
+    const int line = (int)(idx / nx);
+    const int px = B.firstpix + (int)(idx - (long long)line * nx);
+    const float2 a = refl[(long long)line * refl_ld + px];
+    if (a.x == 0.f && a.y == 0.f) return;
+    double X[3];
+    pixel_ecef(B, line, px, (double)B.dem[(long long)line * B.dem_ld + px], X[0], X[1], X[2]);
+    const double wvl = 2.0 / B.K;
+    float2 *out = const_cast<float2 *>(B.burst);
+    for (int k = 0; k < B.P; ++k) {
+        const double *s = B.satloc + 3 * k;
+        const double dx = X[0] - s[0], dy = X[1] - s[1], dz = X[2] - s[2];
+        const double R = sqrt(dx * dx + dy * dy + dz * dz);
+        const double r = (R - B.rngstart) * B.inv_dmrg;
+        if (!(r >= 0.0 && r < (double)(B.S - 1))) continue;
+        const double *v = satvel + 3 * k;
+        const double vn = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        const double spsi = (dx * v[0] + dy * v[1] + dz * v[2]) / (vn * R);
+        const double arg = pi * antenna * spsi / wvl;
+        const double sc = fabs(arg) < 1e-12 ? 1.0 : sin(arg) / arg;
+        const double w = sc * sc;
+        if (w < 1e-7) continue;
+        double sn, cs;
+        sincos(B.k4pi * R, &sn, &cs);
+        // a * w * exp(-j phase)
+        const double vr = w * ((double)a.x * cs + (double)a.y * sn);
+        const double vi = w * ((double)a.y * cs - (double)a.x * sn);
+        const int i = (int)floor(r);
+        const double fr = r - i;
+        float2 *row = out + (long long)k * B.ldb;
+        atomicAdd(&row[i].x, (float)(vr * (1.0 - fr)));
+        atomicAdd(&row[i].y, (float)(vi * (1.0 - fr)));
+        atomicAdd(&row[i + 1].x, (float)(vr * fr));
+        atomicAdd(&row[i + 1].y, (float)(vi * fr));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Compiled shapes of the tiled kernel.  {form, tile_x, tile_y, threads,
+// chunk, window}.
+#define SRG_SHAPES(X)                  \
+    X(FORM_SPLIT, 32, 16, 128, 32, 192) \
+    X(FORM_SPLIT, 64, 8, 128, 32, 256)  \
+    X(FORM_SPLIT, 32, 8, 128, 32, 160)  \
+    X(FORM_SPLIT, 32, 16, 128, 16, 192) \
+    X(FORM_FP64, 32, 8, 128, 32, 160)   \
+    X(FORM_FP64, 32, 4, 128, 32, 128)   \
+    X(FORM_FP64, 32, 16, 128, 16, 192)
+
+#define SRG_ENTRY(F, TXv, TYv, NTv, CKv, WBv) \
+    {F, {TXv, TYv, NTv, CKv, WBv}, params_bytes<F, CKv>(), (const void *)bp_tiles<F, TXv, TYv, NTv, CKv>},
+
+const KernelEntry kKernels[] = {SRG_SHAPES(SRG_ENTRY)};
+const int kNumKernels = sizeof(kKernels) / sizeof(kKernels[0]);
+
+cudaError_t launch_tiles(const KernelEntry &e, int grid, size_t smem, cudaStream_t st,
+                         const BurstDev *bursts, int nb, int total, const CUtensorMap *tmaps,
+                         int *counter, int *err) {
+    int WB = e.shape.window;
+    void *args[] = {(void *)&bursts, (void *)&nb, (void *)&total, (void *)&tmaps,
+                    (void *)&counter, (void *)&err, (void *)&WB};
+    return cudaLaunchKernel(e.fn, dim3(grid), dim3(e.shape.threads), args, smem, st);
+}
+
+cudaError_t launch_line_centres(const BurstDev &B, const Orbit &o, const CentreParams &cp,
+                                double *coef, cudaStream_t st) {
+    const int nt = 128;
+    line_centres_kernel<<<(B.nlines + nt - 1) / nt, nt, 0, st>>>(B, o, cp, coef);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_count_terms(const BurstDev &B, unsigned long long *terms, int sms,
+                               cudaStream_t st) {
+    const int nt = 256;
+    const long long npix = (long long)(B.lastpix_eff - B.firstpix + 1) * B.nlines;
+    if (npix <= 0) return cudaSuccess;
+    long long blocks = (npix + nt - 1) / nt;
+    if (blocks > 64LL * sms) blocks = 64LL * sms;
+    count_terms_kernel<<<(int)blocks, nt, 0, st>>>(B, terms);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_merge(float2 *dst, long long dst_ld, const float2 *src, long long src_ld,
+                         int rows, int cols, int sms, cudaStream_t st) {
+    const long long n = (long long)rows * cols;
+    if (n <= 0) return cudaSuccess;
+    long long blocks = (n + 255) / 256;
+    if (blocks > 32LL * sms) blocks = 32LL * sms;
+    merge_kernel<<<(int)blocks, 256, 0, st>>>(dst, dst_ld, src, src_ld, rows, cols);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pulse_orbit(const double *times, int P, const Orbit &o, double *pos,
+                               double *vel, cudaStream_t st) {
+    if (P <= 0) return cudaSuccess;
+    pulse_orbit_kernel<<<(P + 127) / 128, 128, 0, st>>>(times, P, o, pos, vel);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_forward_project(const BurstDev &B, const float2 *refl, long long refl_ld,
+                                   const double *satvel, double antenna, cudaStream_t st) {
+    const long long npix = (long long)(B.lastpix_eff - B.firstpix + 1) * B.nlines;
+    if (npix <= 0) return cudaSuccess;
+    forward_project_kernel<<<(int)((npix + 127) / 128), 128, 0, st>>>(B, refl, refl_ld, satvel,
+                                                                       antenna);
+    return cudaGetLastError();
+}
+
+}  // namespace srg

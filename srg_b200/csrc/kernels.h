@@ -1,0 +1,43 @@
+// kernels.h -- host-visible launchers of the device kernels.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include "common.cuh"
+#include "geom.cuh"
+
+namespace srg {
+
+// Scalars of the per-line azimuth-centre solve (azimuth_compress.cu:438-481).
+struct CentreParams {
+    double tmid, xm[3], vm[3], wvl, angc0, angc1, prf, pi;
+};
+
+struct KernelEntry {
+    int form;
+    TileShape shape;
+    int params_bytes;
+    const void *fn;
+};
+
+extern const KernelEntry kKernels[];
+extern const int kNumKernels;
+
+cudaError_t launch_tiles(const KernelEntry &e, int grid, size_t smem, cudaStream_t st,
+                         const BurstDev *bursts, int nb, int total, const CUtensorMap *tmaps,
+                         int *counter, int *err);
+cudaError_t launch_line_centres(const BurstDev &B, const Orbit &o, const CentreParams &cp,
+                                double *coef, cudaStream_t st);
+cudaError_t launch_count_terms(const BurstDev &B, unsigned long long *terms, int sms,
+                               cudaStream_t st);
+cudaError_t launch_merge(float2 *dst, long long dst_ld, const float2 *src, long long src_ld,
+                         int rows, int cols, int sms, cudaStream_t st);
+cudaError_t launch_pulse_orbit(const double *times, int P, const Orbit &o, double *pos,
+                               double *vel, cudaStream_t st);
+cudaError_t launch_forward_project(const BurstDev &B, const float2 *refl, long long refl_ld,
+                                   const double *satvel, double antenna, cudaStream_t st);
+
+inline int shared_bytes(const KernelEntry &e) {
+    return e.params_bytes + 1024 + e.shape.chunk * e.shape.window * 8;
+}
+
+}  // namespace srg

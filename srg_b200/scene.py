@@ -1,0 +1,536 @@
+"""Synthetic Sentinel-1-like bursts for the backprojection path.
+
+Builds, deterministically from a seed, every argument of the per-burst
+entry ``azimuth_compress_`` (sentinel/azimuth_compress.cu:181-214) the way the
+reference's drivers derive them:
+
+* orbit state vectors every 10 s around the burst (11 of them, as
+  sentinel/getburststatevectors.f90:112-128 writes), from a circular orbit of
+  radius 7,071 km and inclination 98.18 deg, expressed in the rotating (ECEF)
+  frame;
+* per-pulse satellite positions/velocities by 4-point Hermite interpolation of
+  those vectors, with the window rule of sentinel/sentineltimingsub.f90:55-66
+  and the text quantisation of its write (f16.7 m, f14.8 m/s);
+* burst-centre position/velocity with the clamped window of
+  sentinel/intp_orbit.f90;
+* rngstart/rngend/dmrg/tmid as sentinel/backprojectcpusub.f90:216-227 and the
+  aperture length as backprojectcpusub.f90:195-211;
+* an int16 ellipsoid-height DEM (flat, or a volcano cone plus fBm roughness)
+  on a lat/lon grid whose centre is the beam centre of the burst.
+
+Range-compressed samples are synthesised here for point targets (numpy); the
+distributed-scatterer forward projection of the large configurations runs on
+the GPU (``srg_b200.api.forward_project``).
+
+Everything is float64 numpy; no value here feeds a parity claim except
+through arrays that are handed, bit for bit, to both the CUDA path and the
+oracle.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import List, Optional
+
+import numpy as np
+
+C_LIGHT = 299792458.0
+WGS84_A = 6378137.0
+WGS84_E2 = 0.0066943799901499996
+GM_EARTH = 3.986004418e14
+OMEGA_EARTH = 7.2921159e-5
+
+# Radar constants of the synthetic configurations.
+WAVELENGTH = 0.0554658
+PRF = 1717.13
+RANGE_FS = 64.345e6
+NEAR_RANGE = 800.0e3
+ORBIT_RADIUS = 7071.0e3
+ORBIT_INCL_DEG = 98.18
+SV_SPACING = 10.0
+
+
+@dataclasses.dataclass
+class Burst:
+    """All arguments of one ``azimuth_compress_`` call (names as the reference)."""
+
+    burst: np.ndarray            # [P][S] complex64 range-compressed lines
+    satloc: np.ndarray           # [P][3] float64 ECEF position per pulse
+    satvel: np.ndarray           # [P][3] float64 ECEF velocity per pulse
+    pulse_time: np.ndarray       # [P] float64 line times (s)
+    demwidth: int
+    demlength: int
+    deltalat: float              # deg (negative: lines run north to south)
+    deltalon: float
+    firstlat: float
+    firstlon: float
+    latlons: np.ndarray          # [4] min lat, max lat, min lon, max lon
+    timeorbit: np.ndarray        # [n]
+    xx: np.ndarray               # [n][3]
+    vv: np.ndarray               # [n][3]
+    rngstart: float
+    rngend: float
+    tstart: float
+    tend: float
+    tmid: float
+    xyz_mid: np.ndarray          # [3]
+    vel_mid: np.ndarray          # [3]
+    dtaz: float
+    dmrg: float
+    wvl: float
+    aperture: int
+    iaperture: int
+    angc0: float
+    angc1: float
+    prf: float
+    dem: Optional[np.ndarray] = None     # [demlength][demwidth] int16 (full DEM)
+    targets: Optional[np.ndarray] = None  # [T][3] (line, pixel, amplitude) of point targets
+
+    @property
+    def rawdatalines(self) -> int:
+        return int(self.burst.shape[0])
+
+    @property
+    def samples(self) -> int:
+        return int(self.burst.shape[1])
+
+    @property
+    def numstatevec(self) -> int:
+        return int(self.timeorbit.shape[0])
+
+
+# --------------------------------------------------------------------------
+# orbit
+
+
+@dataclasses.dataclass
+class CircularOrbit:
+    radius: float = ORBIT_RADIUS
+    incl_deg: float = ORBIT_INCL_DEG
+    raan: float = 0.0
+    u0: float = 0.0          # argument of latitude at epoch
+    epoch: float = 0.0       # s; Earth rotation angle is zero here
+    ascending: bool = True
+
+    @property
+    def mean_motion(self) -> float:
+        return math.sqrt(GM_EARTH / self.radius ** 3)
+
+    def state(self, t):
+        """ECEF position and velocity at times t (array) -> ([N,3], [N,3])."""
+        t = np.asarray(t, dtype=np.float64)
+        n = self.mean_motion
+        u = self.u0 + n * (t - self.epoch)
+        inc = math.radians(self.incl_deg)
+        co, so = math.cos(self.raan), math.sin(self.raan)
+        ci, si = math.cos(inc), math.sin(inc)
+        cu, su = np.cos(u), np.sin(u)
+        r = self.radius
+        xi = np.stack([r * (co * cu - so * su * ci), r * (so * cu + co * su * ci), r * su * si], -1)
+        vi = np.stack([r * n * (-co * su - so * cu * ci), r * n * (-so * su + co * cu * ci),
+                       r * n * cu * si], -1)
+        th = OMEGA_EARTH * (t - self.epoch)
+        ct, st = np.cos(th), np.sin(th)
+        # rotate inertial -> ECEF by -theta about z
+        x = np.stack([ct * xi[..., 0] + st * xi[..., 1], -st * xi[..., 0] + ct * xi[..., 1],
+                      xi[..., 2]], -1)
+        vrot = np.stack([ct * vi[..., 0] + st * vi[..., 1], -st * vi[..., 0] + ct * vi[..., 1],
+                         vi[..., 2]], -1)
+        # v_ecef = R v_i - omega x x_ecef
+        v = vrot + np.stack([OMEGA_EARTH * x[..., 1], -OMEGA_EARTH * x[..., 0],
+                             np.zeros_like(x[..., 2])], -1)
+        return x, v
+
+
+def hermite4(ts, xs, vs, t):
+    """4-point position/velocity Hermite interpolation.
+
+    Same basis as sentinel/orbithermite.f:21-70 (value f0/f1 and derivative
+    g0/g1 weights built on the Lagrange polynomials h and their derivatives).
+    ts: [..., 4]; xs, vs: [..., 4, 3]; t: [...].  Returns ([..., 3], [..., 3]).
+    """
+    ts = np.asarray(ts, np.float64)
+    t = np.asarray(t, np.float64)[..., None]
+    n = 4
+    inv = np.zeros(ts.shape[:-1] + (n, n))
+    for i in range(n):
+        for j in range(n):
+            if i != j:
+                inv[..., i, j] = 1.0 / (ts[..., i] - ts[..., j])
+    s = inv.sum(-1)  # sum_j!=i 1/(t_i - t_j)
+    dt = t - ts
+    f0 = 1.0 - 2.0 * dt * s
+    f1 = dt
+    h = np.ones_like(ts)
+    for i in range(n):
+        for k in range(n):
+            if k != i:
+                h[..., i] = h[..., i] * (t[..., 0] - ts[..., k]) / (ts[..., i] - ts[..., k])
+    hd = np.zeros_like(ts)
+    for i in range(n):
+        acc = np.zeros(ts.shape[:-1])
+        for j in range(n):
+            if j == i:
+                continue
+            q = np.ones(ts.shape[:-1])
+            for k in range(n):
+                if k != i and k != j:
+                    q = q * (t[..., 0] - ts[..., k]) / (ts[..., i] - ts[..., k])
+            acc = acc + inv[..., i, j] * q
+        hd[..., i] = acc
+    g1 = h + 2.0 * dt * hd
+    g0 = 2.0 * (f0 * hd - h * s)
+    xq = np.sum((xs * f0[..., None] + vs * f1[..., None]) * (h * h)[..., None], axis=-2)
+    vq = np.sum((xs * g0[..., None] + vs * g1[..., None]) * h[..., None], axis=-2)
+    return xq, vq
+
+
+def interp_pulses(timeorbit, xx, vv, times):
+    """Per-pulse orbit: window start int((t - t1)/dt) - 1 (1-based), unclamped,
+    as sentinel/sentineltimingsub.f90:61-63."""
+    dt = timeorbit[1] - timeorbit[0]
+    loc = np.trunc((times - timeorbit[0]) / dt).astype(np.int64)
+    s = loc - 2
+    if np.any(s < 0) or np.any(s + 3 >= len(timeorbit)):
+        raise ValueError("pulse times fall outside the state-vector window")
+    idx = s[:, None] + np.arange(4)[None, :]
+    return hermite4(timeorbit[idx], xx[idx], vv[idx], times)
+
+
+def intp_orbit(timeorbit, xx, vv, t):
+    """Clamped-window Hermite as sentinel/intp_orbit.f90:1-25."""
+    n = len(timeorbit)
+    loc = int((t - timeorbit[0]) / (timeorbit[1] - timeorbit[0]))
+    loc = min(max(loc, 2), n - 2)
+    s = loc - 2
+    xq, vq = hermite4(timeorbit[s:s + 4], xx[s:s + 4], vv[s:s + 4], np.float64(t))
+    return xq, vq
+
+
+def quantise_positions(x, v):
+    """Round-trip through the text format f16.7 / f14.8
+    (sentinel/sentineltimingsub.f90:65, read back at backprojectcpusub.f90:179)."""
+    xq = np.array([[float(f"{c:.7f}") for c in row] for row in x])
+    vq = np.array([[float(f"{c:.8f}") for c in row] for row in v])
+    return xq, vq
+
+
+# --------------------------------------------------------------------------
+# geodesy
+
+
+def llh_to_ecef(lat_deg, lon_deg, h):
+    lat = np.radians(lat_deg)
+    lon = np.radians(lon_deg)
+    s = np.sin(lat)
+    re = WGS84_A / np.sqrt(1.0 - WGS84_E2 * s * s)
+    x = (re + h) * np.cos(lat) * np.cos(lon)
+    y = (re + h) * np.cos(lat) * np.sin(lon)
+    z = (re * (1.0 - WGS84_E2) + h) * s
+    return np.stack([x, y, z], -1)
+
+
+def ecef_to_llh(p):
+    x, y, z = p[..., 0], p[..., 1], p[..., 2]
+    lon = np.arctan2(y, x)
+    rho = np.hypot(x, y)
+    lat = np.arctan2(z, rho * (1 - WGS84_E2))
+    for _ in range(8):
+        s = np.sin(lat)
+        re = WGS84_A / np.sqrt(1 - WGS84_E2 * s * s)
+        h = rho / np.cos(lat) - re
+        lat = np.arctan2(z, rho * (1 - WGS84_E2 * re / (re + h)))
+    s = np.sin(lat)
+    re = WGS84_A / np.sqrt(1 - WGS84_E2 * s * s)
+    h = rho / np.cos(lat) - re
+    return np.degrees(lat), np.degrees(lon), h
+
+
+def zero_doppler_point(sat, vel, slant, height, right=True):
+    """Ground point at the given slant range and ellipsoid height in the plane
+    through `sat` perpendicular to `vel` (zero Doppler), right-looking."""
+    vhat = vel / np.linalg.norm(vel)
+    down = -sat / np.linalg.norm(sat)
+    down = down - np.dot(down, vhat) * vhat
+    down /= np.linalg.norm(down)
+    side = np.cross(vhat, down)          # right of track for a right-looking SAR
+    if not right:
+        side = -side
+    ang = 0.5
+    for _ in range(60):
+        p = sat + slant * (math.cos(ang) * down + math.sin(ang) * side)
+        _, _, h = ecef_to_llh(p)
+        # d h / d ang by finite difference
+        p2 = sat + slant * (math.cos(ang + 1e-7) * down + math.sin(ang + 1e-7) * side)
+        _, _, h2 = ecef_to_llh(p2)
+        dh = (h2 - h) / 1e-7
+        step = (h - height) / dh
+        ang -= step
+        if abs(step) < 1e-13:
+            break
+    return sat + slant * (math.cos(ang) * down + math.sin(ang) * side)
+
+
+# --------------------------------------------------------------------------
+# DEM
+
+
+def fbm_surface(rng, ny, nx, hurst, rms):
+    """Spectral-synthesis fractional Brownian surface with the given RMS."""
+    ky = np.fft.fftfreq(ny)[:, None]
+    kx = np.fft.rfftfreq(nx)[None, :]
+    k = np.sqrt(kx * kx + ky * ky)
+    k[0, 0] = 1.0
+    amp = k ** (-(hurst + 1.0))
+    amp[0, 0] = 0.0
+    ph = rng.standard_normal((ny, kx.shape[1])) + 1j * rng.standard_normal((ny, kx.shape[1]))
+    surf = np.fft.irfft2(amp * ph, s=(ny, nx))
+    surf -= surf.mean()
+    surf *= rms / max(surf.std(), 1e-30)
+    return surf
+
+
+def volcano_dem(rng, ny, nx, peak=2500.0, base=0.0, radius_frac=0.45, hurst=0.8, rms=30.0):
+    yy, xx = np.mgrid[0:ny, 0:nx]
+    cy, cx = (ny - 1) / 2.0, (nx - 1) / 2.0
+    rad = radius_frac * min(ny, nx) * 1.6
+    d = np.sqrt(((yy - cy) / 1.0) ** 2 + ((xx - cx) / 1.0) ** 2) / rad
+    cone = base + peak * np.clip(1.0 - d, 0.0, 1.0)
+    h = cone + fbm_surface(rng, ny, nx, hurst, rms)
+    return np.clip(np.rint(h), -32768, 32767).astype(np.int16)
+
+
+# --------------------------------------------------------------------------
+# burst geometry
+
+
+def aperture_points(satvel, rngstart, wvl, prf, angc1=0.0):
+    """sentinel/backprojectcpusub.f90:195-211 (TOPS aperture, 50 % of nominal)."""
+    re, ht = 6378137.0, 700000.0
+    p = satvel.shape[0]
+    v = satvel[p // 2 - 1]  # Fortran satvel(:, rawdatalines/2)
+    vmag = math.sqrt(float(np.dot(v, v))) * (re / (re + ht))
+    pi = 4.0 * math.atan2(1.0, 1.0)
+    aperturetime = (rngstart * wvl / 2 / vmag / vmag * prf) / (1.0 + rngstart * angc1 * pi / 180.0 / vmag)
+    return int(aperturetime * prf * 0.5)
+
+
+def make_geometry(*, pulses: int, samples: int, width: int, length: int, spacing: float,
+                  near_range: float = NEAR_RANGE, wvl: float = WAVELENGTH, prf: float = PRF,
+                  fs: float = RANGE_FS, lat0: float = 19.4, tmid_nominal: float = 43200.25,
+                  centre_height: float = 0.0, aperture: Optional[int] = None,
+                  angc0: float = 0.0, angc1: float = 0.0, quantise: bool = True,
+                  grid_centre: Optional[tuple] = None, orbit: Optional[CircularOrbit] = None,
+                  along_offset: float = 0.0) -> Burst:
+    """Orbit, pulses and grid of one burst; samples are left zero."""
+    if orbit is None:
+        inc = math.radians(ORBIT_INCL_DEG)
+        u0 = math.asin(math.sin(math.radians(lat0)) / math.sin(inc))
+        orbit = CircularOrbit(u0=u0, epoch=tmid_nominal)
+    dtaz = 1.0 / prf
+    tstart = tmid_nominal - 0.5 * (pulses - 1) * dtaz + along_offset
+    tend = tstart + (pulses - 1) * dtaz
+    tmid = 0.5 * (tstart + tend)
+    t0 = math.floor((tstart - 30.0) / SV_SPACING) * SV_SPACING + SV_SPACING
+    timeorbit = t0 + SV_SPACING * np.arange(11, dtype=np.float64)
+    xx, vv = orbit.state(timeorbit)
+    ptime = tstart + np.arange(pulses, dtype=np.float64) * dtaz
+    sx, sv = interp_pulses(timeorbit, xx, vv, ptime)
+    if quantise:
+        sx, sv = quantise_positions(sx, sv)
+    xyz_mid, vel_mid = intp_orbit(timeorbit, xx, vv, tmid)
+    dmrg = C_LIGHT / 2.0 / fs
+    rngstart = near_range
+    rngend = rngstart + (samples - 1) * dmrg
+    if grid_centre is None:
+        smid, vmid = orbit.state(np.array([tmid_nominal]))
+        pc = zero_doppler_point(smid[0], vmid[0], 0.5 * (rngstart + rngend), centre_height)
+        clat, clon, _ = ecef_to_llh(pc)
+        clat, clon = float(clat), float(clon)
+    else:
+        clat, clon = grid_centre
+    deltalat = -spacing
+    deltalon = spacing
+    firstlat = clat + 0.5 * (length - 1) * spacing
+    firstlon = clon - 0.5 * (width - 1) * spacing
+    # lat/lon box covering the whole grid (firstpix = 0, lastpix clamps to W)
+    latlons = np.array([firstlat + (length - 0.5) * deltalat, firstlat + 0.25 * spacing,
+                        firstlon + 0.25 * spacing, firstlon + (width + 0.5) * deltalon])
+    if aperture is None:
+        aperture = aperture_points(sv, rngstart, wvl, prf, angc1)
+    return Burst(
+        burst=np.zeros((pulses, samples), np.complex64), satloc=np.ascontiguousarray(sx),
+        satvel=np.ascontiguousarray(sv), pulse_time=ptime, demwidth=width, demlength=length,
+        deltalat=deltalat, deltalon=deltalon, firstlat=firstlat, firstlon=firstlon,
+        latlons=latlons, timeorbit=timeorbit, xx=np.ascontiguousarray(xx),
+        vv=np.ascontiguousarray(vv), rngstart=rngstart, rngend=rngend, tstart=tstart, tend=tend,
+        tmid=tmid, xyz_mid=np.ascontiguousarray(xyz_mid), vel_mid=np.ascontiguousarray(vel_mid),
+        dtaz=dtaz, dmrg=dmrg, wvl=wvl, aperture=int(aperture), iaperture=0, angc0=angc0,
+        angc1=angc1, prf=prf)
+
+
+def grid_ecef(b: Burst, lines, pixels, heights):
+    lat = b.firstlat + np.asarray(lines, np.float64) * b.deltalat
+    lon = b.firstlon + np.asarray(pixels, np.float64) * b.deltalon
+    return llh_to_ecef(lat, lon, np.asarray(heights, np.float64))
+
+
+# --------------------------------------------------------------------------
+# samples
+
+
+def _sinc(x):
+    return np.sinc(x)
+
+
+def add_point_targets(b: Burst, positions, amplitudes, taps: int = 16, antenna: float = 10.0):
+    """Forward-project point targets into the range-compressed lines.
+
+    Per pulse each target adds sinc(bin - r) * exp(-j 4 pi R / lambda), weighted
+    by a sinc^2 azimuth antenna pattern of a `antenna`-metre aperture, with a
+    Hann-tapered +-`taps` bin range response.
+    """
+    P, S = b.burst.shape
+    out = b.burst
+    offs = np.arange(-taps, taps + 1)
+    for pos, amp in zip(np.asarray(positions), np.asarray(amplitudes)):
+        d = pos[None, :] - b.satloc
+        R = np.sqrt(np.sum(d * d, axis=1))
+        vhat = b.satvel / np.linalg.norm(b.satvel, axis=1)[:, None]
+        sin_sq = np.sum(d * vhat, axis=1) / R
+        w_az = _sinc(antenna * sin_sq / b.wvl) ** 2
+        r = (R - b.rngstart) / b.dmrg
+        base = np.floor(r).astype(np.int64)
+        bins = base[:, None] + offs[None, :]
+        x = bins - r[:, None]
+        win = 0.5 * (1.0 + np.cos(np.pi * np.clip(x / (taps + 1), -1, 1)))
+        val = _sinc(x) * win * w_az[:, None]
+        ph = np.exp(-1j * (4.0 * np.pi / b.wvl) * R)
+        contrib = (amp * val * ph[:, None]).astype(np.complex64)
+        ok = (bins >= 0) & (bins < S)
+        rows = np.broadcast_to(np.arange(P)[:, None], bins.shape)
+        np.add.at(out, (rows[ok], bins[ok]), contrib[ok])
+
+
+def add_noise(b: Burst, rng, snr_db: float, ref_amplitude: float = 1.0):
+    """Complex Gaussian noise; SNR is the per-sample ratio of a unit target's
+    peak power (ref_amplitude^2) to the noise power."""
+    sigma2 = ref_amplitude ** 2 / 10 ** (snr_db / 10.0)
+    s = math.sqrt(sigma2 / 2.0)
+    n = rng.standard_normal(b.burst.shape + (2,), dtype=np.float32) * np.float32(s)
+    b.burst += n[..., 0] + 1j * n[..., 1]
+
+
+# --------------------------------------------------------------------------
+# configurations
+
+
+def config0_point_targets(seed: int = 1000, pulses: int = 1024, samples: int = 4096,
+                          width: int = 256, length: int = 256, spacing: float = 0.0002,
+                          ntargets: int = 64, height: float = 500.0, snr_db: float = 10.0,
+                          quantise: bool = True) -> Burst:
+    """64 point targets on flat 500 m terrain, 10 dB SNR (configuration 0)."""
+    rng = np.random.default_rng(seed)
+    b = make_geometry(pulses=pulses, samples=samples, width=width, length=length,
+                      spacing=spacing, centre_height=height, quantise=quantise)
+    b.dem = np.full((length, width), int(height), np.int16)
+    band = formed_line_band(b)
+    lo, hi = band
+    lines = rng.integers(lo + 2, max(lo + 3, hi - 2), ntargets)
+    pixels = rng.integers(8, width - 8, ntargets)
+    amps = np.ones(ntargets)
+    pos = grid_ecef(b, lines, pixels, np.full(ntargets, height))
+    add_point_targets(b, pos, amps)
+    add_noise(b, rng, snr_db)
+    b.targets = np.stack([lines, pixels, amps], -1)
+    return b
+
+
+def formed_line_band(b: Burst):
+    """Approximate range of grid lines whose aperture centre lies inside
+    (aperture/2, P - aperture/2), from the zero-Doppler time of the grid centre
+    column.  Used only to place synthetic targets."""
+    P = b.rawdatalines
+    lines = np.arange(b.demlength)
+    pix = np.full_like(lines, b.demwidth // 2)
+    h = 0.0 if b.dem is None else float(np.median(b.dem))
+    pts = grid_ecef(b, lines, pix, np.full(lines.shape, h))
+    # zero-Doppler pulse index by nearest approach
+    d = pts[:, None, :] - b.satloc[None, ::8, :]
+    dop = np.sum(d * b.satvel[None, ::8, :], axis=-1)
+    k = np.argmin(np.abs(dop), axis=1) * 8
+    ok = (k > b.aperture // 2 + 4) & (k < P - b.aperture // 2 - 4)
+    if not np.any(ok):
+        return 0, 0
+    idx = np.nonzero(ok)[0]
+    return int(idx.min()), int(idx.max())
+
+
+def config1_geometry(seed: int = 1001, pulses: int = 1500, samples: int = 21000,
+                     width: int = 2400, length: int = 1200, spacing: float = 0.0001,
+                     quantise: bool = True, **kw) -> Burst:
+    """IW1-sized burst over a volcano DEM (configuration 1); samples are
+    produced on the GPU by forward projection."""
+    rng = np.random.default_rng(seed)
+    b = make_geometry(pulses=pulses, samples=samples, width=width, length=length,
+                      spacing=spacing, centre_height=1000.0, quantise=quantise, **kw)
+    b.dem = volcano_dem(rng, length, width)
+    return b
+
+
+def mini_samples(seed: int, pulses: int, samples: int) -> np.ndarray:
+    """Integer-valued complex64 samples (components k/16, |k| <= 64), exactly
+    reproducible on any platform from the seed."""
+    rng = np.random.default_rng([seed, 2])
+    raw = rng.integers(-64, 65, size=(pulses, samples, 2), dtype=np.int32).astype(np.float32)
+    return (raw[..., 0] + 1j * raw[..., 1]).astype(np.complex64) * np.float32(1.0 / 16)
+
+
+def mini_fixture(seed: int, pulses: int = 320, samples: int = 384, width: int = 48,
+                 length: int = 40, spacing: float = 0.0002, aperture: int = 96,
+                 angc0: float = 0.0, angc1: float = 0.0, dem_kind: str = "slope",
+                 latlons_inset: int = 0) -> Burst:
+    """Small scene for the golden fixtures: integer-valued samples
+    (``mini_samples``) and an integer DEM, so that everything but the orbit
+    arrays can be regenerated bit for bit; the fixtures store the orbit
+    arrays themselves."""
+    rng = np.random.default_rng([seed, 1])
+    b = make_geometry(pulses=pulses, samples=samples, width=width, length=length,
+                      spacing=spacing, centre_height=200.0, aperture=aperture,
+                      angc0=angc0, angc1=angc1)
+    if dem_kind == "flat":
+        b.dem = np.full((length, width), 200, np.int16)
+    else:
+        yy, xx = np.mgrid[0:length, 0:width]
+        b.dem = (150 + 3 * xx + 2 * yy + rng.integers(-20, 21, (length, width))).astype(np.int16)
+    b.burst = mini_samples(seed, pulses, samples)
+    if latlons_inset:
+        # shrink the pixel box: firstpix = inset, lastpix = W - 1 - inset
+        b.latlons[2] = b.firstlon + (latlons_inset + 0.25) * b.deltalon
+        b.latlons[3] = b.firstlon + (width - 1 - latlons_inset + 0.25) * b.deltalon
+    return b
+
+
+# Fields of a Burst that a fixture stores verbatim.
+ARRAY_FIELDS = ("satloc", "satvel", "pulse_time", "latlons", "timeorbit", "xx", "vv", "xyz_mid",
+                "vel_mid", "dem")
+FLOAT_FIELDS = ("deltalat", "deltalon", "firstlat", "firstlon", "rngstart", "rngend", "tstart",
+                "tend", "tmid", "dtaz", "dmrg", "wvl", "angc0", "angc1", "prf")
+INT_FIELDS = ("demwidth", "demlength", "aperture", "iaperture")
+
+
+def burst_to_arrays(b: Burst) -> dict:
+    out = {k: np.asarray(getattr(b, k)) for k in ARRAY_FIELDS}
+    out["floats"] = np.array([getattr(b, k) for k in FLOAT_FIELDS], np.float64)
+    out["ints"] = np.array([getattr(b, k) for k in INT_FIELDS] + list(b.burst.shape), np.int64)
+    return out
+
+
+def burst_from_arrays(a, samples: np.ndarray) -> Burst:
+    kw = {k: np.array(a[k]) for k in ARRAY_FIELDS if k != "dem"}
+    kw.update({k: float(v) for k, v in zip(FLOAT_FIELDS, a["floats"])})
+    ints = [int(v) for v in a["ints"]]
+    kw.update({k: v for k, v in zip(INT_FIELDS, ints[:len(INT_FIELDS)])})
+    b = Burst(burst=samples, **kw)
+    b.dem = np.array(a["dem"], np.int16)
+    return b

@@ -1,0 +1,189 @@
+"""Parity of the CUDA path (libsrg_bp.so, called through its C ABI) with the
+oracle and the golden fixtures made by the compiled reference."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import MINI_CASES, load_golden, mini_case, phase_amp_errors, rel_err
+from srg_b200 import _lib, api, scene
+
+pytestmark = pytest.mark.gpu
+NAMES = [c[0] for c in MINI_CASES]
+SPLIT_CFGS = [c[0] for c in _lib.tile_configs() if c[1] == _lib.FORM_SPLIT]
+FP64_CFGS = [c[0] for c in _lib.tile_configs() if c[1] == _lib.FORM_FP64]
+
+# Tolerances.  FP64 form vs the oracle's GPU form: identical bins, weights and
+# phases up to the last ulp of sin/cos and of the FP64 accumulation order, so
+# the complex64 outputs agree to FP32 rounding.  Split form: the acceptance
+# bound of the design (<= 1 mrad RMS phase error against the FP64 oracle),
+# with the measured errors ~100x smaller.
+FP64_REL = 2e-6
+SPLIT_PH_RMS_MRAD = 1.0
+SPLIT_PH_MAX_MRAD = 10.0
+SPLIT_AMP_RMS = 1e-3
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("the CUDA path needs a GPU; none is visible")
+    return torch
+
+
+@pytest.fixture(scope="module")
+def orc():
+    O.build()
+    return O.Oracle()
+
+
+def run_dev(b, form, cfg=-1):
+    db = api.to_device(b)
+    api.backproject([db], form=form, tile_cfg=cfg)
+    return db, db.out.cpu().numpy()
+
+
+def oracle_gpu_form(orc, b):
+    return orc.stages(b, gpu_lerp=1, gpu_scale=1, want_acc=True)
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_line_centres_exact(torch_cuda, orc, name):
+    b = mini_case(name)
+    st = orc.stages(b)
+    db = api.to_device(b)
+    coef = api.line_centres(db).cpu().numpy()
+    assert np.array_equal(coef, st["coef"])
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_term_count_exact(torch_cuda, orc, name):
+    b = mini_case(name)
+    st = orc.stages(b)
+    db = api.to_device(b)
+    assert api.count_terms([db]) == st["terms"]
+
+
+@pytest.mark.parametrize("cfg", FP64_CFGS)
+@pytest.mark.parametrize("name", NAMES)
+def test_fp64_form_matches_oracle(torch_cuda, orc, name, cfg):
+    b = mini_case(name)
+    st = oracle_gpu_form(orc, b)
+    _, out = run_dev(b, _lib.FORM_FP64, cfg)
+    ref = st["out"]
+    assert np.array_equal(out != 0, ref != 0)
+    assert rel_err(out, ref) < FP64_REL
+
+
+@pytest.mark.parametrize("cfg", SPLIT_CFGS)
+@pytest.mark.parametrize("name", NAMES)
+def test_split_form_within_phase_budget(torch_cuda, orc, name, cfg):
+    b = mini_case(name)
+    st = oracle_gpu_form(orc, b)
+    _, out = run_dev(b, _lib.FORM_SPLIT, cfg)
+    e = phase_amp_errors(out, st["out"])
+    assert e["n"] > 100
+    assert e["ph_rms"] < SPLIT_PH_RMS_MRAD, e
+    assert e["ph_max"] < SPLIT_PH_MAX_MRAD, e
+    assert e["amp_rms"] < SPLIT_AMP_RMS, e
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_fp64_form_matches_golden_reference(torch_cuda, name):
+    """Against the compiled reference's own raw sums (CPU form: unscaled, FP64
+    interpolation), rescaled by the aperture length."""
+    b, g = load_golden(name)
+    _, out = run_dev(b, _lib.FORM_FP64)
+    az = g["ref_azoff"]
+    a0 = np.clip(np.round(az - b.aperture // 2).astype(int), 0, None)
+    a1 = np.clip(np.round(az + b.aperture // 2).astype(int), None, b.rawdatalines - 1)
+    formed = az > 0
+    ref = np.zeros_like(g["ref_pixelint"])
+    ref[formed] = g["ref_pixelint"][formed] * (1.0 / (a1 - a0)[formed]).astype(np.float32)
+    assert rel_err(out, ref) < 1e-5
+
+
+@pytest.mark.parametrize("form", [_lib.FORM_FP64, _lib.FORM_SPLIT])
+@pytest.mark.parametrize("name", ["slope", "inset", "oddS"])
+def test_dropin_entry_matches_oracle_entry(torch_cuda, orc, name, form):
+    """azimuth_compress_ (33 by-reference arguments, DEM and .geo by file
+    descriptor) against the oracle's entry with the GPU merge rule, starting
+    from a non-zero .geo so that the merge rule is exercised."""
+    b = mini_case(name)
+    rng = np.random.default_rng(7)
+    init = (rng.standard_normal((b.demlength, b.demwidth)) +
+            1j * rng.standard_normal((b.demlength, b.demwidth))).astype(np.complex64)
+    ref = O.run_33_files(orc.lib.srg_oracle_azimuth_compress_, b, geo_init=init)
+    api.set_default_form(form)
+    try:
+        got = O.run_33_files(_lib.lib().azimuth_compress_, b, geo_init=init)
+    finally:
+        api.set_default_form(_lib.FORM_SPLIT)
+    changed_ref = ref != init
+    changed = got != init
+    assert np.array_equal(changed, changed_ref)
+    if form == _lib.FORM_FP64:
+        assert rel_err(got, ref) < FP64_REL
+    else:
+        e = phase_amp_errors(got[changed], ref[changed])
+        assert e["ph_rms"] < SPLIT_PH_RMS_MRAD, e
+
+
+def test_status_entry_reports_errors(torch_cuda):
+    b = mini_case("flat")
+    with tempfile.TemporaryDirectory() as td:
+        dem = os.path.join(td, "d.dem")
+        b.dem.astype(np.int16).tofile(dem)
+        fd = os.open(dem, os.O_RDONLY)
+        try:
+            with pytest.raises(_lib.SrgError) as ei:
+                # output descriptor -1: the DEM is read, the .geo read fails
+                api.azimuth_compress_status(b, -1, fd, form=_lib.FORM_SPLIT)
+            assert ei.value.code == _lib.SRG_E_IO
+        finally:
+            os.close(fd)
+
+
+def test_batched_launch_equals_single(torch_cuda):
+    bs = [mini_case(n) for n in ("flat", "tops", "inset", "oddS")]
+    singles = [run_dev(b, _lib.FORM_SPLIT)[1] for b in bs]
+    dbs = [api.to_device(b) for b in bs]
+    api.backproject(dbs, form=_lib.FORM_SPLIT)
+    for db, s in zip(dbs, singles):
+        assert np.array_equal(db.out.cpu().numpy().view(np.uint32), s.view(np.uint32))
+
+
+def test_pulse_orbit_kernel(torch_cuda):
+    torch = torch_cuda
+    b = scene.make_geometry(pulses=1500, samples=64, width=8, length=8, spacing=1e-4,
+                            quantise=False)
+    t = torch.from_numpy(b.pulse_time).cuda()
+    pos, vel = api.pulse_orbit(t, b)
+    np.testing.assert_allclose(pos.cpu().numpy(), b.satloc, rtol=0, atol=1e-6)
+    np.testing.assert_allclose(vel.cpu().numpy(), b.satvel, rtol=0, atol=1e-9)
+
+
+def test_config0_point_targets(torch_cuda, orc):
+    """Configuration 0: 1,024 x 4,096 burst, 64 point targets, 256 x 256 grid.
+    Both forms against the oracle, and the physics check: every target focuses
+    on its own pixel with a phase near zero."""
+    b = scene.config0_point_targets()
+    st = oracle_gpu_form(orc, b)
+    db = api.to_device(b)
+    assert api.count_terms([db]) == st["terms"]
+    api.backproject([db], form=_lib.FORM_FP64)
+    f64 = db.out.cpu().numpy()
+    assert rel_err(f64, st["out"]) < FP64_REL
+    api.backproject([db], form=_lib.FORM_SPLIT)
+    spl = db.out.cpu().numpy()
+    e = phase_amp_errors(spl, st["out"])
+    assert e["ph_rms"] < SPLIT_PH_RMS_MRAD and e["amp_rms"] < SPLIT_AMP_RMS, e
+    fl = st["firstline"]
+    for line, pix, _ in b.targets.astype(int):
+        li = line - fl
+        win = np.abs(spl[li - 2:li + 3, pix - 2:pix + 3])
+        assert np.unravel_index(np.argmax(win), win.shape) == (2, 2)
+        assert abs(np.angle(spl[li, pix])) < 0.1
