@@ -155,6 +155,11 @@ int srg_pulse_orbit_device(const double *times, int P, const double *timeorbit,
  * library's kernels since the last check (SRG_E_TIMEOUT) or CUDA error. */
 int srg_sync_check(void *stream);
 
+/* Calibration: measured FMA issue-rate peak of the current device in
+ * TFLOP/s (2 flops per FMA), FP32 (fp64 = 0) or FP64 (fp64 = 1), from a
+ * full-occupancy chain-of-FMA kernel timed with CUDA events.  Blocking. */
+int srg_measure_fma_peak(int fp64, double *tflops);
+
 /* Number of compiled kernel shapes, and the shape of one of them. */
 int srg_tile_config_count(void);
 int srg_tile_config(int idx, int *tile_x, int *tile_y, int *threads, int *chunk,

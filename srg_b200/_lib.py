@@ -72,6 +72,7 @@ _SIGS = {
     "srg_pulse_orbit_device": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp, C.c_int, C.c_void_p,
                                          C.c_void_p, C.c_void_p]),
     "srg_sync_check": (C.c_int, [C.c_void_p]),
+    "srg_measure_fma_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
     "srg_tile_config_count": (C.c_int, []),
     "srg_tile_config": (C.c_int, [C.c_int, _ip, _ip, _ip, _ip, _ip]),
     "srg_forward_project_device": (C.c_int, [C.POINTER(BurstDesc), C.c_void_p, C.c_int64, C.c_void_p,
@@ -119,6 +120,12 @@ def default_options(form: int = FORM_SPLIT, tile_cfg: int = -1, device: int = -1
     o.tile_cfg = tile_cfg
     o.device = device
     return o
+
+
+def measure_fma_peak(fp64: bool) -> float:
+    v = C.c_double()
+    check(lib().srg_measure_fma_peak(1 if fp64 else 0, C.byref(v)))
+    return float(v.value)
 
 
 def tile_configs():

@@ -155,9 +155,13 @@ def _stream_ptr(stream) -> Optional[int]:
 
 
 def backproject(bursts: Sequence[DeviceBurst], form: int = FORM_SPLIT, tile_cfg: int = -1,
-                stream=None, sync: bool = True) -> None:
-    """Backproject device bursts into their `out` tensors (one launch)."""
-    arr = (BurstDesc * len(bursts))(*[db.desc() for db in bursts])
+                stream=None, sync: bool = True, coefs=None) -> None:
+    """Backproject device bursts into their `out` tensors (one launch).
+    coefs: optional per-burst device tensors of azimuth-centre parabolas
+    ([nlines][3] float64, from ``line_centres``); without them the centres are
+    solved on the device first."""
+    ptrs = [c.data_ptr() for c in coefs] if coefs is not None else [0] * len(bursts)
+    arr = (BurstDesc * len(bursts))(*[db.desc(p) for db, p in zip(bursts, ptrs)])
     o = default_options(form, tile_cfg)
     st = _stream_ptr(stream)
     check(lib().srg_bp_bursts_device(arr, len(bursts), C.byref(o), C.c_void_p(st)))
@@ -172,13 +176,16 @@ def count_terms(bursts: Sequence[DeviceBurst], stream=None) -> int:
     return int(n.value)
 
 
-def line_centres(db: DeviceBurst, stream=None):
+def line_centres(db: DeviceBurst, stream=None, out=None, sync: bool = True):
+    """Per-line azimuth-centre parabolas of a device burst ([nlines][3] float64)."""
     import torch
-    coef = torch.zeros((db.nlines, 3), dtype=torch.float64, device=db.out.device)
+    coef = out if out is not None else torch.zeros((db.nlines, 3), dtype=torch.float64,
+                                                   device=db.out.device)
     d = db.desc()
     st = _stream_ptr(stream)
     check(lib().srg_line_centres_device(C.byref(d), C.c_void_p(coef.data_ptr()), C.c_void_p(st)))
-    check(lib().srg_sync_check(C.c_void_p(st)))
+    if sync:
+        check(lib().srg_sync_check(C.c_void_p(st)))
     return coef
 
 

@@ -503,6 +503,37 @@ int srg_forward_project_device(const srg_burst_desc *b, const float *refl, int64
     return SRG_OK;
 }
 
+int srg_measure_fma_peak(int fp64, double *tflops) {
+    if (!tflops) return fail(SRG_E_ARG, "null output");
+    DevCtx *c = nullptr;
+    int rc = get_ctx(-1, &c);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> g(c->mu);
+    rc = c->orbit.ensure(sizeof(double) * 64 * 1024);
+    if (rc) return rc;
+    const int blocks = c->sms * 8;   // 8 x 256 threads = full occupancy
+    const int iters = fp64 ? 4096 : 8192;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(launch_fma_peak(fp64, blocks, iters, c->orbit.p, 0));  // warm-up
+    float best = 1e30f;
+    for (int r = 0; r < 5; ++r) {
+        CK(cudaEventRecord(e0, 0));
+        CK(launch_fma_peak(fp64, blocks, iters, c->orbit.p, 0));
+        CK(cudaEventRecord(e1, 0));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        best = std::min(best, ms);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const double flops = 2.0 * 8.0 * (double)iters * 256.0 * (double)blocks;
+    *tflops = flops / (best * 1e-3) / 1e12;
+    return SRG_OK;
+}
+
 int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawdatalines,
                          int samplesPerBurst, int demwidth, int demlength, int fdout, int fddem,
                          double deltalat, double deltalon, double firstlat, double firstlon,

@@ -154,6 +154,33 @@ __global__ void forward_project_kernel(BurstDev B, const float2 *refl, long long
 }
 
 // ---------------------------------------------------------------------------
+// Calibration: FMA issue-rate peak.  Every thread runs 8 independent FMA
+// chains (enough to cover the pipeline latency at full occupancy); the
+// result is written so the work cannot be elided.
+template <typename T>
+__global__ void __launch_bounds__(256) fma_peak_kernel(T *sink, int iters, T a, T b) {
+    T x[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) x[i] = (T)(threadIdx.x + i);
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) x[i] = fma(x[i], a, b);
+    }
+    T s = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) s += x[i];
+    if (s == (T)12345.678) sink[blockIdx.x] = s;
+}
+
+cudaError_t launch_fma_peak(int fp64, int blocks, int iters, void *sink, cudaStream_t st) {
+    if (fp64)
+        fma_peak_kernel<double><<<blocks, 256, 0, st>>>((double *)sink, iters, 0.999999, 1e-7);
+    else
+        fma_peak_kernel<float><<<blocks, 256, 0, st>>>((float *)sink, iters, 0.999999f, 1e-7f);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // Compiled shapes of the tiled kernel.  {form, tile_x, tile_y, threads,
 // chunk, window}.
 #define SRG_SHAPES(X)                  \

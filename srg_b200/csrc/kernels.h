@@ -36,6 +36,8 @@ cudaError_t launch_pulse_orbit(const double *times, int P, const Orbit &o, doubl
 cudaError_t launch_forward_project(const BurstDev &B, const float2 *refl, long long refl_ld,
                                    const double *satvel, double antenna, cudaStream_t st);
 
+cudaError_t launch_fma_peak(int fp64, int blocks, int iters, void *sink, cudaStream_t st);
+
 inline int shared_bytes(const KernelEntry &e) {
     return e.params_bytes + 1024 + e.shape.chunk * e.shape.window * 8;
 }

@@ -429,21 +429,54 @@ def config0_point_targets(seed: int = 1000, pulses: int = 1024, samples: int = 4
                           width: int = 256, length: int = 256, spacing: float = 0.0002,
                           ntargets: int = 64, height: float = 500.0, snr_db: float = 10.0,
                           quantise: bool = True) -> Burst:
-    """64 point targets on flat 500 m terrain, 10 dB SNR (configuration 0)."""
+    """64 point targets on flat 500 m terrain, 10 dB SNR (configuration 0).
+    Targets sit on pixel centres whose aperture centre is well inside the
+    burst, so that every one of them is formed."""
     rng = np.random.default_rng(seed)
     b = make_geometry(pulses=pulses, samples=samples, width=width, length=length,
                       spacing=spacing, centre_height=height, quantise=quantise)
     b.dem = np.full((length, width), int(height), np.int16)
-    band = formed_line_band(b)
-    lo, hi = band
-    lines = rng.integers(lo + 2, max(lo + 3, hi - 2), ntargets)
-    pixels = rng.integers(8, width - 8, ntargets)
+    ok = formed_mask_estimate(b, margin=24)
+    ok[:, :8] = False
+    ok[:, -8:] = False
+    ok[:8] = False
+    ok[-8:] = False
+    cand = np.argwhere(ok)
+    order = rng.permutation(len(cand))
+    chosen = []
+    for i in order:  # keep targets at least 6 pixels apart so each peak is its own
+        y, x = cand[i]
+        if all(max(abs(y - cy), abs(x - cx)) >= 6 for cy, cx in chosen):
+            chosen.append((y, x))
+            if len(chosen) == ntargets:
+                break
+    pick = np.array(chosen)
+    lines, pixels = pick[:, 0], pick[:, 1]
     amps = np.ones(ntargets)
     pos = grid_ecef(b, lines, pixels, np.full(ntargets, height))
     add_point_targets(b, pos, amps)
     add_noise(b, rng, snr_db)
     b.targets = np.stack([lines, pixels, amps], -1)
     return b
+
+
+def formed_mask_estimate(b: Burst, margin: int = 0):
+    """Pixels whose nearest-approach pulse lies inside
+    (aperture/2 + margin, P - aperture/2 - margin): an estimate of the formed
+    region used to place synthetic targets (the exact one is the backprojector's)."""
+    P = b.rawdatalines
+    h = 0.0 if b.dem is None else b.dem.astype(np.float64)
+    ll, pp = np.mgrid[0:b.demlength, 0:b.demwidth]
+    pts = grid_ecef(b, ll, pp, np.broadcast_to(h, ll.shape)).reshape(-1, 3)
+    sub = b.satloc[::4]
+    vel = b.satvel[::4]
+    best = np.empty(len(pts), np.int64)
+    for i0 in range(0, len(pts), 8192):
+        d = pts[i0:i0 + 8192, None, :] - sub[None]
+        dop = np.abs(np.sum(d * vel[None], axis=-1))
+        best[i0:i0 + 8192] = np.argmin(dop, axis=1) * 4
+    lo, hi = b.aperture // 2 + margin, P - b.aperture // 2 - margin
+    return ((best > lo) & (best < hi)).reshape(b.demlength, b.demwidth)
 
 
 def formed_line_band(b: Burst):

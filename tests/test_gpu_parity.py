@@ -184,6 +184,7 @@ def test_config0_point_targets(torch_cuda, orc):
     fl = st["firstline"]
     for line, pix, _ in b.targets.astype(int):
         li = line - fl
+        assert st["azoff"][li, pix] > 0
         win = np.abs(spl[li - 2:li + 3, pix - 2:pix + 3])
         assert np.unravel_index(np.argmax(win), win.shape) == (2, 2)
         assert abs(np.angle(spl[li, pix])) < 0.1
