@@ -155,6 +155,35 @@ int srg_pulse_orbit_device(const double *times, int P, const double *timeorbit,
  * library's kernels since the last check (SRG_E_TIMEOUT) or CUDA error. */
 int srg_sync_check(void *stream);
 
+/* ------------------------------------------------------------------------
+ * No-allocation variant of srg_bp_bursts_device for one burst.  It has no
+ * counterpart in the reference (whose entry allocates and frees device memory
+ * on every burst).
+ *
+ * For callers that cannot call cudaMalloc: a process whose device memory is
+ * already reserved by a pool it does not own (a serving runtime or a
+ * framework allocator holding the HBM), or a latency-critical stream that
+ * cannot take the device-wide synchronisation of cudaMalloc/cudaFree.  The
+ * caller passes the inputs and the output (as for srg_bp_bursts_device);
+ * the work counter, error word, burst and TMA descriptors, orbit state
+ * vectors and per-line azimuth-centre parabolas live in one static device
+ * array of SRG_NOALLOC_SCRATCH_BYTES that every GPU loading this library
+ * holds until the process exits.  Limits: at most SRG_NOALLOC_MAX_LINES grid
+ * lines, and at most SRG_NOALLOC_MAX_STATEVEC state vectors when b->coef is
+ * NULL; larger bursts are rejected with SRG_E_ARG before any GPU work.
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress): make that first call before any stream capture.
+ * Every call shares the array and clears only the counter and the error word;
+ * calls whose GPU work overlaps (other streams, other host threads) race.
+ * Blocking: returns once the work on `stream` has finished, with
+ * SRG_E_TIMEOUT if a device-side wait gave up.
+ * ------------------------------------------------------------------------ */
+#define SRG_NOALLOC_MAX_LINES    8192
+#define SRG_NOALLOC_MAX_STATEVEC 64
+#define SRG_NOALLOC_SCRATCH_BYTES (2048 + 7 * 8 * SRG_NOALLOC_MAX_STATEVEC + 3 * 8 * SRG_NOALLOC_MAX_LINES)
+int srg_bp_burst_device_noalloc(const srg_burst_desc *b, const srg_bp_options *opts,
+                                void *stream);
+
 /* Calibration: measured FMA issue-rate peak of the current device in
  * TFLOP/s (2 flops per FMA), FP32 (fp64 = 0) or FP64 (fp64 = 1), from a
  * full-occupancy chain-of-FMA kernel timed with CUDA events.  Blocking. */

@@ -73,6 +73,7 @@ _SIGS = {
                                          C.c_void_p, C.c_void_p]),
     "srg_sync_check": (C.c_int, [C.c_void_p]),
     "srg_measure_fma_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
+    "srg_bp_burst_device_noalloc": (C.c_int, [C.POINTER(BurstDesc), C.POINTER(Options), C.c_void_p]),
     "srg_tile_config_count": (C.c_int, []),
     "srg_tile_config": (C.c_int, [C.c_int, _ip, _ip, _ip, _ip, _ip]),
     "srg_forward_project_device": (C.c_int, [C.POINTER(BurstDesc), C.c_void_p, C.c_int64, C.c_void_p,

@@ -8,8 +8,8 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsrg_bp.so")
-SOURCES = ["capi.cu", "kernels.cu"]
-HEADERS = ["bp_kernel.cuh", "common.cuh", "geom.cuh", "ptx.cuh", "kernels.h"]
+SOURCES = ["capi.cu", "kernels.cu", "noalloc.cu"]
+HEADERS = ["bp_kernel.cuh", "common.cuh", "geom.cuh", "ptx.cuh", "kernels.h", "host_internal.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -24,11 +24,13 @@
 #include <vector>
 
 #include "../../include/srg_bp.h"
+#include "host_internal.h"
 #include "kernels.h"
 
 using namespace srg;
 
-namespace {
+namespace srg {
+namespace detail {
 
 thread_local std::string g_err;
 
@@ -51,40 +53,6 @@ int fail(int code, const char *fmt, ...) {
 
 srg_bp_options g_default_opts = {SRG_FORM_SPLIT, -1, -1, 0, 0};
 std::mutex g_opts_mu;
-
-// Grow-only device buffer.
-struct DevBuf {
-    void *p = nullptr;
-    size_t cap = 0;
-    int ensure(size_t bytes) {
-        if (bytes <= cap) return SRG_OK;
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
-        size_t want = std::max(bytes, (size_t)256);
-        cudaError_t e = cudaMalloc(&p, want);
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            return fail(SRG_E_NOMEM, "cudaMalloc(%zu) failed: %s", want, cudaGetErrorString(e));
-        }
-        cap = want;
-        return SRG_OK;
-    }
-};
-
-// Per-device scratch, reused by every call on that device.
-struct DevCtx {
-    int dev = -1;
-    int sms = 0;
-    std::mutex mu;
-    DevBuf flags;     // [0] work counter, [1] error word, [2..3] term counter (u64)
-    DevBuf bursts;    // BurstDev[]
-    DevBuf tmaps;     // CUtensorMap[]
-    DevBuf coef;      // doubles
-    DevBuf orbit;     // state vectors
-    DevBuf in_burst, in_sat, in_dem, out;  // drop-in staging
-    bool attrs_done[64] = {};
-};
 
 DevCtx g_ctx[64];
 std::mutex g_ctx_mu;
@@ -264,6 +232,13 @@ void ensure_attrs(DevCtx &c, int idx) {
 }
 
 int kernel_index(const KernelEntry *e) { return (int)(e - kKernels); }
+
+}  // namespace detail
+}  // namespace srg
+
+using namespace srg::detail;
+
+namespace {
 
 // Core: launch the tiled kernel over n prepared bursts.
 int run_bursts(DevCtx &c, const srg_burst_desc *descs, int n, const srg_bp_options &o,

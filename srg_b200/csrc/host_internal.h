@@ -1,0 +1,67 @@
+// host_internal.h -- host-side helpers shared by the C-ABI translation units
+// of libsrg_bp.so (capi.cu, noalloc.cu).  Not part of the public ABI.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <mutex>
+#include <string>
+
+#include "../../include/srg_bp.h"
+#include "kernels.h"
+
+namespace srg {
+namespace detail {
+
+// Record a one-line error message for srg_last_error() and return `code`.
+int fail(int code, const char *fmt, ...);
+
+// Grow-only device buffer.
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    int ensure(size_t bytes) {
+        if (bytes <= cap) return SRG_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = std::max(bytes, (size_t)256);
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(SRG_E_NOMEM, "cudaMalloc(%zu) failed: %s", want, cudaGetErrorString(e));
+        }
+        cap = want;
+        return SRG_OK;
+    }
+};
+
+// Per-device scratch, reused by every call on that device.
+struct DevCtx {
+    int dev = -1;
+    int sms = 0;
+    std::mutex mu;
+    DevBuf flags;     // [0] work counter, [1] error word, [2..3] term counter (u64)
+    DevBuf bursts;    // BurstDev[]
+    DevBuf tmaps;     // CUtensorMap[]
+    DevBuf coef;      // doubles
+    DevBuf orbit;     // state vectors
+    DevBuf in_burst, in_sat, in_dem, out;  // drop-in staging
+    bool attrs_done[64] = {};
+};
+
+// Per-device context (sets the device current).
+int get_ctx(int device, DevCtx **out);
+// Kernel entry for a form and shape index (-1: the default of that form).
+const KernelEntry *pick_kernel(int form, int cfg);
+int kernel_index(const KernelEntry *e);
+void ensure_attrs(DevCtx &c, int idx);
+int validate_desc(const srg_burst_desc &d);
+BurstDev make_burst_dev(const srg_burst_desc &d, const double *coef);
+// 0 and *out filled when a TMA descriptor can describe the burst, else -1.
+int make_tmap(const BurstDev &B, int box_x, int box_y, CUtensorMap *out);
+double ref_pi();
+
+}  // namespace detail
+}  // namespace srg
