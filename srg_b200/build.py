@@ -9,7 +9,6 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsrg_bp.so")
 SOURCES = ["capi.cu", "kernels.cu", "noalloc.cu"]
-HEADERS = ["bp_kernel.cuh", "common.cuh", "geom.cuh", "ptx.cuh", "kernels.h", "host_internal.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -24,7 +23,7 @@ def _stale() -> bool:
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)]
     deps.append(os.path.join(HERE, "..", "include", "srg_bp.h"))
     return any(os.path.getmtime(p) > t for p in deps if os.path.exists(p))
 

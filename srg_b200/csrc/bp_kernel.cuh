@@ -71,9 +71,11 @@ __device__ __forceinline__ void two_prod(float a, float b, float &p, float &e) {
 }
 
 // frac(K * (d . u)) with d = dh + dl, u = uh + ul, K = Kh + Kl, all float,
-// in double-float arithmetic; |result| <= ~0.5.
+// in double-float arithmetic; |result| <= ~0.5.  The dot product d . u is
+// returned as the unevaluated sum whi + wlo.
 __device__ __forceinline__ float seed_phase(const float dh[3], const float dl[3], const float uh[3],
-                                            const float ul[3], float Kh, float Kl) {
+                                            const float ul[3], float Kh, float Kl, float *whi,
+                                            float *wlo) {
     float p0, e0, p1, e1, p2, e2;
     two_prod(dh[0], uh[0], p0, e0);
     two_prod(dh[1], uh[1], p1, e1);
@@ -88,6 +90,10 @@ __device__ __forceinline__ float seed_phase(const float dh[3], const float dl[3]
     lo = fmaf(dl[0], uh[0], lo);
     lo = fmaf(dl[1], uh[1], lo);
     lo = fmaf(dl[2], uh[2], lo);
+    if (whi) {
+        *whi = s2;
+        *wlo = lo;
+    }
     // (s2 + lo) * (Kh + Kl)
     float P, E;
     two_prod(s2, Kh, P, E);
@@ -298,7 +304,7 @@ bp_tiles(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                     d[m][q] = dh[q];
                 }
                 dd[m] = fmaf(dh[0], dh[0], fmaf(dh[1], dh[1], dh[2] * dh[2]));
-                c[m] = seed_phase(dh, dl, ctl.seed_hi, ctl.seed_lo, B.K_hi, B.K_lo);
+                c[m] = seed_phase(dh, dl, ctl.seed_hi, ctl.seed_lo, B.K_hi, B.K_lo, nullptr, nullptr);
             }
         }
         __syncthreads();

@@ -1,0 +1,634 @@
+// bp_ws.cuh -- warp-specialised tiled backprojection (sm_100a).
+//
+// Same sum, work decomposition and arithmetic forms as bp_kernel.cuh (read
+// that header first); this variant reorganises the pulse loop:
+//
+// * One producer warp per CTA prepares chunk c+1.. while NC consumer warps
+//   work on chunk c: it derives the per-pulse quantities in FP64, picks the
+//   chunk's range-bin window and issues the TMA load of CK pulse rows x WB
+//   bins into an NS-deep ring of shared-memory stages.  Full/empty mbarriers
+//   (bounded waits) replace CTA-wide barriers inside a tile.
+// * Chunks lying inside every formed pixel's aperture window and inside the
+//   range window ("interior" chunks, the common case) run without per-term
+//   predicates.  The producer proves, per chunk, that no term can leave the
+//   staged window: a pixel's bin offset from the tile centre is linear in
+//   the look direction u_k, so between the tile's first and last pulse it
+//   deviates from the straight line through its end values (which the
+//   window covers with a one-bin margin) by at most
+//   max|d| * max_k |u_k - u_lin(k)| / dmrg; the chunk is marked interior
+//   only when that bound is below half a bin (a smooth orbit gives ~1e-4).
+//   The taps' index is still clamped for memory safety.  Edge chunks use the
+//   general path (per-term aperture and range tests, global-memory fallback
+//   for taps outside the window).
+// * Split form: the per-term state is w = d.u_k, held as the unevaluated sum
+//   of a per-tile constant whi and a small accumulator dwa (|dwa| < ~1 m, so
+//   its rounding stays below 1e-6 m over a whole aperture), and the phase
+//   c = 2 pi frac(K d.u_k) in radians; whi + dwa and c are seeded once per
+//   pixel and tile in compensated arithmetic and both advance by the same
+//   increment dw = d.(u_{k+1} - u_k), exact to FP32 relative precision
+//   because |dw| <~ 1e-3 m.  The second-order range term
+//   dr2 = (|d|^2 - w^2) (1/(2 R_c) - w/(2 R_c^2)) changes by < 1e-5 m over a
+//   chunk and is linear in the pulse index to ~1e-9 m, so it is evaluated
+//   exactly once per pixel and chunk, with its slope g = (d dr2 / dw) * dw_mid,
+//   and folded into the two accumulators, which then advance by dw + g: per
+//   term only the increment, two accumulations, the bin and the phase remain.
+#pragma once
+#include <climits>
+#include <cuda.h>
+#include "bp_kernel.cuh"
+
+namespace srg {
+
+struct StageHdr {
+    int x0;        // first staged bin
+    int fast;      // 1: interior chunk (no per-term predicates)
+    float tlo, thi;       // range test in window-relative bins (general path)
+    float dmx, dmy, dmz;  // u_{k+1} - u_k at the chunk's middle pulse
+    float inv2R, c2;      // 1/(2 R_c) and 1/(2 R_c^2) at the chunk's middle pulse
+    int pad[3];
+};
+
+struct CtlWS {
+    uint64_t full[4], empty[4];
+    int item, kmin, kmax, azs_max, aze_min, bmin, bmax, abort;
+    int dmax_bits;        // max |d| over formed pixels (non-negative float bits)
+    double xc[3];
+    double rc0, rc1;
+    double ua[3], ub[3];  // unit look vectors at kmin and kmax-1
+    float seed_hi[3], seed_lo[3];
+};
+
+constexpr double kTwoPi = 6.283185307179586476925;
+constexpr float kTwoPiHi = 6.28318548202514648f;     // float(2 pi)
+constexpr float kTwoPiLo = -1.74845553e-7f;          // 2 pi - float(2 pi)
+constexpr float kInvTwoPi = 0.159154943091895336f;
+
+// Per-pulse parameters of one chunk (split: 2 x float4; FP64: satloc + pad).
+template <int FORM>
+struct PulseParams;
+template <>
+struct PulseParams<FORM_SPLIT> {
+    float4 a;  // du (= u_{k+1} - u_k) x, y, z; ref phase (rad)
+    float4 b;  // rb (window-relative bin of R_c), unused x3
+};
+template <>
+struct PulseParams<FORM_FP64> {
+    double s[4];  // satloc x, y, z, unused
+};
+
+template <int FORM, int CK>
+__host__ __device__ constexpr int ws_params_bytes() {
+    return (int)sizeof(PulseParams<FORM>) * CK;
+}
+
+// Dynamic shared memory of a shape: params of every stage, then the sample
+// windows from the first 1024-byte boundary.
+template <int FORM, int CK, int NS>
+__host__ __device__ constexpr int ws_smem_bytes(int WB) {
+    return NS * ws_params_bytes<FORM, CK>() + 1024 + NS * CK * WB * 8;
+}
+
+// Chunk schedule of a tile: the pulse range [kmin, kmax) is cut at ka and kb
+// (the interior segment [ka, kb) lies inside every formed pixel's aperture)
+// and each of the three segments into chunks of at most CK pulses, so that
+// only the edge segments need the general path.
+struct ChunkPlan {
+    int kmin, ka, kb, kmax, na, nb, nc;
+    __device__ __forceinline__ void init(int k0, int k1, int smax, int emin, int CK) {
+        kmin = k0;
+        kmax = k1;
+        ka = max(k0, min(smax, k1));
+        kb = max(ka, min(emin, k1));
+        na = (ka - k0 + CK - 1) / CK;
+        nb = (kb - ka + CK - 1) / CK;
+        nc = (k1 - kb + CK - 1) / CK;
+    }
+    __device__ __forceinline__ int count() const { return na + nb + nc; }
+    // first pulse and length of chunk c
+    __device__ __forceinline__ void chunk(int c, int CK, int &k0, int &nk) const {
+        if (c < na) {
+            k0 = kmin + c * CK;
+            nk = min(CK, ka - k0);
+        } else if (c < na + nb) {
+            k0 = ka + (c - na) * CK;
+            nk = min(CK, kb - k0);
+        } else {
+            k0 = kb + (c - na - nb) * CK;
+            nk = min(CK, kmax - k0);
+        }
+    }
+};
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// MINB: blocks per SM the register allocation is sized for.
+template <int FORM, int TX, int TY, int NC, int CK, int NS, int MINB>
+__global__ void __launch_bounds__((NC + 1) * 32, MINB)
+bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
+      const CUtensorMap *__restrict__ tmaps, int *__restrict__ work_counter,
+      int *__restrict__ err, int WB) {
+    constexpr int NCT = NC * 32;
+    constexpr int M = TX * TY / NCT;
+    constexpr int BX = TX / 8;  // 8 x 4 pixel blocks, one per warp and slot
+    static_assert(TX % 8 == 0 && TY % 4 == 0 && (TX / 8) * (TY / 4) == NC * M, "tile / warp map");
+    static_assert(CK < 32, "the producer warp covers CK + 1 pulses");
+    static_assert(NS >= 2 && NS <= 4, "stage ring");
+    using PP = PulseParams<FORM>;
+
+    extern __shared__ __align__(128) unsigned char dsm[];
+    __shared__ CtlWS ctl;
+    __shared__ StageHdr hdr[NS];
+    PP *prm = reinterpret_cast<PP *>(dsm);
+    float2 *samp0;
+    {
+        const uint32_t off = smem_u32(dsm + NS * ws_params_bytes<FORM, CK>());
+        samp0 = reinterpret_cast<float2 *>(dsm + NS * ws_params_bytes<FORM, CK>() +
+                                           ((1024 - (off & 1023)) & 1023));
+    }
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const bool producer = warp == NC;
+
+    if (tid == 0) {
+        for (int s = 0; s < NS; ++s) {
+            mbar_init(&ctl.full[s], 32);
+            mbar_init(&ctl.empty[s], NC);
+        }
+        fence_barrier_init();
+        ctl.abort = 0;
+    }
+    __syncthreads();
+    uint32_t gchunk = 0;  // chunks issued/consumed by this CTA so far (uniform)
+    uint32_t issued = 0, issued_par = 0;  // producer lane 0: stages with a TMA issued this tile
+
+    for (;;) {
+        if (tid == 0) ctl.item = atomicAdd(work_counter, 1);
+        __syncthreads();
+        const int item = ctl.item;
+        if (item >= total_tiles) break;
+        int b = 0;
+        while (b + 1 < nbursts && bursts[b + 1].tile_base <= item) ++b;
+        const BurstDev &B = bursts[b];
+        const int ti = item - B.tile_base;
+        const int px0 = B.firstpix + (ti % B.tiles_x) * TX;
+        const int ly0 = (ti / B.tiles_x) * TY;
+
+        // ---- prologue (all threads) ----
+        if (tid == 0) {
+            ctl.kmin = INT_MAX;
+            ctl.kmax = INT_MIN;
+            ctl.azs_max = INT_MIN;
+            ctl.aze_min = INT_MAX;
+            ctl.bmin = INT_MAX;
+            ctl.bmax = INT_MIN;
+            ctl.dmax_bits = 0;
+        }
+        __syncthreads();
+        double X[M][3];
+        int azs[M], aze[M];
+        if (!producer) {
+            int k0 = INT_MAX, k1 = INT_MIN, smax = INT_MIN, emin = INT_MAX;
+#pragma unroll
+            for (int m = 0; m < M; ++m) {
+                const int bi = warp + NC * m;
+                const int x = 8 * (bi % BX) + (lane & 7), y = 4 * (bi / BX) + (lane >> 3);
+                const int px = px0 + x, line = ly0 + y;
+                X[m][0] = X[m][1] = X[m][2] = 0.0;
+                azs[m] = aze[m] = 0;
+                if (px <= B.lastpix_eff && line < B.nlines) {
+                    const double h = (double)B.dem[(long long)line * B.dem_ld + px];
+                    pixel_ecef(B, line, px, h, X[m][0], X[m][1], X[m][2]);
+                    pixel_window(B, pixel_azoff(B, B.coef + 3 * line, px), azs[m], aze[m]);
+                    if (aze[m] > azs[m]) {
+                        k0 = min(k0, azs[m]);
+                        k1 = max(k1, aze[m]);
+                        smax = max(smax, azs[m]);
+                        emin = min(emin, aze[m]);
+                    }
+                }
+            }
+            k0 = warp_min(k0);
+            k1 = warp_max(k1);
+            smax = warp_max(smax);
+            emin = warp_min(emin);
+            if (lane == 0 && k0 < k1) {
+                atomicMin(&ctl.kmin, k0);
+                atomicMax(&ctl.kmax, k1);
+                atomicMax(&ctl.azs_max, smax);
+                atomicMin(&ctl.aze_min, emin);
+            }
+        }
+        __syncthreads();
+        const int kmin = ctl.kmin, kmax = ctl.kmax;
+        if (kmin >= kmax) {
+            if (!producer) {
+#pragma unroll
+                for (int m = 0; m < M; ++m) {
+                    const int bi = warp + NC * m;
+                    const int x = 8 * (bi % BX) + (lane & 7), y = 4 * (bi / BX) + (lane >> 3);
+                    const int px = px0 + x, line = ly0 + y;
+                    if (px <= B.lastpix_eff && line < B.nlines)
+                        B.out[(long long)line * B.out_ld + (px - B.out_pix0)] = make_float2(0.f, 0.f);
+                }
+            }
+            __syncthreads();
+            continue;
+        }
+        if (tid == 0) {
+            const int cx = min(max(px0 + TX / 2, B.firstpix), B.lastpix_eff);
+            const int cy = min(ly0 + TY / 2, B.nlines - 1);
+            double xc[3];
+            pixel_ecef(B, cy, cx, (double)B.dem[(long long)cy * B.dem_ld + cx], xc[0], xc[1], xc[2]);
+            ctl.xc[0] = xc[0];
+            ctl.xc[1] = xc[1];
+            ctl.xc[2] = xc[2];
+            const double *s0 = B.satloc + 3 * kmin;
+            const double *s1 = B.satloc + 3 * (kmax - 1);
+            const double u0 = xc[0] - s0[0], u1 = xc[1] - s0[1], u2 = xc[2] - s0[2];
+            const double r0 = sqrt(u0 * u0 + u1 * u1 + u2 * u2);
+            const double v0 = xc[0] - s1[0], v1 = xc[1] - s1[1], v2 = xc[2] - s1[2];
+            ctl.rc0 = r0;
+            ctl.rc1 = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+            const double uu[3] = {u0 / r0, u1 / r0, u2 / r0};
+            ctl.ua[0] = uu[0];
+            ctl.ua[1] = uu[1];
+            ctl.ua[2] = uu[2];
+            ctl.ub[0] = v0 / ctl.rc1;
+            ctl.ub[1] = v1 / ctl.rc1;
+            ctl.ub[2] = v2 / ctl.rc1;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const float hi = __double2float_rn(uu[c]);
+                ctl.seed_hi[c] = hi;
+                ctl.seed_lo[c] = __double2float_rn(uu[c] - (double)hi);
+            }
+        }
+        __syncthreads();
+        float d[M][3], dd[M], cph[M], whi[M], dwa[M], accr[M], acci[M];
+        double accr_d[M], acci_d[M];
+        if (!producer) {
+            int lb0 = INT_MAX, lb1 = INT_MIN;
+            float dmx = 0.f;
+            const double *s0 = B.satloc + 3 * kmin;
+            const double *s1 = B.satloc + 3 * (kmax - 1);
+#pragma unroll
+            for (int m = 0; m < M; ++m) {
+                accr[m] = acci[m] = 0.f;
+                accr_d[m] = acci_d[m] = 0.0;
+                d[m][0] = d[m][1] = d[m][2] = 0.f;
+                dd[m] = cph[m] = whi[m] = dwa[m] = 0.f;
+                if (aze[m] > azs[m]) {
+                    const double a0 = X[m][0] - s0[0], a1 = X[m][1] - s0[1], a2 = X[m][2] - s0[2];
+                    const double c0 = X[m][0] - s1[0], c1 = X[m][1] - s1[1], c2 = X[m][2] - s1[2];
+                    const double e0 = (sqrt(a0 * a0 + a1 * a1 + a2 * a2) - ctl.rc0) * B.inv_dmrg;
+                    const double e1 = (sqrt(c0 * c0 + c1 * c1 + c2 * c2) - ctl.rc1) * B.inv_dmrg;
+                    lb0 = min(lb0, (int)floor(fmin(e0, e1)));
+                    lb1 = max(lb1, (int)ceil(fmax(e0, e1)));
+                    const double q0 = X[m][0] - ctl.xc[0], q1 = X[m][1] - ctl.xc[1],
+                                 q2 = X[m][2] - ctl.xc[2];
+                    dmx = fmaxf(dmx, (float)sqrt(q0 * q0 + q1 * q1 + q2 * q2) * 1.0001f);
+                    if (FORM == FORM_SPLIT) {
+                        float dh[3], dl[3];
+#pragma unroll
+                        for (int q = 0; q < 3; ++q) {
+                            const double dv = X[m][q] - ctl.xc[q];
+                            dh[q] = __double2float_rn(dv);
+                            dl[q] = __double2float_rn(dv - (double)dh[q]);
+                            d[m][q] = dh[q];
+                        }
+                        dd[m] = fmaf(dh[0], dh[0], fmaf(dh[1], dh[1], dh[2] * dh[2]));
+                        cph[m] = (float)kTwoPi * seed_phase(dh, dl, ctl.seed_hi, ctl.seed_lo, B.K_hi,
+                                                            B.K_lo, &whi[m], &dwa[m]);
+                    }
+                }
+            }
+            lb0 = warp_min(lb0);
+            lb1 = warp_max(lb1);
+            const int dbits = __reduce_max_sync(0xffffffffu, __float_as_int(dmx));
+            if (lane == 0 && lb0 <= lb1) {
+                atomicMin(&ctl.bmin, lb0);
+                atomicMax(&ctl.bmax, lb1);
+                atomicMax(&ctl.dmax_bits, dbits);
+            }
+        }
+        __syncthreads();
+        ChunkPlan plan;
+        plan.init(kmin, kmax, ctl.azs_max, ctl.aze_min, CK);
+        const int nchunks = plan.count();
+        const bool use_tma = B.tmap >= 0;
+
+        issued = 0;
+        if (producer) {
+            // ---- producer warp ----
+            const int bmin = ctl.bmin - 1, bmax = ctl.bmax + 2;
+            const double xcx = ctl.xc[0], xcy = ctl.xc[1], xcz = ctl.xc[2];
+            const int azs_max = ctl.azs_max, aze_min = ctl.aze_min;
+            const double rmaxb = (B.rmax - B.rngstart) * B.inv_dmrg;
+            const double uax = ctl.ua[0], uay = ctl.ua[1], uaz = ctl.ua[2];
+            const double dux = ctl.ub[0] - uax, duy = ctl.ub[1] - uay, duz = ctl.ub[2] - uaz;
+            const double span = kmax - 1 > kmin ? 1.0 / (double)(kmax - 1 - kmin) : 0.0;
+            const double dev_scale = (double)__int_as_float(ctl.dmax_bits) * B.inv_dmrg;
+            const double *satl = B.satloc;
+            const int Pm1 = B.P - 1;
+            // satellite position of this lane's pulse, one chunk ahead
+            double nsx, nsy, nsz;
+            {
+                int k0n, nkn;
+                plan.chunk(0, CK, k0n, nkn);
+                const double *sp = satl + 3 * min(k0n + lane, Pm1);
+                nsx = sp[0];
+                nsy = sp[1];
+                nsz = sp[2];
+            }
+            for (int c = 0; c < nchunks; ++c) {
+                const uint32_t g = gchunk + c;
+                const int s = g % NS;
+                const uint32_t r = g / NS;
+                int k0, nk;
+                plan.chunk(c, CK, k0, nk);
+                const int k = min(k0 + lane, Pm1);
+                const double sx = nsx, sy = nsy, sz = nsz;
+                if (c + 1 < nchunks) {  // prefetch the next chunk's orbit
+                    int k0n, nkn;
+                    plan.chunk(c + 1, CK, k0n, nkn);
+                    const double *sp = satl + 3 * min(k0n + lane, Pm1);
+                    nsx = sp[0];
+                    nsy = sp[1];
+                    nsz = sp[2];
+                }
+                const double ux = xcx - sx, uy = xcy - sy, uz = xcz - sz;
+                const double uu = ux * ux + uy * uy + uz * uz;
+                const double rs = rsqrt(uu);
+                const double R = uu * rs;
+                const double ex = ux * rs, ey = uy * rs, ez = uz * rs;
+                const double nx = __shfl_down_sync(0xffffffffu, ex, 1);
+                const double ny = __shfl_down_sync(0xffffffffu, ey, 1);
+                const double nz = __shfl_down_sync(0xffffffffu, ez, 1);
+                const double rbabs = (R - B.rngstart) * B.inv_dmrg;
+                const bool act = lane < nk;
+                // deviation of the look vector from the tile's straight line
+                const double f = (double)(k - kmin) * span;
+                const double gx = ex - (uax + f * dux), gy = ey - (uay + f * duy),
+                             gz = ez - (uaz + f * duz);
+                const float dev = act ? (float)(sqrt(gx * gx + gy * gy + gz * gz) * dev_scale) : 0.f;
+                const int lo = __reduce_min_sync(0xffffffffu, act ? (int)floor(rbabs) : INT_MAX);
+                const int hi = __reduce_max_sync(0xffffffffu, act ? (int)ceil(rbabs) : INT_MIN);
+                const int devmax = __reduce_max_sync(0xffffffffu, __float_as_int(dev));
+                const int x0 = (lo + bmin) & ~1;  // TMA: x * 8 bytes on a 16-byte boundary
+                const int need = hi + bmax - x0 + 1;
+                const double Rmid = __shfl_sync(0xffffffffu, R, nk / 2);
+                const double mdx = __shfl_sync(0xffffffffu, nx - ex, nk / 2);
+                const double mdy = __shfl_sync(0xffffffffu, ny - ey, nk / 2);
+                const double mdz = __shfl_sync(0xffffffffu, nz - ez, nk / 2);
+                if (!mbar_wait_backoff(&ctl.empty[s], (r & 1) ^ 1)) {
+                    ctl.abort = 1;
+                    break;
+                }
+                if constexpr (FORM == FORM_FP64) {
+                    if (lane < CK) {
+                        double *q = prm[s * CK + lane].s;
+                        q[0] = sx;
+                        q[1] = sy;
+                        q[2] = sz;
+                    }
+                }
+                if constexpr (FORM == FORM_SPLIT) {
+                    if (lane < CK) {
+                        const double q = R * B.K;
+                        const double ref = kTwoPi * (q - rint(q));
+                        PP &p = prm[s * CK + lane];
+                        p.a = make_float4(__double2float_rn(nx - ex), __double2float_rn(ny - ey),
+                                          __double2float_rn(nz - ez), __double2float_rn(ref));
+                        p.b = make_float4(__double2float_rn(rbabs - (double)x0), 0.f, 0.f, 0.f);
+                    }
+                }
+                if (lane == 0) {
+                    StageHdr &h = hdr[s];
+                    h.x0 = x0;
+                    const bool interior = k0 >= azs_max && k0 + nk <= aze_min;
+                    const bool rangeok = x0 >= 1 && (double)(x0 + WB) <= rmaxb - 1.0;
+                    const bool bounded = __int_as_float(devmax) < 0.5f;
+                    h.fast = (interior && rangeok && bounded && need <= WB) ? 1 : 0;
+                    h.tlo = (float)(-(double)x0);
+                    h.thi = __double2float_rn(rmaxb - (double)x0);
+                    h.dmx = __double2float_rn(mdx);
+                    h.dmy = __double2float_rn(mdy);
+                    h.dmz = __double2float_rn(mdz);
+                    h.inv2R = __double2float_rn(0.5 / Rmid);
+                    h.c2 = __double2float_rn(0.5 / (Rmid * Rmid));
+                }
+                if (!use_tma) {
+                    // no TMA descriptor for this burst: stage the window with plain loads
+                    float2 *w = samp0 + (size_t)s * CK * WB;
+                    for (int idx = lane; idx < CK * WB; idx += 32) {
+                        const int j = idx / WB;
+                        w[idx] = ld_sample(B, k0 + j, x0 + (idx - j * WB));
+                    }
+                }
+                __syncwarp();
+                if (lane == 0 && use_tma) {
+                    if (c == 0) fence_tensormap_acquire(tmaps + B.tmap);
+                    fence_proxy_async_shared();
+                    mbar_arrive_expect_tx(&ctl.full[s], (uint32_t)(WB * CK * 8));
+                    tma_load_2d(samp0 + (size_t)s * CK * WB, tmaps + B.tmap, &ctl.full[s], x0, k0);
+                    issued |= 1u << s;
+                    issued_par = (issued_par & ~(1u << s)) | ((r & 1u) << s);
+                } else {
+                    mbar_arrive(&ctl.full[s]);
+                }
+            }
+        } else {
+            // ---- consumer warps ----
+            for (int c = 0; c < nchunks; ++c) {
+                const uint32_t g = gchunk + c;
+                const int s = g % NS;
+                const uint32_t r = g / NS;
+                if (!mbar_wait_bounded(&ctl.full[s], r & 1)) {
+                    ctl.abort = 1;
+                    break;
+                }
+                const StageHdr h = hdr[s];
+                int k0, nk;
+                plan.chunk(c, CK, k0, nk);
+                const float2 *win = samp0 + (size_t)s * CK * WB;
+                const PP *pp = prm + s * CK;
+                if constexpr (FORM == FORM_SPLIT) {
+                    const float invd = B.inv_dmrg_f;
+                    const float Kr = (float)(kTwoPi * B.K);
+                    // per pixel and chunk: second-order term and its slope, folded
+                    // into the accumulators (uacc = dwa + dr2, cphp = cph + Kr dr2)
+                    float uacc[M], cphp[M], gsl[M], dr0[M];
+#pragma unroll
+                    for (int m = 0; m < M; ++m) {
+                        const float w0 = whi[m] + dwa[m];
+                        const float n0 = fmaf(-w0, w0, dd[m]);
+                        const float q0 = fmaf(-w0, h.c2, h.inv2R);
+                        dr0[m] = n0 * q0;
+                        const float dwm = fmaf(d[m][0], h.dmx, fmaf(d[m][1], h.dmy, d[m][2] * h.dmz));
+                        gsl[m] = fmaf(-2.f * w0, q0, -n0 * h.c2) * dwm;
+                        uacc[m] = dwa[m] + dr0[m];
+                        cphp[m] = fmaf(dr0[m], Kr, cph[m]);
+                    }
+                    if (h.fast) {
+                        // consecutive pulses share only the two accumulators, so
+                        // unrolling gives the scheduler independent terms
+#pragma unroll 2
+                        for (int j = 0; j < nk; ++j) {
+                            const float4 pa = pp[j].a;
+                            const float rb = pp[j].b.x;
+                            const float2 *row = win + j * WB;
+#pragma unroll
+                            for (int m = 0; m < M; ++m) {
+                                const float dwp = fmaf(d[m][0], pa.x, fmaf(d[m][1], pa.y, fmaf(d[m][2], pa.z, gsl[m])));
+                                const float t = fmaf(whi[m] + uacc[m], invd, rb);
+                                const float ph = cphp[m] + pa.w;
+                                uacc[m] += dwp;
+                                cphp[m] = fmaf(dwp, Kr, cphp[m]);
+                                const float fl = floorf(t);
+                                const float fr = t - fl;
+                                // proven in range by the producer; clamped for memory safety
+                                const unsigned ic = min((unsigned)(int)fl, (unsigned)(WB - 2));
+                                const float2 s0 = row[ic], s1 = row[ic + 1];
+                                const float vr = fmaf(fr, s1.x - s0.x, s0.x);
+                                const float vi = fmaf(fr, s1.y - s0.y, s0.y);
+                                float sn, cs;
+                                __sincosf(ph, &sn, &cs);
+                                accr[m] = fmaf(vr, cs, fmaf(-vi, sn, accr[m]));
+                                acci[m] = fmaf(vr, sn, fmaf(vi, cs, acci[m]));
+                            }
+                        }
+                    } else {
+                        // general path: exact aperture and range tests, taps from
+                        // global memory when outside the staged window
+                        for (int j = 0; j < nk; ++j) {
+                            const int k = k0 + j;
+                            const float4 pa = pp[j].a;
+                            const float rb = pp[j].b.x;
+                            const float2 *row = win + j * WB;
+#pragma unroll
+                            for (int m = 0; m < M; ++m) {
+                                const float dwp = fmaf(d[m][0], pa.x, fmaf(d[m][1], pa.y, fmaf(d[m][2], pa.z, gsl[m])));
+                                const float t = fmaf(whi[m] + uacc[m], invd, rb);
+                                const float ph = cphp[m] + pa.w;
+                                uacc[m] += dwp;
+                                cphp[m] = fmaf(dwp, Kr, cphp[m]);
+                                const float fl = floorf(t);
+                                const int i = (int)fl;
+                                const float fr = t - fl;
+                                const bool ok = (k >= azs[m]) & (k < aze[m]) & (t >= h.tlo) & (t <= h.thi);
+                                const bool inwin = (unsigned)i < (unsigned)(WB - 1);
+                                const int is = inwin ? i : 0;
+                                float2 s0 = row[is], s1 = row[is + 1];
+                                if (ok && !inwin) {
+                                    s0 = ld_sample(B, k, i + h.x0);
+                                    s1 = ld_sample(B, k, i + h.x0 + 1);
+                                }
+                                float vr = fmaf(fr, s1.x - s0.x, s0.x);
+                                float vi = fmaf(fr, s1.y - s0.y, s0.y);
+                                vr = ok ? vr : 0.f;
+                                vi = ok ? vi : 0.f;
+                                float sn, cs;
+                                __sincosf(ph, &sn, &cs);
+                                accr[m] = fmaf(vr, cs, fmaf(-vi, sn, accr[m]));
+                                acci[m] = fmaf(vr, sn, fmaf(vi, cs, acci[m]));
+                            }
+                        }
+                    }
+                    // back to the plain accumulators: remove the folded dr2 terms
+#pragma unroll
+                    for (int m = 0; m < M; ++m) {
+                        const float lin = fmaf((float)nk, gsl[m], dr0[m]);
+                        dwa[m] = uacc[m] - lin;
+                        cph[m] = fmaf(-lin, Kr, cphp[m]);
+                    }
+                    // keep the carried phase in [-pi, pi]
+#pragma unroll
+                    for (int m = 0; m < M; ++m) {
+                        const float nr = rintf(cph[m] * kInvTwoPi);
+                        cph[m] = fmaf(-nr, kTwoPiLo, fmaf(-nr, kTwoPiHi, cph[m]));
+                    }
+                } else {
+                    const double rs = B.rngstart, rmx = B.rmax, dm = B.dmrg, k4 = B.k4pi;
+                    const int x0 = h.x0;
+                    const bool fast = h.fast;
+                    for (int j = 0; j < nk; ++j) {
+                        const int k = k0 + j;
+                        const double sx = pp[j].s[0], sy = pp[j].s[1], sz = pp[j].s[2];
+                        const float2 *row = win + j * WB;
+#pragma unroll
+                        for (int m = 0; m < M; ++m) {
+                            if (!fast && (k < azs[m] || k >= aze[m])) continue;
+                            const double vx = dsub(X[m][0], sx), vy = dsub(X[m][1], sy),
+                                         vz = dsub(X[m][2], sz);
+                            const double R = __dsqrt_rn(dadd(dadd(dmul(vx, vx), dmul(vy, vy)), dmul(vz, vz)));
+                            const bool inr = R >= rs && R <= rmx;
+                            if (!fast && !inr) continue;
+                            const double rr = ddiv(dsub(R, rs), dm);
+                            const double fl = floor(rr);
+                            const int ig = (int)fl;
+                            const double fr = dsub(rr, fl);
+                            const float w0 = __double2float_rn(dsub(1.0, fr));
+                            const float w1 = __double2float_rn(fr);
+                            const int i = ig - x0;
+                            float2 s0, s1;
+                            if ((unsigned)i < (unsigned)(WB - 1)) {
+                                s0 = row[i];
+                                s1 = row[i + 1];
+                            } else {
+                                // outside the staged window (the window estimate missed):
+                                // the fast path skipped the range test, apply it here
+                                if (!inr) continue;
+                                s0 = ld_sample(B, k, ig);
+                                s1 = ld_sample(B, k, ig + 1);
+                            }
+                            const float cre = __fadd_rn(__fmul_rn(s0.x, w0), __fmul_rn(s1.x, w1));
+                            const float cim = __fadd_rn(__fmul_rn(s0.y, w0), __fmul_rn(s1.y, w1));
+                            double sn, cs;
+                            sincos(dmul(k4, R), &sn, &cs);
+                            const double a = (double)cre, bq = (double)cim;
+                            accr_d[m] += a * cs - bq * sn;
+                            acci_d[m] += a * sn + bq * cs;
+                        }
+                    }
+                }
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&ctl.empty[s]);
+            }
+            // ---- epilogue ----
+            if (!ctl.abort) {
+#pragma unroll
+                for (int m = 0; m < M; ++m) {
+                    const int bi = warp + NC * m;
+                    const int x = 8 * (bi % BX) + (lane & 7), y = 4 * (bi / BX) + (lane >> 3);
+                    const int px = px0 + x, line = ly0 + y;
+                    if (px <= B.lastpix_eff && line < B.nlines) {
+                        float2 o = make_float2(0.f, 0.f);
+                        const int n = aze[m] - azs[m];
+                        if (n > 0) {
+                            const float sc = __double2float_rn(ddiv(1.0, (double)n));
+                            const float re = FORM == FORM_SPLIT ? accr[m] : __double2float_rn(accr_d[m]);
+                            const float im = FORM == FORM_SPLIT ? acci[m] : __double2float_rn(acci_d[m]);
+                            o = make_float2(__fmul_rn(re, sc), __fmul_rn(im, sc));
+                        }
+                        B.out[(long long)line * B.out_ld + (px - B.out_pix0)] = o;
+                    }
+                }
+            }
+        }
+        gchunk += nchunks;
+        __syncthreads();
+        if (ctl.abort) {
+            if (tid == 0) atomicOr(err, ERR_TMA_TIMEOUT);
+            // let the copies this CTA issued drain before it leaves (bounded)
+            if (producer && lane == 0) {
+                for (int s = 0; s < NS; ++s)
+                    if (issued & (1u << s)) mbar_wait_bounded(&ctl.full[s], (issued_par >> s) & 1u);
+            }
+            return;
+        }
+    }
+}
+
+}  // namespace srg

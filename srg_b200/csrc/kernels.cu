@@ -1,6 +1,7 @@
 // kernels.cu -- auxiliary device kernels and the compiled shapes of the
 // tiled backprojection.
 #include "bp_kernel.cuh"
+#include "bp_ws.cuh"
 #include "kernels.h"
 
 namespace srg {
@@ -181,21 +182,37 @@ cudaError_t launch_fma_peak(int fp64, int blocks, int iters, void *sink, cudaStr
 }
 
 // ---------------------------------------------------------------------------
-// Compiled shapes of the tiled kernel.  {form, tile_x, tile_y, threads,
-// chunk, window}.
+// Compiled shapes.  First generation (bp_tiles): {form, tile_x, tile_y,
+// threads, chunk, window}.  Warp-specialised (bp_ws): {form, tile_x, tile_y,
+// consumer warps, chunk, stages, window, min blocks per SM}; block = consumer
+// warps + 1.
 #define SRG_SHAPES(X)                  \
-    X(FORM_SPLIT, 32, 16, 128, 32, 192) \
-    X(FORM_SPLIT, 64, 8, 128, 32, 256)  \
     X(FORM_SPLIT, 32, 8, 128, 32, 160)  \
     X(FORM_SPLIT, 32, 16, 128, 16, 192) \
-    X(FORM_FP64, 32, 8, 128, 32, 160)   \
     X(FORM_FP64, 32, 4, 128, 32, 128)   \
-    X(FORM_FP64, 32, 16, 128, 16, 192)
+    X(FORM_FP64, 32, 8, 128, 32, 160)
 
-#define SRG_ENTRY(F, TXv, TYv, NTv, CKv, WBv) \
-    {F, {TXv, TYv, NTv, CKv, WBv}, params_bytes<F, CKv>(), (const void *)bp_tiles<F, TXv, TYv, NTv, CKv>},
+#define SRG_WS_SHAPES(X)                    \
+    X(FORM_SPLIT, 32, 8, 4, 16, 3, 128, 3)  \
+    X(FORM_SPLIT, 32, 8, 4, 16, 3, 128, 4)  \
+    X(FORM_SPLIT, 32, 8, 4, 16, 2, 128, 3)  \
+    X(FORM_SPLIT, 32, 8, 4, 24, 3, 128, 3)  \
+    X(FORM_SPLIT, 32, 8, 4, 31, 2, 128, 3)  \
+    X(FORM_SPLIT, 16, 16, 4, 16, 3, 96, 3)  \
+    X(FORM_SPLIT, 32, 16, 4, 16, 3, 144, 2) \
+    X(FORM_FP64, 32, 4, 4, 16, 2, 128, 3)   \
+    X(FORM_FP64, 32, 8, 4, 16, 2, 128, 2)
 
-const KernelEntry kKernels[] = {SRG_SHAPES(SRG_ENTRY)};
+#define SRG_ENTRY(F, TXv, TYv, NTv, CKv, WBv)                                                   \
+    {F, {TXv, TYv, NTv, CKv, WBv}, params_bytes<F, CKv>() + 1024 + CKv * WBv * 8,               \
+     (const void *)bp_tiles<F, TXv, TYv, NTv, CKv>},
+#define SRG_WS_ENTRY(F, TXv, TYv, NCv, CKv, NSv, WBv, MBv)                                      \
+    {F, {TXv, TYv, (NCv + 1) * 32, CKv, WBv}, ws_smem_bytes<F, CKv, NSv>(WBv),                  \
+     (const void *)bp_ws<F, TXv, TYv, NCv, CKv, NSv, MBv>},
+
+// The warp-specialised shapes come first: the first shape of a form is its
+// default.
+const KernelEntry kKernels[] = {SRG_WS_SHAPES(SRG_WS_ENTRY) SRG_SHAPES(SRG_ENTRY)};
 const int kNumKernels = sizeof(kKernels) / sizeof(kKernels[0]);
 
 cudaError_t launch_tiles(const KernelEntry &e, int grid, size_t smem, cudaStream_t st,

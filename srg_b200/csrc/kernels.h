@@ -14,8 +14,8 @@ struct CentreParams {
 
 struct KernelEntry {
     int form;
-    TileShape shape;
-    int params_bytes;
+    TileShape shape;   // threads = block size
+    int smem;          // dynamic shared memory bytes
     const void *fn;
 };
 
@@ -38,8 +38,6 @@ cudaError_t launch_forward_project(const BurstDev &B, const float2 *refl, long l
 
 cudaError_t launch_fma_peak(int fp64, int blocks, int iters, void *sink, cudaStream_t st);
 
-inline int shared_bytes(const KernelEntry &e) {
-    return e.params_bytes + 1024 + e.shape.chunk * e.shape.window * 8;
-}
+inline int shared_bytes(const KernelEntry &e) { return e.smem; }
 
 }  // namespace srg

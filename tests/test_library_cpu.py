@@ -31,7 +31,7 @@ def test_tile_shapes_are_valid():
     assert any(c[1] == _lib.FORM_SPLIT for c in cfgs)
     assert any(c[1] == _lib.FORM_FP64 for c in cfgs)
     for idx, form, tx, ty, nt, ck, wb in cfgs:
-        assert (tx * ty) % nt == 0 and nt % 32 == 0
+        assert nt % 32 == 0 and tx % 8 == 0 and ty % 4 == 0
         assert 1 <= ck <= 32
         assert wb % 2 == 0 and 2 <= wb <= 256  # TMA box limits; 16-byte rows
         assert ck * wb * 8 + ck * 48 <= 227 * 1024
