@@ -175,38 +175,86 @@ def phase_error(torch, wl):
 
 
 def e2e_dropin(torch, wl, steps, form):
-    """End to end through azimuth_compress_ (the drop-in C ABI): pinned host
-    burst buffer, DEM and .geo on tmpfs; returns (s per step, h2d, d2h bytes)."""
+    """End to end through azimuth_compress_ (the drop-in C ABI), one call per
+    burst in acquisition order as the reference's driver makes them: burst
+    lines in pinned host memory, the DEM and the .geo raster as files on tmpfs
+    (when it has room, else the temp dir).  Returns (s per step, h2d, d2h
+    bytes per step)."""
     from srg_b200 import api
     api.set_default_form(form)
-    tmp = "/dev/shm" if os.path.isdir("/dev/shm") else None
+    b0 = wl.bursts[0].b
+    geo_bytes = b0.demlength * b0.demwidth * 8
+    dem_bytes = b0.demlength * b0.demwidth * 2
+    tmp = None
+    if os.path.isdir("/dev/shm"):
+        st = os.statvfs("/dev/shm")
+        if st.f_bavail * st.f_frsize > 2 * (geo_bytes + dem_bytes):
+            tmp = "/dev/shm"
+    h2d = d2h = 0
     with tempfile.TemporaryDirectory(dir=tmp) as td:
-        prepared = []
-        for i, db in enumerate(wl.bursts):
-            b = db.b
-            host = torch.empty(tuple(db.burst.shape), dtype=torch.complex64, pin_memory=True)
-            host.copy_(db.burst)
-            dem_path = os.path.join(td, f"dem{i}")
-            geo_path = os.path.join(td, f"geo{i}")
-            np.ascontiguousarray(b.dem, np.int16).tofile(dem_path)
-            np.zeros((b.demlength, b.demwidth), np.complex64).tofile(geo_path)
-            prepared.append((b, host, os.open(dem_path, os.O_RDWR), os.open(geo_path, os.O_RDWR)))
+        dem_path = os.path.join(td, "elevation.dem")
+        geo_path = os.path.join(td, "scene.geo")
+        np.ascontiguousarray(b0.dem, np.int16).tofile(dem_path)
+        with open(geo_path, "wb") as f:
+            f.truncate(geo_bytes)
+        fd_dem = os.open(dem_path, os.O_RDWR)
+        fd_geo = os.open(geo_path, os.O_RDWR)
+        hosts = []
         try:
-            for b, host, fd_dem, fd_geo in prepared:   # warm-up
-                api.azimuth_compress_files(b, fd_geo, fd_dem, burst=host.numpy())
+            for db in wl.bursts:
+                host = torch.empty(tuple(db.burst.shape), dtype=torch.complex64, pin_memory=True)
+                host.copy_(db.burst)
+                hosts.append(host)
+                fl, ll, fp, lp = api.limits(db.b)
+                nl = ll - fl + 1
+                ncols = max(0, min(lp, db.b.demwidth - 1) - fp + 1)
+                h2d += host.numel() * 8 + db.b.rawdatalines * 24 + nl * db.b.demwidth * 2
+                d2h += nl * ncols * 8
+            for db, host in zip(wl.bursts, hosts):   # warm-up
+                api.azimuth_compress_files(db.b, fd_geo, fd_dem, burst=host.numpy())
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             for _ in range(steps):
-                for b, host, fd_dem, fd_geo in prepared:
-                    api.azimuth_compress_files(b, fd_geo, fd_dem, burst=host.numpy())
+                for db, host in zip(wl.bursts, hosts):
+                    api.azimuth_compress_files(db.b, fd_geo, fd_dem, burst=host.numpy())
             torch.cuda.synchronize()
             dt = (time.perf_counter() - t0) / steps
         finally:
-            for _, _, a, c in prepared:
-                os.close(a)
-                os.close(c)
-    h2d, d2h = wl.descs_bytes()
+            os.close(fd_dem)
+            os.close(fd_geo)
+            del hosts
     return dt, h2d, d2h
+
+
+def time_plan(torch, plan, steps, warmup, stream, stages=None):
+    """K passes of a scene plan on `stream` (graph replay), or of chosen
+    stages; returns ms per pass (CUDA events on the stream)."""
+    sp = stream.cuda_stream
+    run = (lambda: plan.run(sp)) if stages is None else (lambda: plan.run_stages(stages, sp))
+    for _ in range(warmup):
+        run()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(steps)]
+    for e0, e1 in ev:
+        e0.record(stream)
+        run()
+        e1.record(stream)
+    torch.cuda.synchronize()
+    plan.sync(sp)
+    return sum(e0.elapsed_time(e1) for e0, e1 in ev) / steps
+
+
+def raster_phase_error(torch, a, ref):
+    a = a.to(torch.complex128)
+    r = ref.to(torch.complex128)
+    amp = r.abs()
+    rms = torch.sqrt((amp[amp > 0] ** 2).mean())
+    m = amp > 0.05 * rms
+    ph = torch.angle(a[m] * r[m].conj()) * 1e3
+    ar = (a[m].abs() - amp[m]).abs() / amp[m]
+    return {"ph_rms_mrad": float(torch.sqrt((ph ** 2).mean())), "ph_max_mrad": float(ph.abs().max()),
+            "amp_rel_rms": float(torch.sqrt((ar ** 2).mean())), "pixels": int(ph.numel())}
 
 
 # ---------------------------------------------------------------------------
@@ -263,9 +311,9 @@ def reference_cpu_sample(wl, budget_s: float = 15.0):
     while True:
         s = slab(n)
         with quiet_stdout():
-            t0 = time.perf_counter()
-            ref.azimuth_compress_cpu(s)
-            dt = time.perf_counter() - t0
+            timing = {}
+            ref.azimuth_compress_cpu(s, timing=timing)
+            dt = timing["call_s"]
         if dt > budget_s / 8 or n >= db.nlines:
             break
         n = min(db.nlines, max(n * 2, int(n * budget_s / 4 / max(dt, 1e-3))))
@@ -285,7 +333,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c1", choices=["c1"])
+    ap.add_argument("--workload", default="c3", choices=["c1", "c3"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -300,10 +348,12 @@ def main():
     torch.cuda.set_device(local)
     from srg_b200 import _lib, workloads
 
+    build = workloads.config3 if args.workload == "c3" else workloads.config1
     if args.impl == "reference":
-        wl = workloads.config1(device=f"cuda:{local}")
+        wl = build(device=f"cuda:{local}")
         from srg_b200 import api
-        api.backproject(wl.bursts, form=_lib.FORM_FP64, coefs=wl.coefs)  # marks formed rows
+        for db in wl.bursts[:1]:  # marks the formed rows of the sampled burst
+            api.backproject([db], form=_lib.FORM_FP64)
         vals = []
         for _ in range(max(1, args.steps)):
             v, cores, sample = reference_cpu_sample(wl, budget_s=8.0)
@@ -320,31 +370,52 @@ def main():
         print(json.dumps(line))
         return
 
-    wl = workloads.config1(device=f"cuda:{local}", seed=1001 + rank)
+    wl = build(device=f"cuda:{local}", seed=(1003 if args.workload == "c3" else 1001) + rank)
     stream = torch.cuda.Stream()
     fp32_peak = _lib.measure_fma_peak(False)
     fp64_peak = _lib.measure_fma_peak(True)
-    with ClockSampler(local) as clk:
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
-        s_ms, s_kern, launches = time_steps(torch, wl, _lib.FORM_SPLIT, args.steps, args.warmup,
-                                            stream)
-        if world > 1:
-            dist.barrier()
-    d_ms, d_kern, _ = time_steps(torch, wl, _lib.FORM_FP64, max(3, args.steps // 2),
-                                 args.warmup, stream)
+    tuned = {}
+    if args.workload == "c3":
+        plan = wl.plan
+        tuned["split"] = plan.tune(iters=2)
+        with ClockSampler(local) as clk:
+            if world > 1:
+                dist.barrier()
+            s_ms = time_plan(torch, plan, args.steps, args.warmup, stream)
+            if world > 1:
+                dist.barrier()
+        s_kern = time_plan(torch, plan, args.steps, 1, stream, stages=2)
+        split_raster = wl.raster.clone()
+        plan.set_form(_lib.FORM_FP64)
+        tuned["fp64"] = plan.tune(iters=1)
+        d_ms = time_plan(torch, plan, max(3, args.steps // 3), 1, stream)
+        d_kern = d_ms
+        perr = raster_phase_error(torch, split_raster, wl.raster)
+        del split_raster
+        plan.set_form(_lib.FORM_SPLIT, tuned["split"][0])
+        launches = 3  # azimuth centres, backprojection, merge (one graph per pass)
+    else:
+        with ClockSampler(local) as clk:
+            if world > 1:
+                dist.barrier()
+            torch.cuda.synchronize()
+            s_ms, s_kern, launches = time_steps(torch, wl, _lib.FORM_SPLIT, args.steps,
+                                                args.warmup, stream)
+            if world > 1:
+                dist.barrier()
+        d_ms, d_kern, _ = time_steps(torch, wl, _lib.FORM_FP64, max(3, args.steps // 2),
+                                     args.warmup, stream)
+        perr = phase_error(torch, wl)
     if world > 1:
         t = torch.tensor([s_ms, d_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         s_ms, d_ms = float(t[0]), float(t[1])
-    perr = phase_error(torch, wl)
     e2e_s, h2d, d2h = e2e_dropin(torch, wl, args.e2e_steps, _lib.FORM_SPLIT)
     terms_all = wl.terms * world
     value = terms_all / (s_ms * 1e-3) / 1e9
     fp64_value = terms_all / (d_ms * 1e-3) / 1e9
     achieved = FLOPS_PER_TERM * wl.terms / (s_kern * 1e-3) / 1e12
-    traffic = load_traffic("bp_tiles_split", wl.name)
+    traffic = load_traffic("bp_split", wl.name)
     cpu = None
     if rank == 0 and not args.no_cpu_baseline and os.path.exists(
             os.path.join(ROOT, "oracle", "_ref", "libref_cpu.so")):
@@ -358,10 +429,16 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": s_ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 (split; FP64 orbit/ECEF/reference range)",
-        "data": "synthetic (forward-projected; seeded)",
+        "data": ("synthetic, seeded: complex Gaussian clutter + forward-projected point targets"
+                 if args.workload == "c3" else "synthetic, seeded: forward-projected scatterers"),
         "config": {"workload": wl.description, "bursts": len(wl.bursts),
-                   "terms_per_step_per_gpu": wl.terms, "l2": "inputs 252 MB per burst > 126 MB L2; no flush",
-                   "parallelism": f"replicas x{world} (one workload per GPU)"},
+                   "terms_per_step_per_gpu": wl.terms,
+                   "l2": "range lines of every burst > 126 MB L2; no flush between steps",
+                   "parallelism": f"replicas x{world} (one workload per GPU)",
+                   "kernel_shapes": {k: _lib.tile_configs()[v[0]][2:] for k, v in tuned.items()},
+                   "step": ("one graph replay: azimuth centres of every line, one persistent "
+                            "backprojection launch for all bursts, ordered merge into the scene raster")
+                   if args.workload == "c3" else "azimuth centres + backprojection of one burst"},
         "fp64_form": {"value": fp64_value, "ms_per_step": d_ms, "kernel_ms": d_kern,
                       "split_over_fp64": value / fp64_value},
         "phase_error_vs_fp64": perr,

@@ -129,6 +129,47 @@ typedef struct srg_burst_desc {
 int srg_bp_bursts_device(const srg_burst_desc *bursts, int n,
                          const srg_bp_options *opts, void *stream);
 
+/* ------------------------------------------------------------------------
+ * Scene plans: a reusable, graph-captured pass over a fixed set of
+ * device-resident bursts (e.g. the 27 bursts of an IW scene, or a stack of
+ * repeat-pass acquisitions), with an ordered merge into a scene raster.
+ * No reference counterpart: the reference processes one burst per call
+ * (sentinel/backprojectgpusub.f90:140-248 loops azimuth_compress_ serially)
+ * and merges each into the .geo file in that order.
+ * ------------------------------------------------------------------------ */
+typedef struct srg_scene srg_scene;
+
+/* Build a plan.  Every descriptor's coef must be NULL (the plan solves the
+ * azimuth centres on the device each pass).  scene (device, complex64,
+ * scene_lines x scene_cols, row stride scene_ld) may be NULL; otherwise each
+ * pass merges burst outputs into it in burst order with the reference's rule
+ * (|Re| > 1e-18), burst rows placed at grid line firstline + row and column
+ * out_pix0 + c.  Allocates the plan's own device memory. */
+int srg_scene_create(const srg_burst_desc *bursts, int n, float *scene, int64_t scene_ld,
+                     int scene_lines, int scene_cols, const srg_bp_options *opts,
+                     srg_scene **out);
+/* Enqueue one pass on `stream`: azimuth centres of every line of every burst
+ * (one launch), the persistent backprojection of all bursts (one launch),
+ * the ordered merge (one launch).  On a non-default stream the first pass
+ * is captured in a CUDA graph that later passes replay. */
+int srg_scene_run(srg_scene *s, void *stream);
+/* Enqueue chosen stages of a pass without a graph: 1 = azimuth centres,
+ * 2 = backprojection, 4 = merge (OR them). */
+int srg_scene_run_stages(srg_scene *s, int stages, void *stream);
+/* Wait for `stream` and report device-side errors of the plan's kernels. */
+int srg_scene_sync(srg_scene *s, void *stream);
+/* Exact executed-term count of one pass (computed once, blocking). */
+int srg_scene_terms(srg_scene *s, int64_t *terms);
+/* Autotuner: time every compiled kernel shape of the plan's form on this
+ * scene (`iters` timed launches each) and keep the fastest. */
+int srg_scene_tune(srg_scene *s, int iters, int *best_cfg, double *best_ms);
+/* Select a kernel shape, or a form and shape (-1: that form's default). */
+int srg_scene_set_shape(srg_scene *s, int tile_cfg);
+int srg_scene_set_form(srg_scene *s, int form, int tile_cfg);
+/* Kernel shape index in use. */
+int srg_scene_shape(const srg_scene *s);
+void srg_scene_destroy(srg_scene *s);
+
 /* Exact count of executed terms (pixel, pulse pairs inside the aperture
  * window that pass the reference's range test) of the given bursts, computed
  * on the device with the reference's FP64 arithmetic.  Blocking. */

@@ -181,9 +181,10 @@ def call_33(fn, b, fdout: int, fddem: int, burst=None):
        r(dbl["angc0"]), r(dbl["angc1"]), r(dbl["prf"]))
 
 
-def run_33_files(fn, b, geo_init=None):
+def run_33_files(fn, b, geo_init=None, timing=None):
     """Run a 33-arg entry with a temporary DEM file and .geo file; return the
-    resulting [L][W] complex64 raster."""
+    resulting [L][W] complex64 raster.  timing (dict, optional) receives the
+    wall time of the entry call alone as timing["call_s"]."""
     with tempfile.TemporaryDirectory() as td:
         dem_path = os.path.join(td, "elevation.dem")
         geo_path = os.path.join(td, "scene.geo")
@@ -194,7 +195,11 @@ def run_33_files(fn, b, geo_init=None):
         fddem = os.open(dem_path, os.O_RDWR)
         fdout = os.open(geo_path, os.O_RDWR)
         try:
+            import time as _t
+            t0 = _t.perf_counter()
             call_33(fn, b, fdout, fddem)
+            if timing is not None:
+                timing["call_s"] = _t.perf_counter() - t0
             # The reference leaves its fdopen() stream unflushed; write out its
             # buffered tail before the descriptor is closed.
             C.CDLL(None).fflush(None)
@@ -245,5 +250,5 @@ class RefCPU:
                           C.c_int(b.rawdatalines))
         return az
 
-    def azimuth_compress_cpu(self, b, geo_init=None):
-        return run_33_files(self.lib.azimuth_compress_cpu_, b, geo_init)
+    def azimuth_compress_cpu(self, b, geo_init=None, timing=None):
+        return run_33_files(self.lib.azimuth_compress_cpu_, b, geo_init, timing)

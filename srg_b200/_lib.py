@@ -74,6 +74,17 @@ _SIGS = {
     "srg_sync_check": (C.c_int, [C.c_void_p]),
     "srg_measure_fma_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
     "srg_bp_burst_device_noalloc": (C.c_int, [C.POINTER(BurstDesc), C.POINTER(Options), C.c_void_p]),
+    "srg_scene_create": (C.c_int, [C.POINTER(BurstDesc), C.c_int, C.c_void_p, C.c_int64, C.c_int,
+                                   C.c_int, C.POINTER(Options), C.POINTER(C.c_void_p)]),
+    "srg_scene_run": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "srg_scene_sync": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "srg_scene_run_stages": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "srg_scene_terms": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "srg_scene_tune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+    "srg_scene_set_shape": (C.c_int, [C.c_void_p, C.c_int]),
+    "srg_scene_set_form": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "srg_scene_shape": (C.c_int, [C.c_void_p]),
+    "srg_scene_destroy": (None, [C.c_void_p]),
     "srg_tile_config_count": (C.c_int, []),
     "srg_tile_config": (C.c_int, [C.c_int, _ip, _ip, _ip, _ip, _ip]),
     "srg_forward_project_device": (C.c_int, [C.POINTER(BurstDesc), C.c_void_p, C.c_int64, C.c_void_p,

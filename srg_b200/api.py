@@ -99,6 +99,7 @@ class DeviceBurst:
     nlines: int
     firstpix: int
     lastpix: int
+    out_pix0: int = 0      # grid pixel of out[:, 0]
     keep: dict = dataclasses.field(default_factory=dict)
 
     def desc(self, coef_ptr: int = 0) -> BurstDesc:
@@ -117,7 +118,7 @@ class DeviceBurst:
         d.demwidth = b.demwidth
         d.firstline, d.nlines, d.firstpix, d.lastpix = (self.firstline, self.nlines, self.firstpix,
                                                         self.lastpix)
-        d.out_pix0 = 0
+        d.out_pix0 = self.out_pix0
         d.aperture = b.aperture
         d.firstlat, d.deltalat, d.firstlon, d.deltalon = b.firstlat, b.deltalat, b.firstlon, b.deltalon
         d.rngstart, d.rngend, d.dmrg, d.wvl = b.rngstart, b.rngend, b.dmrg, b.wvl
@@ -133,7 +134,11 @@ class DeviceBurst:
         return d
 
 
-def to_device(b: Burst, device="cuda", burst_tensor=None) -> DeviceBurst:
+def to_device(b: Burst, device="cuda", burst_tensor=None, dem_tensor=None,
+              narrow_out: bool = False) -> DeviceBurst:
+    """Device copy of a burst.  dem_tensor: an already-resident full DEM
+    ([demlength][demwidth] int16) to take the slab from without copying;
+    narrow_out: output columns only for [firstpix, min(lastpix, W-1)]."""
     import torch
 
     fl, ll, fp, lp = limits(b)
@@ -141,10 +146,19 @@ def to_device(b: Burst, device="cuda", burst_tensor=None) -> DeviceBurst:
     if burst_tensor is None:
         burst_tensor = torch.from_numpy(np.ascontiguousarray(b.burst, np.complex64)).to(device)
     sat = torch.from_numpy(_d(b.satloc)).to(device)
-    dem = torch.from_numpy(np.ascontiguousarray(b.dem[fl:fl + nl], np.int16)).to(device)
-    out = torch.zeros((nl, b.demwidth), dtype=torch.complex64, device=device)
+    if dem_tensor is not None:
+        dem = dem_tensor[fl:fl + nl]
+    else:
+        dem = torch.from_numpy(np.ascontiguousarray(b.dem[fl:fl + nl], np.int16)).to(device)
+    if narrow_out:
+        ncols = max(0, min(lp, b.demwidth - 1) - fp + 1)
+        out = torch.zeros((nl, max(ncols, 1)), dtype=torch.complex64, device=device)
+        pix0 = fp
+    else:
+        out = torch.zeros((nl, b.demwidth), dtype=torch.complex64, device=device)
+        pix0 = 0
     return DeviceBurst(b=b, burst=burst_tensor, satloc=sat, dem=dem, out=out, firstline=fl,
-                       nlines=nl, firstpix=fp, lastpix=lp)
+                       nlines=nl, firstpix=fp, lastpix=lp, out_pix0=pix0)
 
 
 def _stream_ptr(stream) -> Optional[int]:
@@ -217,3 +231,61 @@ def forward_project(db: DeviceBurst, refl, satvel, antenna: float = 10.0, stream
     check(lib().srg_forward_project_device(C.byref(d), C.c_void_p(refl.data_ptr()), refl.stride(0),
                                            C.c_void_p(satvel.data_ptr()), antenna,
                                            C.c_void_p(_stream_ptr(stream))))
+
+
+class Scene:
+    """A reusable plan over device bursts (srg_scene_*): azimuth centres,
+    one persistent backprojection launch for all bursts and the ordered merge
+    into `raster` (optional, [lines][cols] complex64 on the device), replayed
+    from a CUDA graph on a non-default stream."""
+
+    def __init__(self, bursts: Sequence[DeviceBurst], raster=None, form: int = FORM_SPLIT,
+                 tile_cfg: int = -1):
+        self.bursts = list(bursts)
+        self.raster = raster
+        self._descs = (BurstDesc * len(self.bursts))(*[db.desc() for db in self.bursts])
+        o = default_options(form, tile_cfg)
+        h = C.c_void_p()
+        if raster is not None:
+            args = (C.c_void_p(raster.data_ptr()), raster.stride(0), raster.shape[0], raster.shape[1])
+        else:
+            args = (None, 0, 0, 0)
+        check(lib().srg_scene_create(self._descs, len(self.bursts), *args, C.byref(o), C.byref(h)))
+        self.handle = h
+
+    def run(self, stream=None) -> None:
+        check(lib().srg_scene_run(self.handle, C.c_void_p(_stream_ptr(stream))))
+
+    def run_stages(self, stages: int, stream=None) -> None:
+        """1 = azimuth centres, 2 = backprojection, 4 = merge (no graph)."""
+        check(lib().srg_scene_run_stages(self.handle, stages, C.c_void_p(_stream_ptr(stream))))
+
+    def sync(self, stream=None) -> None:
+        check(lib().srg_scene_sync(self.handle, C.c_void_p(_stream_ptr(stream))))
+
+    def terms(self) -> int:
+        n = C.c_int64()
+        check(lib().srg_scene_terms(self.handle, C.byref(n)))
+        return int(n.value)
+
+    def tune(self, iters: int = 3):
+        cfg, ms = C.c_int(), C.c_double()
+        check(lib().srg_scene_tune(self.handle, iters, C.byref(cfg), C.byref(ms)))
+        return int(cfg.value), float(ms.value)
+
+    def set_form(self, form: int, tile_cfg: int = -1) -> None:
+        check(lib().srg_scene_set_form(self.handle, form, tile_cfg))
+
+    def shape(self) -> int:
+        return int(lib().srg_scene_shape(self.handle))
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib().srg_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

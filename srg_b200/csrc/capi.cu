@@ -529,35 +529,49 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
         std::lock_guard<std::mutex> g(g_opts_mu);
         o = g_default_opts;
     }
-    int fl, ll, fp, lp;
-    ref_limits(latlons, firstlat, deltalat, firstlon, deltalon, demwidth, demlength, &fl, &ll, &fp,
-               &lp);
+    int fl, ll, fp_, lp_;
+    ref_limits(latlons, firstlat, deltalat, firstlon, deltalon, demwidth, demlength, &fl, &ll, &fp_,
+               &lp_);
     const int nl = ll - fl + 1;
     if (o.verbose) printf("Burst line limits, size (first,last,nlines) %d %d %d\n", fl, ll, nl);
     const int W = demwidth;
     const size_t npix = (size_t)nl * W;
+    const int fp = fp_, lp = lp_;
 
-    // DEM slab (azimuth_compress.cu:399-408); a short read leaves zeros.
-    std::vector<int16_t> slab(npix, 0);
-    {
-        const ssize_t want = (ssize_t)(npix * 2);
-        const ssize_t got = pread(fddem, slab.data(), want, (off_t)fl * W * 2);
-        if (got < 0) return fail(SRG_E_IO, "DEM read failed (fd %d, offset %lld)", fddem,
-                                 (long long)fl * W * 2);
-    }
     DevCtx *c = nullptr;
     int rc = get_ctx(o.device, &c);
     if (rc) return rc;
     std::lock_guard<std::mutex> g(c->mu);
     cudaStream_t st = 0;
+    // pinned staging: the DEM slab in, the output window back
+    const int fp_eff = std::max(fp, 0);
+    const int lp_eff = std::min(lp, W - 1);
+    const int ncols = lp_eff >= fp_eff ? lp_eff - fp_eff + 1 : 0;
+    const size_t dem_bytes = npix * 2;
+    const size_t win_bytes = (size_t)nl * ncols * 8;
+    const size_t stage_bytes = std::max(dem_bytes, win_bytes) + 64;
+    if (stage_bytes > c->host_cap) {
+        if (c->host_stage) cudaFreeHost(c->host_stage);
+        c->host_stage = nullptr;
+        c->host_cap = 0;
+        if (cudaMallocHost(&c->host_stage, stage_bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(SRG_E_NOMEM, "pinned staging of %zu bytes failed", stage_bytes);
+        }
+        c->host_cap = stage_bytes;
+    }
+    // DEM slab (azimuth_compress.cu:399-408); a short read leaves zeros
+    int16_t *slab = static_cast<int16_t *>(c->host_stage);
+    std::memset(slab, 0, dem_bytes);
+    if (pread(fddem, slab, dem_bytes, (off_t)fl * W * 2) < 0)
+        return fail(SRG_E_IO, "DEM read failed (fd %d, offset %lld)", fddem, (long long)fl * W * 2);
     const size_t bbytes = (size_t)rawdatalines * samplesPerBurst * 8;
     if ((rc = c->in_burst.ensure(bbytes)) || (rc = c->in_sat.ensure(24 * (size_t)rawdatalines)) ||
-        (rc = c->in_dem.ensure(npix * 2)) || (rc = c->out.ensure(npix * 8)))
+        (rc = c->in_dem.ensure(dem_bytes)) || (rc = c->out.ensure(npix * 8)))
         return rc;
     CK(cudaMemcpyAsync(c->in_burst.p, burstdata, bbytes, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(c->in_sat.p, satloc, 24 * (size_t)rawdatalines, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(c->in_dem.p, slab.data(), npix * 2, cudaMemcpyHostToDevice, st));
-    CK(cudaMemsetAsync(c->out.p, 0, npix * 8, st));
+    CK(cudaMemcpyAsync(c->in_dem.p, slab, dem_bytes, cudaMemcpyHostToDevice, st));
 
     srg_burst_desc d{};
     d.burst = static_cast<const float *>(c->in_burst.p);
@@ -597,29 +611,39 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     d.angc0 = angc0;
     d.angc1 = angc1;
     d.prf = prf;
-    if (fp <= std::min(lp, W - 1)) {
-        rc = run_bursts(*c, &d, 1, o, st);
-        if (rc) return rc;
-    }
-    std::vector<float> out(2 * npix), cur(2 * npix, 0.f);
-    CK(cudaMemcpyAsync(out.data(), c->out.p, npix * 8, cudaMemcpyDeviceToHost, st));
+    if (ncols == 0) return SRG_OK;  // no pixel of the grid in the burst's box
+    rc = run_bursts(*c, &d, 1, o, st);
+    if (rc) return rc;
+    // the kernel wrote every pixel of the window: bring back only the window
+    float *win = static_cast<float *>(c->host_stage);
+    CK(cudaMemcpy2DAsync(win, (size_t)ncols * 8, static_cast<float2 *>(c->out.p) + fp_eff,
+                         (size_t)W * 8, (size_t)ncols * 8, nl, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     CK(cudaGetLastError());
     rc = check_flags(*c, st);
     if (rc) return rc;
 
-    // merge into the .geo rows (azimuth_compress.cu:510-537)
-    const off_t off = (off_t)fl * W * 8;
-    if (pread(fdout, cur.data(), npix * 8, off) < 0)
-        return fail(SRG_E_IO, "output read failed (fd %d)", fdout);
-    for (size_t i = 0; i < npix; ++i) {
-        if (std::fabs((double)out[2 * i]) > 1.e-18) {
-            cur[2 * i] = out[2 * i];
-            cur[2 * i + 1] = out[2 * i + 1];
+    // merge into the .geo rows (azimuth_compress.cu:510-537); pixels outside
+    // the window are never replaced, so only the window is read and written
+    std::vector<float> cur(2 * (size_t)ncols);
+    for (int r = 0; r < nl; ++r) {
+        const off_t off = ((off_t)(fl + r) * W + fp_eff) * 8;
+        const ssize_t want = (ssize_t)ncols * 8;
+        const ssize_t got = pread(fdout, cur.data(), want, off);
+        if (got < 0) return fail(SRG_E_IO, "output read failed (fd %d)", fdout);
+        if (got < want) std::memset(reinterpret_cast<char *>(cur.data()) + got, 0, want - got);
+        const float *o2 = win + 2 * (size_t)r * ncols;
+        bool changed = false;
+        for (int i = 0; i < ncols; ++i) {
+            if (std::fabs((double)o2[2 * i]) > 1.e-18) {
+                cur[2 * i] = o2[2 * i];
+                cur[2 * i + 1] = o2[2 * i + 1];
+                changed = true;
+            }
         }
+        if (changed && pwrite(fdout, cur.data(), want, off) != want)
+            return fail(SRG_E_IO, "output write failed (fd %d)", fdout);
     }
-    const ssize_t wr = pwrite(fdout, cur.data(), npix * 8, off);
-    if (wr != (ssize_t)(npix * 8)) return fail(SRG_E_IO, "output write failed (fd %d)", fdout);
     return SRG_OK;
 }
 

@@ -33,6 +33,12 @@ struct DevBuf {
             return fail(SRG_E_NOMEM, "cudaMalloc(%zu) failed: %s", want, cudaGetErrorString(e));
         }
         cap = want;
+        // new scratch starts at zero (flag words are read before any kernel writes them)
+        e = cudaMemset(p, 0, want);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(SRG_E_CUDA, "cudaMemset of new scratch failed: %s", cudaGetErrorString(e));
+        }
         return SRG_OK;
     }
 };
@@ -48,6 +54,8 @@ struct DevCtx {
     DevBuf coef;      // doubles
     DevBuf orbit;     // state vectors
     DevBuf in_burst, in_sat, in_dem, out;  // drop-in staging
+    void *host_stage = nullptr;            // pinned host staging (drop-in entry)
+    size_t host_cap = 0;
     bool attrs_done[64] = {};
 };
 

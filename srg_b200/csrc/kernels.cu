@@ -12,14 +12,8 @@ namespace srg {
 // host; the arithmetic here is the same operation for operation.  Lines
 // firstline .. lastline-1 get a parabola; the last line keeps zeros (the
 // reference leaves it unset), so it is never formed.
-__global__ void line_centres_kernel(BurstDev B, Orbit o, CentreParams cp, double *coef) {
-    const int line = blockIdx.x * blockDim.x + threadIdx.x;
-    if (line >= B.nlines) return;
-    double *cl = coef + 3 * line;
-    if (line == B.nlines - 1) {
-        cl[0] = cl[1] = cl[2] = 0.0;
-        return;
-    }
+__device__ void line_coef(const BurstDev &B, const Orbit &o, const CentreParams &cp, int line,
+                          double *cl) {
     const int half = (B.lastpix - B.firstpix) / 2 - 1;
     int y[3];
     for (int s = 0; s < 3; ++s) {
@@ -48,6 +42,36 @@ __global__ void line_centres_kernel(BurstDev B, Orbit o, CentreParams cp, double
     cl[0] = dmul(0.5, dsub((double)(y[0] + y[2]), dmul(2.0, (double)y[1])));
     cl[1] = dmul(0.5, (double)(y[2] - y[0]));
     cl[2] = (double)y[1];
+}
+
+__global__ void line_centres_kernel(BurstDev B, Orbit o, CentreParams cp, double *coef) {
+    const int line = blockIdx.x * blockDim.x + threadIdx.x;
+    if (line >= B.nlines) return;
+    double *cl = coef + 3 * line;
+    if (line == B.nlines - 1) {
+        cl[0] = cl[1] = cl[2] = 0.0;
+        return;
+    }
+    line_coef(B, o, cp, line, cl);
+}
+
+// Batched per-line azimuth centres: one thread per (burst, line) over all
+// bursts of a scene (the same arithmetic as line_centres_kernel).
+__global__ void line_centres_batch_kernel(const BurstDev *__restrict__ bursts,
+                                          const CentreJob *__restrict__ jobs, int n, int total) {
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= total) return;
+    int b = 0;
+    while (b + 1 < n && jobs[b + 1].line_base <= gid) ++b;
+    const CentreJob &J = jobs[b];
+    const BurstDev &B = bursts[b];
+    const int line = gid - J.line_base;
+    double *cl = J.coef + 3 * line;
+    if (line == B.nlines - 1) {
+        cl[0] = cl[1] = cl[2] = 0.0;
+        return;
+    }
+    line_coef(B, J.orbit, J.cp, line, cl);
 }
 
 // ---------------------------------------------------------------------------
@@ -89,6 +113,47 @@ __global__ void merge_kernel(float2 *dst, long long dst_ld, const float2 *src, l
         const int c = (int)(i - (long long)r * cols);
         const float2 v = src[(long long)r * src_ld + c];
         if (fabs((double)v.x) > 1.e-18) dst[(long long)r * dst_ld + c] = v;
+    }
+}
+
+// Ordered merge of every burst of a scene into the scene raster: for each
+// scene pixel the last burst (in order) whose output there has
+// |Re| > 1e-18 wins, which is what merging the bursts one after the other
+// with the reference's rule gives.  Each CTA covers a 32 x 8 patch and first
+// collects (ballot) the bursts whose output window meets it.
+__global__ void merge_scene_kernel(const BurstDev *__restrict__ bursts, int n, float2 *dst,
+                                   long long dst_ld, int lines, int cols) {
+    const int c0 = blockIdx.x * 32, l0 = blockIdx.y * 8;
+    __shared__ unsigned mask[8];  // up to 256 bursts
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    for (int w = 0; w < 8; ++w) {
+        const int b = w * 32 + (tid & 31);
+        bool hit = false;
+        if (tid < 32 && b < n) {
+            const BurstDev &B = bursts[b];
+            const int gl0 = B.firstline, gl1 = B.firstline + B.nlines - 1;
+            hit = !(gl1 < l0 || gl0 > l0 + 7 || B.lastpix_eff < c0 || B.firstpix > c0 + 31);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, hit);
+        if (tid == 0) mask[w] = m;
+    }
+    __syncthreads();
+    const int l = l0 + threadIdx.y, c = c0 + threadIdx.x;
+    if (l >= lines || c >= cols) return;
+    for (int w = (n - 1) / 32; w >= 0; --w) {
+        unsigned m = mask[w];
+        while (m) {
+            const int bit = 31 - __clz(m);
+            m &= ~(1u << bit);
+            const BurstDev &B = bursts[w * 32 + bit];
+            const int ll = l - B.firstline;
+            if (ll < 0 || ll >= B.nlines || c < B.firstpix || c > B.lastpix_eff) continue;
+            const float2 v = B.out[(long long)ll * B.out_ld + (c - B.out_pix0)];
+            if (fabs((double)v.x) > 1.e-18) {
+                dst[(long long)l * dst_ld + c] = v;
+                return;
+            }
+        }
     }
 }
 
@@ -249,6 +314,22 @@ cudaError_t launch_merge(float2 *dst, long long dst_ld, const float2 *src, long 
     long long blocks = (n + 255) / 256;
     if (blocks > 32LL * sms) blocks = 32LL * sms;
     merge_kernel<<<(int)blocks, 256, 0, st>>>(dst, dst_ld, src, src_ld, rows, cols);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_line_centres_batch(const BurstDev *bursts, const CentreJob *jobs, int n,
+                                      int total, cudaStream_t st) {
+    if (total <= 0) return cudaSuccess;
+    line_centres_batch_kernel<<<(total + 127) / 128, 128, 0, st>>>(bursts, jobs, n, total);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_merge_scene(const BurstDev *bursts, int n, float2 *dst, long long dst_ld,
+                               int lines, int cols, cudaStream_t st) {
+    if (lines <= 0 || cols <= 0 || n <= 0) return cudaSuccess;
+    if (n > 256) return cudaErrorInvalidValue;
+    dim3 grid((cols + 31) / 32, (lines + 7) / 8);
+    merge_scene_kernel<<<grid, dim3(32, 8), 0, st>>>(bursts, n, dst, dst_ld, lines, cols);
     return cudaGetLastError();
 }
 

@@ -12,6 +12,15 @@ struct CentreParams {
     double tmid, xm[3], vm[3], wvl, angc0, angc1, prf, pi;
 };
 
+// One burst's share of a batched azimuth-centre launch.
+struct CentreJob {
+    Orbit orbit;          // device state vectors
+    CentreParams cp;
+    double *coef;         // [nlines][3] output (device)
+    int line_base;        // first global index of this burst's lines
+    int pad;
+};
+
 struct KernelEntry {
     int form;
     TileShape shape;   // threads = block size
@@ -27,6 +36,10 @@ cudaError_t launch_tiles(const KernelEntry &e, int grid, size_t smem, cudaStream
                          int *counter, int *err);
 cudaError_t launch_line_centres(const BurstDev &B, const Orbit &o, const CentreParams &cp,
                                 double *coef, cudaStream_t st);
+cudaError_t launch_line_centres_batch(const BurstDev *bursts, const CentreJob *jobs, int n,
+                                      int total, cudaStream_t st);
+cudaError_t launch_merge_scene(const BurstDev *bursts, int n, float2 *dst, long long dst_ld,
+                               int lines, int cols, cudaStream_t st);
 cudaError_t launch_count_terms(const BurstDev &B, unsigned long long *terms, int sms,
                                cudaStream_t st);
 cudaError_t launch_merge(float2 *dst, long long dst_ld, const float2 *src, long long src_ld,

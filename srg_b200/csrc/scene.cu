@@ -1,0 +1,381 @@
+// scene.cu -- reusable plans for batched scenes (srg_scene_* in srg_bp.h).
+//
+// A plan holds, in device memory, everything one pass over a set of bursts
+// needs besides the caller's inputs and outputs: the burst descriptors, one
+// TMA descriptor per burst, the orbit state vectors and centre parameters of
+// every burst, the per-line azimuth-centre parabolas and the work counter.
+// A pass is four launches -- azimuth centres of every line of every burst
+// (one launch), the counter reset, the persistent backprojection (one
+// launch for all bursts) and, when a scene raster is given, the ordered
+// merge of every burst into it (one launch).  On a non-default stream the
+// first pass is captured into a CUDA graph and later passes replay it.
+#include <cstring>
+#include <vector>
+
+#include "host_internal.h"
+
+using namespace srg;
+using namespace srg::detail;
+
+struct srg_scene {
+    int dev = -1;
+    int n = 0;
+    srg_bp_options opts{};
+    int kernel = -1;                 // index into kKernels
+    std::vector<srg_burst_desc> descs;
+    std::vector<BurstDev> hb;        // host copy (tiles depend on the kernel shape)
+    int total_tiles = 0;
+    int total_lines = 0;
+    int64_t terms = -1;
+    float2 *scene = nullptr;
+    long long scene_ld = 0;
+    int scene_lines = 0, scene_cols = 0;
+    // device memory owned by the plan
+    BurstDev *d_bursts = nullptr;
+    CUtensorMap *d_tmaps = nullptr;
+    CentreJob *d_jobs = nullptr;
+    double *d_coef = nullptr;
+    double *d_orbit = nullptr;
+    int *d_flags = nullptr;          // [0] work counter, [1] error word, [2..3] u64 term counter
+    cudaGraphExec_t graph = nullptr;
+    cudaStream_t graph_stream = nullptr;
+};
+
+namespace {
+
+#define SCK(call)                                                                     \
+    do {                                                                              \
+        cudaError_t e_ = (call);                                                      \
+        if (e_ != cudaSuccess)                                                        \
+            return fail(SRG_E_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));  \
+    } while (0)
+
+int alloc(void **p, size_t bytes) {
+    const size_t n = bytes < 256 ? 256 : bytes;
+    cudaError_t e = cudaMalloc(p, n);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return fail(SRG_E_NOMEM, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+    }
+    // zeroed: the flag words are read before any kernel has written them
+    if (cudaMemset(*p, 0, n) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(SRG_E_CUDA, "cudaMemset of plan memory failed");
+    }
+    return SRG_OK;
+}
+
+void drop_graph(srg_scene *s) {
+    if (s->graph) cudaGraphExecDestroy(s->graph);
+    s->graph = nullptr;
+    s->graph_stream = nullptr;
+}
+
+// (Re)build the burst table and TMA descriptors for kernel shape `idx`.
+int set_kernel(srg_scene *s, int idx) {
+    const KernelEntry &ke = kKernels[idx];
+    std::vector<CUtensorMap> hm(s->n);
+    int total = 0;
+    for (int i = 0; i < s->n; ++i) {
+        BurstDev &B = s->hb[i];
+        const int nx = B.lastpix_eff - B.firstpix + 1;
+        B.tiles_x = nx > 0 ? (nx + ke.shape.tx - 1) / ke.shape.tx : 0;
+        B.tiles_y = (B.nlines + ke.shape.ty - 1) / ke.shape.ty;
+        B.tile_base = total;
+        total += B.tiles_x * B.tiles_y;
+        std::memset(&hm[i], 0, sizeof(CUtensorMap));
+        B.tmap = make_tmap(B, ke.shape.window, ke.shape.chunk, &hm[i]) == 0 ? i : -1;
+    }
+    SCK(cudaMemcpy(s->d_bursts, s->hb.data(), sizeof(BurstDev) * s->n, cudaMemcpyHostToDevice));
+    SCK(cudaMemcpy(s->d_tmaps, hm.data(), sizeof(CUtensorMap) * s->n, cudaMemcpyHostToDevice));
+    s->total_tiles = total;
+    s->kernel = idx;
+    drop_graph(s);
+    return SRG_OK;
+}
+
+int enqueue_centres(srg_scene *s, cudaStream_t st) {
+    SCK(launch_line_centres_batch(s->d_bursts, s->d_jobs, s->n, s->total_lines, st));
+    return SRG_OK;
+}
+
+int enqueue_backprojection(srg_scene *s, cudaStream_t st) {
+    if (s->total_tiles == 0) return SRG_OK;
+    DevCtx *c = nullptr;
+    int rc = get_ctx(s->dev, &c);
+    if (rc) return rc;
+    const KernelEntry &ke = kKernels[s->kernel];
+    ensure_attrs(*c, s->kernel);
+    int per_sm = 0;
+    SCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ke.fn, ke.shape.threads, ke.smem));
+    if (per_sm < 1) return fail(SRG_E_UNSUPPORTED, "kernel shape %d does not fit an SM", s->kernel);
+    SCK(cudaMemsetAsync(s->d_flags, 0, sizeof(int), st));
+    SCK(launch_tiles(ke, std::min(s->total_tiles, per_sm * c->sms), ke.smem, st, s->d_bursts, s->n,
+                     s->total_tiles, s->d_tmaps, s->d_flags, s->d_flags + 1));
+    return SRG_OK;
+}
+
+int enqueue_pass(srg_scene *s, cudaStream_t st) {
+    int rc = enqueue_centres(s, st);
+    if (rc) return rc;
+    rc = enqueue_backprojection(s, st);
+    if (rc) return rc;
+    if (s->scene)
+        SCK(launch_merge_scene(s->d_bursts, s->n, s->scene, s->scene_ld, s->scene_lines,
+                               s->scene_cols, st));
+    return SRG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int srg_scene_create(const srg_burst_desc *bursts, int n, float *scene, int64_t scene_ld,
+                     int scene_lines, int scene_cols, const srg_bp_options *opts,
+                     srg_scene **out) {
+    if (!out) return fail(SRG_E_ARG, "null output handle");
+    *out = nullptr;
+    if (!bursts || n < 1) return fail(SRG_E_ARG, "no bursts");
+    if (scene && n > 256) return fail(SRG_E_ARG, "scene merge supports at most 256 bursts");
+    srg_bp_options o;
+    srg_bp_default_options(&o);
+    if (opts) o = *opts;
+    const KernelEntry *ke = pick_kernel(o.form, o.tile_cfg);
+    if (!ke) return fail(SRG_E_ARG, "no kernel for form %d shape %d", o.form, o.tile_cfg);
+    for (int i = 0; i < n; ++i) {
+        int rc = validate_desc(bursts[i]);
+        if (rc) return rc;
+        if (bursts[i].coef)
+            return fail(SRG_E_ARG, "burst %d: a scene plan solves its own azimuth centres (coef must be NULL)", i);
+        if (bursts[i].numstatevec < 4 || bursts[i].numstatevec > 4096)
+            return fail(SRG_E_ARG, "burst %d: numstatevec %d", i, bursts[i].numstatevec);
+    }
+    DevCtx *c = nullptr;
+    int rc = get_ctx(o.device, &c);
+    if (rc) return rc;
+    srg_scene *s = new srg_scene();
+    s->dev = c->dev;
+    s->n = n;
+    s->opts = o;
+    s->descs.assign(bursts, bursts + n);
+    s->scene = reinterpret_cast<float2 *>(scene);
+    s->scene_ld = scene_ld;
+    s->scene_lines = scene_lines;
+    s->scene_cols = scene_cols;
+    size_t lines = 0, orbit = 0;
+    for (int i = 0; i < n; ++i) {
+        lines += (size_t)bursts[i].nlines;
+        orbit += 7 * (size_t)bursts[i].numstatevec;
+    }
+    if ((rc = alloc((void **)&s->d_bursts, sizeof(BurstDev) * n)) ||
+        (rc = alloc((void **)&s->d_tmaps, sizeof(CUtensorMap) * n)) ||
+        (rc = alloc((void **)&s->d_jobs, sizeof(CentreJob) * n)) ||
+        (rc = alloc((void **)&s->d_coef, sizeof(double) * 3 * lines)) ||
+        (rc = alloc((void **)&s->d_orbit, sizeof(double) * orbit)) ||
+        (rc = alloc((void **)&s->d_flags, 64))) {
+        srg_scene_destroy(s);
+        return rc;
+    }
+    std::vector<double> horb(orbit);
+    std::vector<CentreJob> jobs(n);
+    s->hb.resize(n);
+    size_t lo = 0, oo = 0;
+    for (int i = 0; i < n; ++i) {
+        const srg_burst_desc &d = bursts[i];
+        const int k = d.numstatevec;
+        std::memcpy(&horb[oo], d.timeorbit, sizeof(double) * k);
+        std::memcpy(&horb[oo + k], d.xx, sizeof(double) * 3 * k);
+        std::memcpy(&horb[oo + 4 * k], d.vv, sizeof(double) * 3 * k);
+        CentreJob &J = jobs[i];
+        J.orbit = Orbit{s->d_orbit + oo, s->d_orbit + oo + k, s->d_orbit + oo + 4 * k, k};
+        J.cp.tmid = d.tmid;
+        for (int q = 0; q < 3; ++q) {
+            J.cp.xm[q] = d.xyz_mid[q];
+            J.cp.vm[q] = d.vel_mid[q];
+        }
+        J.cp.wvl = d.wvl;
+        J.cp.angc0 = d.angc0;
+        J.cp.angc1 = d.angc1;
+        J.cp.prf = d.prf;
+        J.cp.pi = ref_pi();
+        J.coef = s->d_coef + 3 * lo;
+        J.line_base = (int)lo;
+        s->hb[i] = make_burst_dev(d, J.coef);
+        lo += (size_t)d.nlines;
+        oo += 7 * (size_t)k;
+    }
+    s->total_lines = (int)lines;
+    if (cudaMemcpy(s->d_orbit, horb.data(), sizeof(double) * orbit, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(s->d_jobs, jobs.data(), sizeof(CentreJob) * n, cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaGetLastError();
+        srg_scene_destroy(s);
+        return fail(SRG_E_CUDA, "plan upload failed");
+    }
+    rc = set_kernel(s, kernel_index(ke));
+    if (rc) {
+        srg_scene_destroy(s);
+        return rc;
+    }
+    *out = s;
+    return SRG_OK;
+}
+
+int srg_scene_run(srg_scene *s, void *stream) {
+    if (!s) return fail(SRG_E_ARG, "null plan");
+    int rc = cudaSetDevice(s->dev) == cudaSuccess ? SRG_OK : fail(SRG_E_CUDA, "cudaSetDevice");
+    if (rc) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (st == nullptr) return enqueue_pass(s, st);  // the legacy stream cannot be captured
+    if (!s->graph || s->graph_stream != st) {
+        drop_graph(s);
+        // make sure attributes and lazily loaded kernels are settled outside capture
+        DevCtx *c = nullptr;
+        if ((rc = get_ctx(s->dev, &c))) return rc;
+        ensure_attrs(*c, s->kernel);
+        cudaGraph_t g = nullptr;
+        SCK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        rc = enqueue_pass(s, st);
+        cudaError_t e = cudaStreamEndCapture(st, &g);
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (e != cudaSuccess) return fail(SRG_E_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&s->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            s->graph = nullptr;
+            return fail(SRG_E_CUDA, "graph instantiation failed: %s", cudaGetErrorString(e));
+        }
+        s->graph_stream = st;
+    }
+    SCK(cudaGraphLaunch(s->graph, st));
+    return SRG_OK;
+}
+
+int srg_scene_run_stages(srg_scene *s, int stages, void *stream) {
+    if (!s) return fail(SRG_E_ARG, "null plan");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int rc = SRG_OK;
+    if (stages & 1) rc = enqueue_centres(s, st);
+    if (!rc && (stages & 2)) rc = enqueue_backprojection(s, st);
+    if (!rc && (stages & 4) && s->scene)
+        SCK(launch_merge_scene(s->d_bursts, s->n, s->scene, s->scene_ld, s->scene_lines,
+                               s->scene_cols, st));
+    return rc;
+}
+
+int srg_scene_sync(srg_scene *s, void *stream) {
+    if (!s) return fail(SRG_E_ARG, "null plan");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    SCK(cudaStreamSynchronize(st));
+    int h[2] = {0, 0};
+    SCK(cudaMemcpy(h, s->d_flags, sizeof h, cudaMemcpyDeviceToHost));
+    if (h[1]) {
+        cudaMemset(s->d_flags + 1, 0, sizeof(int));
+        return fail(SRG_E_TIMEOUT, "device error word 0x%x (TMA wait timed out)", h[1]);
+    }
+    return SRG_OK;
+}
+
+int srg_scene_terms(srg_scene *s, int64_t *terms) {
+    if (!s || !terms) return fail(SRG_E_ARG, "bad arguments");
+    if (s->terms < 0) {
+        DevCtx *c = nullptr;
+        int rc = get_ctx(s->dev, &c);
+        if (rc) return rc;
+        rc = enqueue_centres(s, 0);
+        if (rc) return rc;
+        unsigned long long *cnt = reinterpret_cast<unsigned long long *>(s->d_flags + 2);
+        SCK(cudaMemset(cnt, 0, sizeof(unsigned long long)));
+        for (int i = 0; i < s->n; ++i) SCK(launch_count_terms(s->hb[i], cnt, c->sms, 0));
+        unsigned long long h = 0;
+        SCK(cudaMemcpy(&h, cnt, sizeof h, cudaMemcpyDeviceToHost));
+        s->terms = (int64_t)h;
+    }
+    *terms = s->terms;
+    return SRG_OK;
+}
+
+int srg_scene_tune(srg_scene *s, int iters, int *best_cfg, double *best_ms) {
+    if (!s) return fail(SRG_E_ARG, "null plan");
+    if (iters < 1) iters = 3;
+    cudaStream_t st = nullptr;
+    SCK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int rc = enqueue_centres(s, st);
+    if (rc == SRG_OK && cudaStreamSynchronize(st) != cudaSuccess)
+        rc = fail(SRG_E_CUDA, "azimuth centres failed: %s", cudaGetErrorString(cudaGetLastError()));
+    int best = -1;
+    float best_t = 1e30f;
+    for (int idx = 0; idx < kNumKernels && rc == SRG_OK; ++idx) {
+        if (kKernels[idx].form != s->opts.form) continue;
+        if ((rc = set_kernel(s, idx))) break;
+        if ((rc = enqueue_backprojection(s, st))) break;  // warm-up
+        float tot = 0.f;
+        for (int it = 0; it < iters && rc == SRG_OK; ++it) {
+            cudaEventRecord(e0, st);
+            rc = enqueue_backprojection(s, st);
+            cudaEventRecord(e1, st);
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            tot += ms;
+        }
+        if (rc) break;
+        const float t = tot / iters;
+        if (t < best_t) {
+            best_t = t;
+            best = idx;
+        }
+    }
+    if (rc == SRG_OK && cudaStreamSynchronize(st) != cudaSuccess)
+        rc = fail(SRG_E_CUDA, "tuning launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(st);
+    if (rc) return rc;
+    if (best < 0) return fail(SRG_E_UNSUPPORTED, "no kernel shape of form %d", s->opts.form);
+    rc = set_kernel(s, best);
+    if (rc) return rc;
+    s->opts.tile_cfg = best;
+    if (best_cfg) *best_cfg = best;
+    if (best_ms) *best_ms = best_t;
+    return SRG_OK;
+}
+
+int srg_scene_set_shape(srg_scene *s, int tile_cfg) {
+    if (!s) return fail(SRG_E_ARG, "null plan");
+    const KernelEntry *ke = pick_kernel(s->opts.form, tile_cfg);
+    if (!ke) return fail(SRG_E_ARG, "no kernel for form %d shape %d", s->opts.form, tile_cfg);
+    s->opts.tile_cfg = tile_cfg;
+    return set_kernel(s, kernel_index(ke));
+}
+
+int srg_scene_set_form(srg_scene *s, int form, int tile_cfg) {
+    if (!s) return fail(SRG_E_ARG, "null plan");
+    const KernelEntry *ke = pick_kernel(form, tile_cfg);
+    if (!ke) return fail(SRG_E_ARG, "no kernel for form %d shape %d", form, tile_cfg);
+    s->opts.form = form;
+    s->opts.tile_cfg = tile_cfg;
+    return set_kernel(s, kernel_index(ke));
+}
+
+int srg_scene_shape(const srg_scene *s) { return s ? s->kernel : -1; }
+
+void srg_scene_destroy(srg_scene *s) {
+    if (!s) return;
+    drop_graph(s);
+    cudaFree(s->d_bursts);
+    cudaFree(s->d_tmaps);
+    cudaFree(s->d_jobs);
+    cudaFree(s->d_coef);
+    cudaFree(s->d_orbit);
+    cudaFree(s->d_flags);
+    delete s;
+}
+
+}  // extern "C"

@@ -85,10 +85,11 @@ class Burst:
     prf: float
     dem: Optional[np.ndarray] = None     # [demlength][demwidth] int16 (full DEM)
     targets: Optional[np.ndarray] = None  # [T][3] (line, pixel, amplitude) of point targets
+    pulses: int = 0   # pulse count when the samples live only on the device (burst has 0 rows)
 
     @property
     def rawdatalines(self) -> int:
-        return int(self.burst.shape[0])
+        return int(self.pulses or self.burst.shape[0])
 
     @property
     def samples(self) -> int:
@@ -290,13 +291,53 @@ def fbm_surface(rng, ny, nx, hurst, rms):
     return surf
 
 
-def volcano_dem(rng, ny, nx, peak=2500.0, base=0.0, radius_frac=0.45, hurst=0.8, rms=30.0):
-    yy, xx = np.mgrid[0:ny, 0:nx]
+def volcano_dem_torch(seed: int, ny, nx, device, peak=2500.0, base=0.0, radius_frac=0.45,
+                      hurst=0.8, rms=30.0):
+    """The same surface as volcano_dem, synthesised on a torch device (for
+    scene-sized grids); returns an int16 tensor on that device."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
     cy, cx = (ny - 1) / 2.0, (nx - 1) / 2.0
     rad = radius_frac * min(ny, nx) * 1.6
-    d = np.sqrt(((yy - cy) / 1.0) ** 2 + ((xx - cx) / 1.0) ** 2) / rad
-    cone = base + peak * np.clip(1.0 - d, 0.0, 1.0)
-    h = cone + fbm_surface(rng, ny, nx, hurst, rms)
+    yy = ((torch.arange(ny, device=device, dtype=torch.float32) - cy) / rad)[:, None]
+    xx = ((torch.arange(nx, device=device, dtype=torch.float32) - cx) / rad)[None, :]
+    h = base + peak * torch.clamp(1.0 - torch.sqrt(yy * yy + xx * xx), 0.0, 1.0)
+    ky = torch.fft.fftfreq(ny, device=device)[:, None]
+    kx = torch.fft.rfftfreq(nx, device=device)[None, :]
+    k = torch.sqrt(kx * kx + ky * ky)
+    k[0, 0] = 1.0
+    amp = k ** (-(hurst + 1.0))
+    amp[0, 0] = 0.0
+    ph = torch.complex(torch.randn(amp.shape, generator=g, device=device),
+                       torch.randn(amp.shape, generator=g, device=device))
+    surf = torch.fft.irfft2(amp * ph, s=(ny, nx))
+    surf = surf - surf.mean()
+    surf = surf * (rms / torch.clamp(surf.std(), min=1e-30))
+    return torch.clamp(torch.round(h + surf), -32768, 32767).to(torch.int16)
+
+
+def volcano_dem(rng, ny, nx, peak=2500.0, base=0.0, radius_frac=0.45, hurst=0.8, rms=30.0,
+                max_fbm_points: int = 4_000_000):
+    """Volcano cone (0..peak m) plus fBm roughness (Hurst `hurst`, `rms` m).
+    The fBm is synthesised at full resolution up to `max_fbm_points`, beyond
+    that on a coarser grid and interpolated bilinearly (its power at the
+    finest scales is negligible for H = 0.8)."""
+    cy, cx = (ny - 1) / 2.0, (nx - 1) / 2.0
+    rad = radius_frac * min(ny, nx) * 1.6
+    yy = ((np.arange(ny, dtype=np.float32) - cy) / rad)[:, None]
+    xx = ((np.arange(nx, dtype=np.float32) - cx) / rad)[None, :]
+    h = base + peak * np.clip(1.0 - np.sqrt(yy * yy + xx * xx), 0.0, 1.0)
+    f = 1
+    while (ny // f) * (nx // f) > max_fbm_points:
+        f *= 2
+    if f == 1:
+        rough = fbm_surface(rng, ny, nx, hurst, rms)
+    else:
+        from scipy import ndimage
+        coarse = fbm_surface(rng, -(-ny // f), -(-nx // f), hurst, rms).astype(np.float32)
+        rough = ndimage.zoom(coarse, f, order=1)[:ny, :nx]
+    h = h + rough
     return np.clip(np.rint(h), -32768, 32767).astype(np.int16)
 
 
@@ -567,3 +608,139 @@ def burst_from_arrays(a, samples: np.ndarray) -> Burst:
     b = Burst(burst=samples, **kw)
     b.dem = np.array(a["dem"], np.int16)
     return b
+
+
+# --------------------------------------------------------------------------
+# multi-burst scenes
+
+
+@dataclasses.dataclass
+class SceneGrid:
+    """A shared lat/lon grid and DEM for several bursts."""
+    firstlat: float
+    firstlon: float
+    spacing: float
+    width: int
+    length: int
+    dem: np.ndarray  # [length][width] int16
+
+
+def _burst_on_grid(grid: SceneGrid, orbit: CircularOrbit, tmid: float, pulses: int, samples: int,
+                   near_range: float, window, aperture: Optional[int] = None, wvl=WAVELENGTH,
+                   prf=PRF, fs=RANGE_FS) -> Burst:
+    """One burst of `pulses` lines centred at time tmid, whose latlons select
+    the pixel window ((line0, line1), (pix0, pix1)) of the shared grid."""
+    dtaz = 1.0 / prf
+    tstart = tmid - 0.5 * (pulses - 1) * dtaz
+    tend = tstart + (pulses - 1) * dtaz
+    t0 = math.floor((tstart - 30.0) / SV_SPACING) * SV_SPACING + SV_SPACING
+    timeorbit = t0 + SV_SPACING * np.arange(11, dtype=np.float64)
+    xx, vv = orbit.state(timeorbit)
+    ptime = tstart + np.arange(pulses, dtype=np.float64) * dtaz
+    sx, sv = interp_pulses(timeorbit, xx, vv, ptime)
+    sx, sv = quantise_positions(sx, sv)
+    xyz_mid, vel_mid = intp_orbit(timeorbit, xx, vv, 0.5 * (tstart + tend))
+    dmrg = C_LIGHT / 2.0 / fs
+    (l0, l1), (p0, p1) = window
+    sp = grid.spacing
+    latlons = np.array([grid.firstlat - (l1 + 0.25) * sp, grid.firstlat - (l0 + 0.25) * sp,
+                        grid.firstlon + (p0 + 0.25) * sp, grid.firstlon + (p1 + 0.25) * sp])
+    b = Burst(
+        burst=np.zeros((0, samples), np.complex64), satloc=np.ascontiguousarray(sx),
+        satvel=np.ascontiguousarray(sv), pulse_time=ptime, demwidth=grid.width,
+        demlength=grid.length, deltalat=-sp, deltalon=sp, firstlat=grid.firstlat,
+        firstlon=grid.firstlon, latlons=latlons, timeorbit=timeorbit,
+        xx=np.ascontiguousarray(xx), vv=np.ascontiguousarray(vv), rngstart=near_range,
+        rngend=near_range + (samples - 1) * dmrg, tstart=tstart, tend=tend,
+        tmid=0.5 * (tstart + tend), xyz_mid=np.ascontiguousarray(xyz_mid),
+        vel_mid=np.ascontiguousarray(vel_mid), dtaz=dtaz, dmrg=dmrg, wvl=wvl,
+        aperture=aperture if aperture is not None else aperture_points(sv, near_range, wvl, prf),
+        iaperture=0, angc0=0.0, angc1=0.0, prf=prf)
+    b.dem = grid.dem
+    b.pulses = pulses
+    return b
+
+
+def iw_scene(seed: int = 1003, nswaths: int = 3, nbursts: int = 9,
+             samples=(18000, 21500, 25600), near=(800.0e3, 838.0e3, 884.0e3),
+             pulses=(1380, 1620), widths=(2000, 2600), lengths=(1000, 1300),
+             spacing: float = 1e-4, burst_step_s: float = 0.45, lat0: float = 19.4,
+             dem_kind: str = "volcano", device=None):
+    """Configuration 3: a full IW scene -- `nswaths` subswaths x `nbursts`
+    bursts of uneven size (P uniform in `pulses`, S per subswath), each mapped
+    to its own overlapping sub-grid (W in `widths`, L in `lengths`) of one
+    shared grid and DEM.  Returns (SceneGrid, [Burst]) in acquisition order
+    (burst-major, subswath-minor).  Burst samples are left empty (shape
+    [0][S]); the workload builder fills them on the device.  With a torch
+    `device` the DEM is synthesised there (grid.dem is then a device tensor)."""
+    rng = np.random.default_rng(seed)
+    inc = math.radians(ORBIT_INCL_DEG)
+    T0 = 43200.25
+    u0 = math.asin(math.sin(math.radians(lat0)) / math.sin(inc))
+    orbit = CircularOrbit(u0=u0, epoch=T0)
+    dmrg = C_LIGHT / 2.0 / RANGE_FS
+    plan = []
+    for ib in range(nbursts):
+        for isw in range(nswaths):
+            tm = T0 + (ib - (nbursts - 1) / 2.0) * burst_step_s
+            P = int(rng.integers(pulses[0], pulses[1] + 1))
+            S = int(samples[isw])
+            r0 = float(near[isw])
+            smid, vmid = orbit.state(np.array([tm]))
+            pc = zero_doppler_point(smid[0], vmid[0], r0 + 0.5 * (S - 1) * dmrg, 1000.0)
+            clat, clon, _ = ecef_to_llh(pc)
+            W = int(rng.integers(widths[0], widths[1] + 1))
+            L = int(rng.integers(lengths[0], lengths[1] + 1))
+            plan.append((tm, P, S, r0, float(clat), float(clon), W, L))
+    lat_hi = max(p[4] + 0.5 * p[7] * spacing for p in plan) + 20 * spacing
+    lat_lo = min(p[4] - 0.5 * p[7] * spacing for p in plan) - 20 * spacing
+    lon_lo = min(p[5] - 0.5 * p[6] * spacing for p in plan) - 20 * spacing
+    lon_hi = max(p[5] + 0.5 * p[6] * spacing for p in plan) + 20 * spacing
+    length = int(math.ceil((lat_hi - lat_lo) / spacing)) + 1
+    width = int(math.ceil((lon_hi - lon_lo) / spacing)) + 1
+    if dem_kind == "volcano" and device is not None:
+        dem = volcano_dem_torch(int(rng.integers(2**31)), length, width, device, radius_frac=0.35)
+    elif dem_kind == "volcano":
+        dem = volcano_dem(rng, length, width, radius_frac=0.35)
+    else:
+        dem = np.full((length, width), 1000, np.int16)
+    grid = SceneGrid(firstlat=lat_hi, firstlon=lon_lo, spacing=spacing, width=width,
+                     length=length, dem=dem)
+    bursts = []
+    for tm, P, S, r0, clat, clon, W, L in plan:
+        cl = int(round((grid.firstlat - clat) / spacing))
+        cp = int(round((clon - grid.firstlon) / spacing))
+        l0 = max(0, cl - L // 2)
+        p0 = max(0, cp - W // 2)
+        win = ((l0, min(length - 1, l0 + L - 1)), (p0, min(width - 1, p0 + W - 1)))
+        bursts.append(_burst_on_grid(grid, orbit, tm, P, S, r0, win))
+    return grid, bursts
+
+
+def mini_scene(seed: int = 21, width: int = 64, length: int = 60, spacing: float = 0.0002):
+    """Three small bursts on one shared grid, for tests: consecutive in time
+    (overlapping output windows), uneven pulse and sample counts (one odd),
+    integer-valued samples (``mini_samples``).  Returns (SceneGrid, [Burst])."""
+    rng = np.random.default_rng([seed, 3])
+    inc = math.radians(ORBIT_INCL_DEG)
+    T0 = 43200.25
+    orbit = CircularOrbit(u0=math.asin(math.sin(math.radians(19.4)) / math.sin(inc)), epoch=T0)
+    dmrg = C_LIGHT / 2.0 / RANGE_FS
+    smid, vmid = orbit.state(np.array([T0]))
+    pc = zero_doppler_point(smid[0], vmid[0], 800.0e3, 200.0)
+    clat, clon, _ = ecef_to_llh(pc)
+    grid = SceneGrid(firstlat=float(clat) + 0.5 * (length - 1) * spacing,
+                     firstlon=float(clon) - 0.5 * (width - 1) * spacing, spacing=spacing,
+                     width=width, length=length,
+                     dem=(150 + 2 * np.arange(width)[None, :] + np.arange(length)[:, None] +
+                          rng.integers(-15, 16, (length, width))).astype(np.int16))
+    specs = [(-0.05, 300, 384, ((4, 40), (3, 58))), (0.0, 320, 401, ((14, 50), (6, 63))),
+             (0.05, 280, 416, ((22, 59), (0, 55)))]
+    bursts = []
+    for i, (dt, P, S, win) in enumerate(specs):
+        b = _burst_on_grid(grid, orbit, T0 + dt, P, S, 800.0e3 - 0.5 * (S - 1) * dmrg, win,
+                           aperture=96)
+        b.burst = mini_samples(seed * 10 + i, P, S)
+        b.pulses = 0
+        bursts.append(b)
+    return grid, bursts

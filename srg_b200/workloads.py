@@ -30,6 +30,8 @@ class Workload:
     terms: int               # exact executed-term count of all bursts
     setup_s: float
     description: str
+    raster: object = None    # scene raster (device) the bursts merge into, if any
+    grid: object = None      # scene.SceneGrid of a multi-burst scene
 
     def descs_bytes(self):
         """Bytes a host-resident copy of the step inputs/outputs moves."""
@@ -83,3 +85,65 @@ def config1(device="cuda", seed: int = 1001, forward: bool = True) -> Workload:
     return Workload("c1", [db], [coef], terms, time.time() - t0,
                     "IW1 burst 1500x21000 complex64 -> 2400x1200 grid at 1e-4 deg, volcano DEM, "
                     "forward-projected scatterers + 200 targets at +30 dB")
+
+
+def _add_targets(db: api.DeviceBurst, refl_buf, rng, ntargets: int, amp: float):
+    """Forward-project `ntargets` point targets at random pixels of the burst
+    window into db.burst (accumulates)."""
+    import torch
+    b = db.b
+    dev = db.out.device
+    refl = refl_buf[:db.nlines]
+    refl.zero_()
+    lines = rng.integers(0, db.nlines, ntargets)
+    pix = rng.integers(max(db.firstpix, 0), min(db.lastpix, b.demwidth - 1) + 1, ntargets)
+    refl[torch.from_numpy(lines).to(dev), torch.from_numpy(pix).to(dev)] = amp
+    satvel = torch.from_numpy(np.ascontiguousarray(b.satvel)).to(dev)
+    api.forward_project(db, refl, satvel)
+
+
+def config3(device="cuda", seed: int = 1003, ntargets: int = 200, target_db: float = 30.0,
+            form=None) -> Workload:
+    """A full IW scene: 3 subswaths x 9 bursts of uneven size (P uniform in
+    1,380-1,620; S = 18,000 / 21,500 / 25,600), each mapped to its own
+    overlapping sub-grid (2,000-2,600 x 1,000-1,300 at 1e-4 deg) of a shared
+    volcano DEM, merged in burst order into one scene raster.  Range lines:
+    circular complex Gaussian clutter (unit power per sample) plus
+    forward-projected point targets at +30 dB."""
+    import torch
+    from . import _lib
+    t0 = time.time()
+    grid, bursts = scene.iw_scene(seed=seed, device=device)
+    dem_dev = grid.dem
+    rng = np.random.default_rng(seed)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    maxl = 0
+    dbs = []
+    for b in bursts:
+        P, S = b.rawdatalines, b.samples
+        bt = torch.complex(torch.randn((P, S), generator=gen, device=device),
+                           torch.randn((P, S), generator=gen, device=device)) * (1.0 / np.sqrt(2.0))
+        db = api.to_device(b, device=device, burst_tensor=bt, dem_tensor=dem_dev, narrow_out=True)
+        maxl = max(maxl, db.nlines)
+        dbs.append(db)
+    refl = torch.zeros((maxl, grid.width), dtype=torch.complex64, device=device)
+    amp = 10.0 ** (target_db / 20.0)
+    for db in dbs:
+        _add_targets(db, refl, rng, ntargets, amp)
+    del refl
+    raster = torch.zeros((grid.length, grid.width), dtype=torch.complex64, device=device)
+    torch.cuda.synchronize(device)
+    sc = api.Scene(dbs, raster=raster, form=_lib.FORM_SPLIT if form is None else form)
+    terms = sc.terms()
+    wl = Workload("c3", dbs, [], terms, time.time() - t0,
+                  "IW scene: 3 subswaths x 9 bursts (P 1380-1620, S 18000/21500/25600 complex64, "
+                  f"{sum(db.burst.numel() * 8 for db in dbs) / 1e9:.2f} GB), sub-grids 2000-2600 x "
+                  f"1000-1300 at 1e-4 deg on a shared {grid.width}x{grid.length} volcano DEM, "
+                  "merged in burst order", raster=raster, grid=grid)
+    wl.plan = sc
+    # host copy of the shared DEM for the file-based entry
+    host_dem = dem_dev.cpu().numpy()
+    for b in bursts:
+        b.dem = host_dem
+    return wl
