@@ -435,7 +435,7 @@ def main():
                    "terms_per_step_per_gpu": wl.terms,
                    "l2": "range lines of every burst > 126 MB L2; no flush between steps",
                    "parallelism": f"replicas x{world} (one workload per GPU)",
-                   "kernel_shapes": {k: _lib.tile_configs()[v[0]][2:] for k, v in tuned.items()},
+                   "kernel_shapes": {k: _lib.tile_config_name(v[0]) for k, v in tuned.items()},
                    "step": ("one graph replay: azimuth centres of every line, one persistent "
                             "backprojection launch for all bursts, ordered merge into the scene raster")
                    if args.workload == "c3" else "azimuth centres + backprojection of one burst"},

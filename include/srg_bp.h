@@ -234,6 +234,8 @@ int srg_measure_fma_peak(int fp64, double *tflops);
 int srg_tile_config_count(void);
 int srg_tile_config(int idx, int *tile_x, int *tile_y, int *threads, int *chunk,
                     int *window);
+/* Human-readable kernel template and shape of shape `idx` ("" if none). */
+const char *srg_tile_config_name(int idx);
 
 /* Synthetic-scene support: forward-project a per-pixel reflectivity field
  * (complex64, [nlines][dem_ld-aligned W] of the burst's grid, device) into

@@ -87,6 +87,7 @@ _SIGS = {
     "srg_scene_destroy": (None, [C.c_void_p]),
     "srg_tile_config_count": (C.c_int, []),
     "srg_tile_config": (C.c_int, [C.c_int, _ip, _ip, _ip, _ip, _ip]),
+    "srg_tile_config_name": (C.c_char_p, [C.c_int]),
     "srg_forward_project_device": (C.c_int, [C.POINTER(BurstDesc), C.c_void_p, C.c_int64, C.c_void_p,
                                              C.c_double, C.c_void_p]),
     "srg_azimuth_compress": (C.c_int, [
@@ -138,6 +139,10 @@ def measure_fma_peak(fp64: bool) -> float:
     v = C.c_double()
     check(lib().srg_measure_fma_peak(1 if fp64 else 0, C.byref(v)))
     return float(v.value)
+
+
+def tile_config_name(idx: int) -> str:
+    return lib().srg_tile_config_name(idx).decode()
 
 
 def tile_configs():

@@ -341,6 +341,11 @@ void srg_set_default_options(const srg_bp_options *o) {
 
 int srg_tile_config_count(void) { return kNumKernels; }
 
+const char *srg_tile_config_name(int idx) {
+    if (idx < 0 || idx >= kNumKernels) return "";
+    return kKernels[idx].name;
+}
+
 int srg_tile_config(int idx, int *tile_x, int *tile_y, int *threads, int *chunk, int *window) {
     if (idx < 0 || idx >= kNumKernels) return fail(SRG_E_ARG, "shape index %d", idx);
     const TileShape &s = kKernels[idx].shape;

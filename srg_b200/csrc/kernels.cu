@@ -258,26 +258,32 @@ cudaError_t launch_fma_peak(int fp64, int blocks, int iters, void *sink, cudaStr
     X(FORM_FP64, 32, 8, 128, 32, 160)
 
 #define SRG_WS_SHAPES(X)                    \
+    X(FORM_SPLIT, 32, 8, 4, 31, 2, 128, 3)  \
     X(FORM_SPLIT, 32, 8, 4, 16, 3, 128, 3)  \
     X(FORM_SPLIT, 32, 8, 4, 16, 3, 128, 4)  \
     X(FORM_SPLIT, 32, 8, 4, 16, 2, 128, 3)  \
     X(FORM_SPLIT, 32, 8, 4, 24, 3, 128, 3)  \
-    X(FORM_SPLIT, 32, 8, 4, 31, 2, 128, 3)  \
     X(FORM_SPLIT, 16, 16, 4, 16, 3, 96, 3)  \
-    X(FORM_SPLIT, 32, 16, 4, 16, 3, 144, 2) \
+    X(FORM_SPLIT, 32, 16, 4, 16, 3, 144, 2)
+
+#define SRG_WS_FP64_SHAPES(X)               \
     X(FORM_FP64, 32, 4, 4, 16, 2, 128, 3)   \
     X(FORM_FP64, 32, 8, 4, 16, 2, 128, 2)
 
 #define SRG_ENTRY(F, TXv, TYv, NTv, CKv, WBv)                                                   \
     {F, {TXv, TYv, NTv, CKv, WBv}, params_bytes<F, CKv>() + 1024 + CKv * WBv * 8,               \
-     (const void *)bp_tiles<F, TXv, TYv, NTv, CKv>},
+     (const void *)bp_tiles<F, TXv, TYv, NTv, CKv>,                                             \
+     "bp_tiles<" #F "," #TXv "x" #TYv ",threads " #NTv ",chunk " #CKv ",window " #WBv ">"},
 #define SRG_WS_ENTRY(F, TXv, TYv, NCv, CKv, NSv, WBv, MBv)                                      \
     {F, {TXv, TYv, (NCv + 1) * 32, CKv, WBv}, ws_smem_bytes<F, CKv, NSv>(WBv),                  \
-     (const void *)bp_ws<F, TXv, TYv, NCv, CKv, NSv, MBv>},
+     (const void *)bp_ws<F, TXv, TYv, NCv, CKv, NSv, MBv>,                                      \
+     "bp_ws<" #F "," #TXv "x" #TYv ",consumer warps " #NCv ",chunk " #CKv ",stages " #NSv       \
+     ",window " #WBv ",min blocks " #MBv ">"},
 
-// The warp-specialised shapes come first: the first shape of a form is its
-// default.
-const KernelEntry kKernels[] = {SRG_WS_SHAPES(SRG_WS_ENTRY) SRG_SHAPES(SRG_ENTRY)};
+// The first shape of a form is its default: the fastest measured on the
+// B200 (warp-specialised for the split form, first generation for FP64).
+const KernelEntry kKernels[] = {SRG_WS_SHAPES(SRG_WS_ENTRY) SRG_SHAPES(SRG_ENTRY)
+                                    SRG_WS_FP64_SHAPES(SRG_WS_ENTRY)};
 const int kNumKernels = sizeof(kKernels) / sizeof(kKernels[0]);
 
 cudaError_t launch_tiles(const KernelEntry &e, int grid, size_t smem, cudaStream_t st,

@@ -26,6 +26,7 @@ struct KernelEntry {
     TileShape shape;   // threads = block size
     int smem;          // dynamic shared memory bytes
     const void *fn;
+    const char *name;  // template and shape, for reports
 };
 
 extern const KernelEntry kKernels[];
