@@ -208,7 +208,7 @@ def e2e_dropin(torch, wl, steps, form):
                 fl, ll, fp, lp = api.limits(db.b)
                 nl = ll - fl + 1
                 ncols = max(0, min(lp, db.b.demwidth - 1) - fp + 1)
-                h2d += host.numel() * 8 + db.b.rawdatalines * 24 + nl * db.b.demwidth * 2
+                h2d += host.numel() * 8 + db.b.rawdatalines * 24 + nl * ncols * 2
                 d2h += nl * ncols * 8
             for db, host in zip(wl.bursts, hosts):   # warm-up
                 api.azimuth_compress_files(db.b, fd_geo, fd_dem, burst=host.numpy())

@@ -32,20 +32,39 @@
 //   exactly once per pixel and chunk, with its slope g = (d dr2 / dw) * dw_mid,
 //   and folded into the two accumulators, which then advance by dw + g: per
 //   term only the increment, two accumulations, the bin and the phase remain.
+// * Closed forms (split form, chunks whose taps all lie in the staged window;
+//   at the aperture edges with a per-term azimuth-window test): over one chunk R_c is a
+//   quadratic in the pulse index and u_{k+1} - u_k is linear in it (a smooth
+//   orbit leaves residuals of ~1e-10 m), so the bin and the phase of every
+//   term are quadratics in the pulse index whose coefficients each pixel
+//   derives once per chunk; a term then costs two FMAs for each, with no
+//   recurrence carried from term to term.  The producer fits R_c and the
+//   increments and checks the fits at every pulse of the chunk; a chunk whose
+//   bound exceeds kPolyTolRad of phase (an orbit with a kink, a chunk shorter
+//   than three pulses) takes the per-pulse form instead.  The tap index comes
+//   from an add rounded toward -inf (floor in the mantissa), which keeps the
+//   conversion pipe free for the sine and cosine.
 #pragma once
 #include <climits>
 #include <cuda.h>
+#include <type_traits>
 #include "bp_kernel.cuh"
 
 namespace srg {
 
 struct StageHdr {
     int x0;        // first staged bin
-    int fast;      // 1: interior chunk (no per-term predicates)
+    int fast;      // 1: every tap of the chunk lies in the staged window and the range limits
+    int interior;  // 1: the chunk lies inside every formed pixel's azimuth window
+    int poly;      // 1: the closed forms below hold to < kPolyTolRad of phase
     float tlo, thi;       // range test in window-relative bins (general path)
     float dmx, dmy, dmz;  // u_{k+1} - u_k at the chunk's middle pulse
     float inv2R, c2;      // 1/(2 R_c) and 1/(2 R_c^2) at the chunk's middle pulse
-    int pad[3];
+    // closed forms over the chunk in the centred pulse index f = j - (nk-1)/2:
+    float r0, r1, r2;     // window-relative bin of R_c = r0 + f r1 + f^2 r2
+    float p0, p1, p2;     // reference phase (rad) = p0 + f p1 + f^2 p2, p0 in [-pi, pi]
+    float u0x, u0y, u0z;  // u_{j+1} - u_j = u0 + j us (j = pulse index within the chunk)
+    float usx, usy, usz;
 };
 
 struct CtlWS {
@@ -62,6 +81,15 @@ constexpr double kTwoPi = 6.283185307179586476925;
 constexpr float kTwoPiHi = 6.28318548202514648f;     // float(2 pi)
 constexpr float kTwoPiLo = -1.74845553e-7f;          // 2 pi - float(2 pi)
 constexpr float kInvTwoPi = 0.159154943091895336f;
+// Largest phase error (rad) the producer accepts from the chunk's closed forms
+// (quadratic R_c, linear look-vector increments) before it falls back to the
+// per-pulse form; the fit residuals of a smooth orbit are ~1e-8 rad.
+constexpr double kPolyTolRad = 1e-4;
+
+// floor(t) for -2^22 <= t < 2^22 without the conversion pipe: adding 1.5 * 2^23
+// rounded toward -inf leaves floor(t) in the low mantissa bits.
+constexpr float kFloorMagic = 12582912.f;
+constexpr int kFloorMagicBits = 0x4B400000;
 
 // Per-pulse parameters of one chunk (split: 2 x float4; FP64: satloc + pad).
 template <int FORM>
@@ -378,10 +406,89 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                 const int devmax = __reduce_max_sync(0xffffffffu, __float_as_int(dev));
                 const int x0 = (lo + bmin) & ~1;  // TMA: x * 8 bytes on a 16-byte boundary
                 const int need = hi + bmax - x0 + 1;
-                const double Rmid = __shfl_sync(0xffffffffu, R, nk / 2);
-                const double mdx = __shfl_sync(0xffffffffu, nx - ex, nk / 2);
-                const double mdy = __shfl_sync(0xffffffffu, ny - ey, nk / 2);
-                const double mdz = __shfl_sync(0xffffffffu, nz - ez, nk / 2);
+                // Everything the stage needs is reduced to floats before the stage
+                // wait, so that no FP64 value stays live across it.
+                StageHdr hv;
+                hv.x0 = x0;
+                {
+                    const bool interior = k0 >= azs_max && k0 + nk <= aze_min;
+                    const bool rangeok = x0 >= 1 && (double)(x0 + WB) <= rmaxb - 1.0;
+                    const bool bounded = __int_as_float(devmax) < 0.5f;
+                    hv.fast = (rangeok && bounded && need <= WB) ? 1 : 0;
+                    hv.interior = interior ? 1 : 0;
+                }
+                hv.tlo = (float)(-(double)x0);
+                hv.thi = __double2float_rn(rmaxb - (double)x0);
+                {
+                    const double Rmid = __shfl_sync(0xffffffffu, R, nk / 2);
+                    hv.dmx = __double2float_rn(__shfl_sync(0xffffffffu, nx - ex, nk / 2));
+                    hv.dmy = __double2float_rn(__shfl_sync(0xffffffffu, ny - ey, nk / 2));
+                    hv.dmz = __double2float_rn(__shfl_sync(0xffffffffu, nz - ez, nk / 2));
+                    hv.inv2R = __double2float_rn(0.5 / Rmid);
+                    hv.c2 = __double2float_rn(0.5 / (Rmid * Rmid));
+                }
+                hv.poly = 0;
+                hv.r0 = hv.r1 = hv.r2 = hv.p0 = hv.p1 = hv.p2 = 0.f;
+                hv.u0x = hv.u0y = hv.u0z = hv.usx = hv.usy = hv.usz = 0.f;
+                float4 pa = make_float4(0.f, 0.f, 0.f, 0.f);
+                float pb = 0.f;
+                if constexpr (FORM == FORM_SPLIT) {
+                    {
+                        const double q = R * B.K;
+                        pa = make_float4(__double2float_rn(nx - ex), __double2float_rn(ny - ey),
+                                         __double2float_rn(nz - ez), __double2float_rn(kTwoPi * (q - rint(q))));
+                        pb = __double2float_rn(rbabs - (double)x0);
+                    }
+                    // closed forms: R_c - R_c(0) quadratic through pulses 0, jm, jb
+                    // (Newton form, recentred on jc); look-vector increments linear
+                    // through 0 and jb; each checked against every pulse of the
+                    // chunk.  The offsets from pulse 0 are < ~1 m, so FP32 carries
+                    // them to ~1e-7 m, well inside the tolerance.
+                    const int jm = (nk - 1) >> 1, jb = nk - 1;
+                    const float jc = 0.5f * (float)jb;
+                    const double Ra = __shfl_sync(0xffffffffu, R, 0);
+                    const float dR = (float)(R - Ra);
+                    const float dRm = __shfl_sync(0xffffffffu, dR, jm);
+                    const float dRb = __shfl_sync(0xffffffffu, dR, jb);
+                    float c0 = 0.f, c1 = 0.f, c2 = 0.f;
+                    float u0[3], us[3];
+                    const float pq[3] = {pa.x, pa.y, pa.z};
+                    if (nk >= 3) {
+                        const float D1 = dRm / (float)jm;
+                        const float D2 = ((dRb - dRm) / (float)(jb - jm) - D1) / (float)jb;
+                        c2 = D2;
+                        c1 = fmaf(D2, 2.f * jc - (float)jm, D1);
+                        c0 = fmaf(jc * (jc - (float)jm), D2, jc * D1);
+                    }
+                    const float fj = (float)lane - jc;
+                    float err = fabsf(dR - fmaf(fmaf(c2, fj, c1), fj, c0));
+                    const float ij = nk >= 3 ? 1.f / (float)jb : 0.f;
+                    const float dmaxc = (float)nk * __int_as_float(ctl.dmax_bits);
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        u0[c] = __shfl_sync(0xffffffffu, pq[c], 0);
+                        us[c] = (__shfl_sync(0xffffffffu, pq[c], jb) - u0[c]) * ij;
+                        // w error accumulated over the chunk: nk * step error * max |d|
+                        err = fmaf(fabsf(pq[c] - fmaf((float)lane, us[c], u0[c])), dmaxc, err);
+                    }
+                    const double cR = Ra + (double)c0;
+                    const double q = cR * B.K;
+                    hv.r0 = __double2float_rn((cR - B.rngstart) * B.inv_dmrg - (double)x0);
+                    hv.r1 = __double2float_rn((double)c1 * B.inv_dmrg);
+                    hv.r2 = __double2float_rn((double)c2 * B.inv_dmrg);
+                    hv.p0 = __double2float_rn(kTwoPi * (q - rint(q)));
+                    hv.p1 = __double2float_rn(kTwoPi * B.K * (double)c1);
+                    hv.p2 = __double2float_rn(kTwoPi * B.K * (double)c2);
+                    hv.u0x = u0[0];
+                    hv.u0y = u0[1];
+                    hv.u0z = u0[2];
+                    hv.usx = us[0];
+                    hv.usy = us[1];
+                    hv.usz = us[2];
+                    const float resmax =
+                        __int_as_float(__reduce_max_sync(0xffffffffu, __float_as_int(act ? err : 0.f)));
+                    hv.poly = (nk >= 3 && (double)resmax * kTwoPi * B.K < kPolyTolRad) ? 1 : 0;
+                }
                 if (!mbar_wait_backoff(&ctl.empty[s], (r & 1) ^ 1)) {
                     ctl.abort = 1;
                     break;
@@ -396,29 +503,12 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                 }
                 if constexpr (FORM == FORM_SPLIT) {
                     if (lane < CK) {
-                        const double q = R * B.K;
-                        const double ref = kTwoPi * (q - rint(q));
                         PP &p = prm[s * CK + lane];
-                        p.a = make_float4(__double2float_rn(nx - ex), __double2float_rn(ny - ey),
-                                          __double2float_rn(nz - ez), __double2float_rn(ref));
-                        p.b = make_float4(__double2float_rn(rbabs - (double)x0), 0.f, 0.f, 0.f);
+                        p.a = pa;
+                        p.b = make_float4(pb, 0.f, 0.f, 0.f);
                     }
                 }
-                if (lane == 0) {
-                    StageHdr &h = hdr[s];
-                    h.x0 = x0;
-                    const bool interior = k0 >= azs_max && k0 + nk <= aze_min;
-                    const bool rangeok = x0 >= 1 && (double)(x0 + WB) <= rmaxb - 1.0;
-                    const bool bounded = __int_as_float(devmax) < 0.5f;
-                    h.fast = (interior && rangeok && bounded && need <= WB) ? 1 : 0;
-                    h.tlo = (float)(-(double)x0);
-                    h.thi = __double2float_rn(rmaxb - (double)x0);
-                    h.dmx = __double2float_rn(mdx);
-                    h.dmy = __double2float_rn(mdy);
-                    h.dmz = __double2float_rn(mdz);
-                    h.inv2R = __double2float_rn(0.5 / Rmid);
-                    h.c2 = __double2float_rn(0.5 / (Rmid * Rmid));
-                }
+                if (lane == 0) hdr[s] = hv;
                 if (!use_tma) {
                     // no TMA descriptor for this burst: stage the window with plain loads
                     float2 *w = samp0 + (size_t)s * CK * WB;
@@ -457,6 +547,81 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                 if constexpr (FORM == FORM_SPLIT) {
                     const float invd = B.inv_dmrg_f;
                     const float Kr = (float)(kTwoPi * B.K);
+                  if (h.fast && h.poly) {
+                    // Closed forms.  Within the chunk the pixel's range offset from
+                    // R_c advances by dw_j = d.(u0 + j us) + g (g: slope of the folded
+                    // second-order term), so uacc_j = dwa + dr2_0 + sum_{i<j} dw_i is
+                    // a quadratic in j; with R_c's quadratic the bin and the phase are
+                    // quadratics in f = j - jc, evaluated per term in two FMAs each.
+                    const float jc = 0.5f * (float)(nk - 1);
+                    const float jmid = (float)(nk >> 1);
+                    float T0[M], T1[M], T2[M], P0[M], P1[M], P2[M];
+#pragma unroll
+                    for (int m = 0; m < M; ++m) {
+                        const float w0 = whi[m] + dwa[m];
+                        const float n0 = fmaf(-w0, w0, dd[m]);
+                        const float q0 = fmaf(-w0, h.c2, h.inv2R);
+                        const float dr0 = n0 * q0;
+                        const float a1 = fmaf(d[m][0], h.u0x, fmaf(d[m][1], h.u0y, d[m][2] * h.u0z));
+                        const float bq = fmaf(d[m][0], h.usx, fmaf(d[m][1], h.usy, d[m][2] * h.usz));
+                        const float g = fmaf(-2.f * w0, q0, -n0 * h.c2) * fmaf(bq, jmid, a1);
+                        const float A = a1 + g;
+                        const float U2 = 0.5f * bq;
+                        const float U1 = fmaf(bq, jc - 0.5f, A);
+                        const float V0 = fmaf(U2, jc * jc - jc, fmaf(A, jc, dr0));
+                        T0[m] = fmaf(whi[m] + (dwa[m] + V0), invd, h.r0);
+                        T1[m] = fmaf(U1, invd, h.r1);
+                        T2[m] = fmaf(U2, invd, h.r2);
+                        float p0 = fmaf(Kr, V0, cph[m] + h.p0);
+                        const float nr = rintf(p0 * kInvTwoPi);
+                        P0[m] = fmaf(-nr, kTwoPiLo, fmaf(-nr, kTwoPiHi, p0));
+                        P1[m] = fmaf(Kr, U1, h.p1);
+                        P2[m] = fmaf(Kr, U2, h.p2);
+                        // state at the next chunk: sum of d.(u0 + j us) over the chunk
+                        const float S = (float)nk * fmaf(bq, jc, a1);
+                        dwa[m] += S;
+                        cph[m] = fmaf(Kr, S, cph[m]);
+                    }
+                    // edge chunks add the exact azimuth-window test of every term
+                    auto terms = [&](auto masked) {
+                        constexpr bool MASKED = decltype(masked)::value;
+                        int ja[M], nj[M];
+#pragma unroll
+                        for (int m = 0; m < M; ++m) {
+                            ja[m] = max(azs[m] - k0, 0);
+                            nj[m] = max(min(aze[m] - k0, nk) - ja[m], 0);
+                        }
+                        float f = -jc;
+#pragma unroll 2
+                        for (int j = 0; j < nk; ++j, f += 1.f) {
+                            const float2 *row = win + j * WB;
+#pragma unroll
+                            for (int m = 0; m < M; ++m) {
+                                const float t = fmaf(fmaf(T2[m], f, T1[m]), f, T0[m]);
+                                const float ph = fmaf(fmaf(P2[m], f, P1[m]), f, P0[m]);
+                                const float tm = __fadd_rd(t, kFloorMagic);
+                                const float fr = t - (tm - kFloorMagic);
+                                // proven in range by the producer; clamped for memory safety
+                                const unsigned ic = min((unsigned)(__float_as_int(tm) - kFloorMagicBits),
+                                                        (unsigned)(WB - 2));
+                                const float2 s0 = row[ic], s1 = row[ic + 1];
+                                float vr = fmaf(fr, s1.x - s0.x, s0.x);
+                                float vi = fmaf(fr, s1.y - s0.y, s0.y);
+                                if constexpr (MASKED) {
+                                    const bool ok = (unsigned)(j - ja[m]) < (unsigned)nj[m];
+                                    vr = ok ? vr : 0.f;
+                                    vi = ok ? vi : 0.f;
+                                }
+                                float sn, cs;
+                                __sincosf(ph, &sn, &cs);
+                                accr[m] = fmaf(vr, cs, fmaf(-vi, sn, accr[m]));
+                                acci[m] = fmaf(vr, sn, fmaf(vi, cs, acci[m]));
+                            }
+                        }
+                    };
+                    if (h.interior) terms(std::false_type{});
+                    else terms(std::true_type{});
+                  } else {
                     // per pixel and chunk: second-order term and its slope, folded
                     // into the accumulators (uacc = dwa + dr2, cphp = cph + Kr dr2)
                     float uacc[M], cphp[M], gsl[M], dr0[M];
@@ -471,7 +636,7 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                         uacc[m] = dwa[m] + dr0[m];
                         cphp[m] = fmaf(dr0[m], Kr, cph[m]);
                     }
-                    if (h.fast) {
+                    if (h.fast && h.interior) {
                         // consecutive pulses share only the two accumulators, so
                         // unrolling gives the scheduler independent terms
 #pragma unroll 2
@@ -486,10 +651,11 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                                 const float ph = cphp[m] + pa.w;
                                 uacc[m] += dwp;
                                 cphp[m] = fmaf(dwp, Kr, cphp[m]);
-                                const float fl = floorf(t);
-                                const float fr = t - fl;
+                                const float tm = __fadd_rd(t, kFloorMagic);
+                                const float fr = t - (tm - kFloorMagic);
                                 // proven in range by the producer; clamped for memory safety
-                                const unsigned ic = min((unsigned)(int)fl, (unsigned)(WB - 2));
+                                const unsigned ic = min((unsigned)(__float_as_int(tm) - kFloorMagicBits),
+                                                        (unsigned)(WB - 2));
                                 const float2 s0 = row[ic], s1 = row[ic + 1];
                                 const float vr = fmaf(fr, s1.x - s0.x, s0.x);
                                 const float vi = fmaf(fr, s1.y - s0.y, s0.y);
@@ -543,6 +709,7 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                         dwa[m] = uacc[m] - lin;
                         cph[m] = fmaf(-lin, Kr, cphp[m]);
                     }
+                  }
                     // keep the carried phase in [-pi, pi]
 #pragma unroll
                     for (int m = 0; m < M; ++m) {
@@ -552,7 +719,7 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                 } else {
                     const double rs = B.rngstart, rmx = B.rmax, dm = B.dmrg, k4 = B.k4pi;
                     const int x0 = h.x0;
-                    const bool fast = h.fast;
+                    const bool fast = h.fast && h.interior;
                     for (int j = 0; j < nk; ++j) {
                         const int k = k0 + j;
                         const double sx = pp[j].s[0], sy = pp[j].s[1], sz = pp[j].s[2];

@@ -6,9 +6,12 @@
 // per-pixel sum (500), and the read-modify-write merge of the output rows
 // into the .geo raster (510-537).  Differences: every CUDA call is checked
 // and reported; device scratch is cached per device and reused across calls
-// instead of being allocated and freed on every burst; the merge uses
-// pread/pwrite on the descriptor instead of an fdopen() stream that is never
-// flushed or closed.
+// instead of being allocated and freed on every burst; only the pixel box
+// [firstpix, min(lastpix, W-1)] of the DEM rows is read (the only columns the
+// sum touches) and only that box of the output rows is merged, row by row with
+// pread/pwrite on the descriptors (instead of an fdopen() stream that is never
+// flushed or closed), by several host threads; the DEM read overlaps the
+// upload of the burst.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
@@ -19,8 +22,10 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/srg_bp.h"
@@ -318,6 +323,34 @@ int check_flags(DevCtx &c, cudaStream_t st) {
     return SRG_OK;
 }
 
+// Host threads for the row-wise DEM read and merge of one burst: enough to
+// hide the per-call latency of pread/pwrite, at least 256 rows each.
+int row_threads(int rows) {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    return std::max(1, std::min({(int)std::min(hw, 16u), rows / 256, 16}));
+}
+
+// Start fn(r0, r1) over `nthr` contiguous blocks of [0, rows) on host threads
+// (a block whose thread cannot be started runs on the caller's); join() waits.
+struct RowPool {
+    std::vector<std::thread> th;
+    template <class F>
+    void start(int rows, int nthr, F fn) {
+        for (int t = 0; t < nthr; ++t) {
+            const int r0 = (int)((long long)rows * t / nthr), r1 = (int)((long long)rows * (t + 1) / nthr);
+            try {
+                th.emplace_back(fn, r0, r1);
+            } catch (...) {
+                fn(r0, r1);
+            }
+        }
+    }
+    void join() {
+        for (auto &x : th) x.join();
+        th.clear();
+    }
+    ~RowPool() { join(); }
+};
 }  // namespace
 
 extern "C" {
@@ -540,7 +573,6 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     const int nl = ll - fl + 1;
     if (o.verbose) printf("Burst line limits, size (first,last,nlines) %d %d %d\n", fl, ll, nl);
     const int W = demwidth;
-    const size_t npix = (size_t)nl * W;
     const int fp = fp_, lp = lp_;
 
     DevCtx *c = nullptr;
@@ -548,11 +580,12 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     if (rc) return rc;
     std::lock_guard<std::mutex> g(c->mu);
     cudaStream_t st = 0;
-    // pinned staging: the DEM slab in, the output window back
     const int fp_eff = std::max(fp, 0);
     const int lp_eff = std::min(lp, W - 1);
     const int ncols = lp_eff >= fp_eff ? lp_eff - fp_eff + 1 : 0;
-    const size_t dem_bytes = npix * 2;
+    if (ncols == 0) return SRG_OK;  // no pixel of the grid in the burst's box
+    // pinned staging: the DEM box in, the output box back
+    const size_t dem_bytes = (size_t)nl * ncols * 2;
     const size_t win_bytes = (size_t)nl * ncols * 8;
     const size_t stage_bytes = std::max(dem_bytes, win_bytes) + 64;
     if (stage_bytes > c->host_cap) {
@@ -565,28 +598,49 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
         }
         c->host_cap = stage_bytes;
     }
-    // DEM slab (azimuth_compress.cu:399-408); a short read leaves zeros
-    int16_t *slab = static_cast<int16_t *>(c->host_stage);
-    std::memset(slab, 0, dem_bytes);
-    if (pread(fddem, slab, dem_bytes, (off_t)fl * W * 2) < 0)
-        return fail(SRG_E_IO, "DEM read failed (fd %d, offset %lld)", fddem, (long long)fl * W * 2);
     const size_t bbytes = (size_t)rawdatalines * samplesPerBurst * 8;
     if ((rc = c->in_burst.ensure(bbytes)) || (rc = c->in_sat.ensure(24 * (size_t)rawdatalines)) ||
-        (rc = c->in_dem.ensure(dem_bytes)) || (rc = c->out.ensure(npix * 8)))
+        (rc = c->in_dem.ensure(dem_bytes)) || (rc = c->out.ensure(win_bytes)))
         return rc;
-    CK(cudaMemcpyAsync(c->in_burst.p, burstdata, bbytes, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(c->in_sat.p, satloc, 24 * (size_t)rawdatalines, cudaMemcpyHostToDevice, st));
+    // DEM box of rows [fl, fl + nl) (azimuth_compress.cu:399-408), read by host
+    // threads while the burst uploads; bytes past the end of the file read as 0
+    int16_t *slab = static_cast<int16_t *>(c->host_stage);
+    std::atomic<int> dem_err{0};
+    const int nthr = row_threads(nl);
+    RowPool readers;
+    readers.start(nl, nthr, [&](int r0, int r1) {
+        const size_t want = (size_t)ncols * 2;
+        for (int r = r0; r < r1; ++r) {
+            char *dst = reinterpret_cast<char *>(slab + (size_t)r * ncols);
+            const ssize_t got = pread(fddem, dst, want, ((off_t)(fl + r) * W + fp_eff) * 2);
+            if (got < 0) {
+                dem_err = 1;
+                return;
+            }
+            if ((size_t)got < want) std::memset(dst + got, 0, want - (size_t)got);
+        }
+    });
+    cudaError_t e1 = cudaMemcpyAsync(c->in_burst.p, burstdata, bbytes, cudaMemcpyHostToDevice, st);
+    cudaError_t e2 = cudaSuccess;
+    if (e1 == cudaSuccess)
+        e2 = cudaMemcpyAsync(c->in_sat.p, satloc, 24 * (size_t)rawdatalines, cudaMemcpyHostToDevice, st);
+    readers.join();
+    CK(e1);
+    CK(e2);
+    if (dem_err) return fail(SRG_E_IO, "DEM read failed (fd %d)", fddem);
     CK(cudaMemcpyAsync(c->in_dem.p, slab, dem_bytes, cudaMemcpyHostToDevice, st));
 
     srg_burst_desc d{};
     d.burst = static_cast<const float *>(c->in_burst.p);
     d.satloc = static_cast<const double *>(c->in_sat.p);
-    d.dem = static_cast<const int16_t *>(c->in_dem.p);
+    // the sum reads DEM columns [firstpix, lastpix_eff] only: the descriptor's
+    // column 0 lies fp_eff entries before the box
+    d.dem = static_cast<const int16_t *>(c->in_dem.p) - fp_eff;
     d.out = static_cast<float *>(c->out.p);
     d.coef = nullptr;
     d.ldb = samplesPerBurst;
-    d.dem_ld = W;
-    d.out_ld = W;
+    d.dem_ld = ncols;
+    d.out_ld = ncols;
     d.P = rawdatalines;
     d.S = samplesPerBurst;
     d.demwidth = W;
@@ -594,7 +648,7 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     d.nlines = nl;
     d.firstpix = fp;
     d.lastpix = lp;
-    d.out_pix0 = 0;
+    d.out_pix0 = fp_eff;
     d.aperture = aperture;
     d.firstlat = firstlat;
     d.deltalat = deltalat;
@@ -616,39 +670,49 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     d.angc0 = angc0;
     d.angc1 = angc1;
     d.prf = prf;
-    if (ncols == 0) return SRG_OK;  // no pixel of the grid in the burst's box
     rc = run_bursts(*c, &d, 1, o, st);
     if (rc) return rc;
-    // the kernel wrote every pixel of the window: bring back only the window
+    // the kernel wrote every pixel of the box: bring back only the box
     float *win = static_cast<float *>(c->host_stage);
-    CK(cudaMemcpy2DAsync(win, (size_t)ncols * 8, static_cast<float2 *>(c->out.p) + fp_eff,
-                         (size_t)W * 8, (size_t)ncols * 8, nl, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(win, c->out.p, win_bytes, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     CK(cudaGetLastError());
     rc = check_flags(*c, st);
     if (rc) return rc;
 
     // merge into the .geo rows (azimuth_compress.cu:510-537); pixels outside
-    // the window are never replaced, so only the window is read and written
-    std::vector<float> cur(2 * (size_t)ncols);
-    for (int r = 0; r < nl; ++r) {
-        const off_t off = ((off_t)(fl + r) * W + fp_eff) * 8;
+    // the box are never replaced, so only the box is read and written
+    std::atomic<int> io_err{0};
+    RowPool mergers;
+    mergers.start(nl, nthr, [&](int r0, int r1) {
+        std::vector<float> cur(2 * (size_t)ncols);
         const ssize_t want = (ssize_t)ncols * 8;
-        const ssize_t got = pread(fdout, cur.data(), want, off);
-        if (got < 0) return fail(SRG_E_IO, "output read failed (fd %d)", fdout);
-        if (got < want) std::memset(reinterpret_cast<char *>(cur.data()) + got, 0, want - got);
-        const float *o2 = win + 2 * (size_t)r * ncols;
-        bool changed = false;
-        for (int i = 0; i < ncols; ++i) {
-            if (std::fabs((double)o2[2 * i]) > 1.e-18) {
-                cur[2 * i] = o2[2 * i];
-                cur[2 * i + 1] = o2[2 * i + 1];
-                changed = true;
+        for (int r = r0; r < r1; ++r) {
+            const off_t off = ((off_t)(fl + r) * W + fp_eff) * 8;
+            const ssize_t got = pread(fdout, cur.data(), want, off);
+            if (got < 0) {
+                io_err = 1;
+                return;
+            }
+            if (got < want) std::memset(reinterpret_cast<char *>(cur.data()) + got, 0, want - got);
+            const float *o2 = win + 2 * (size_t)r * ncols;
+            bool changed = false;
+            for (int i = 0; i < ncols; ++i) {
+                if (std::fabs((double)o2[2 * i]) > 1.e-18) {
+                    cur[2 * i] = o2[2 * i];
+                    cur[2 * i + 1] = o2[2 * i + 1];
+                    changed = true;
+                }
+            }
+            if (changed && pwrite(fdout, cur.data(), want, off) != want) {
+                io_err = 2;
+                return;
             }
         }
-        if (changed && pwrite(fdout, cur.data(), want, off) != want)
-            return fail(SRG_E_IO, "output write failed (fd %d)", fdout);
-    }
+    });
+    mergers.join();
+    if (io_err == 1) return fail(SRG_E_IO, "output read failed (fd %d)", fdout);
+    if (io_err == 2) return fail(SRG_E_IO, "output write failed (fd %d)", fdout);
     return SRG_OK;
 }
 
