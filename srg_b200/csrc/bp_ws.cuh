@@ -110,10 +110,21 @@ __host__ __device__ constexpr int ws_params_bytes() {
 }
 
 // Dynamic shared memory of a shape: params of every stage, then the sample
-// windows from the first 1024-byte boundary.
+// windows from the first 1024-byte boundary, then a 16-byte guard (a tap index
+// masked to the row width may address the first sample after the last row).
 template <int FORM, int CK, int NS>
 __host__ __device__ constexpr int ws_smem_bytes(int WB) {
-    return NS * ws_params_bytes<FORM, CK>() + 1024 + NS * CK * WB * 8;
+    return NS * ws_params_bytes<FORM, CK>() + 1024 + NS * CK * WB * 8 + 16;
+}
+
+// Tap index of a term from the bits of floor(t) + kFloorMagic.  The fast paths
+// have proven t in [0, WB - 1); for memory safety any other t still lands in
+// the stage: masked to the row when WB is a power of two (the magic's low bits
+// are zero), clamped otherwise.
+template <int WB>
+__device__ __forceinline__ unsigned tap_index(float tm) {
+    if constexpr ((WB & (WB - 1)) == 0) return __float_as_uint(tm) & (unsigned)(WB - 1);
+    else return min(__float_as_uint(tm) - (unsigned)kFloorMagicBits, (unsigned)(WB - 2));
 }
 
 // Chunk schedule of a tile: the pulse range [kmin, kmax) is cut at ka and kb
@@ -151,12 +162,14 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
     asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-// MINB: blocks per SM the register allocation is sized for.
-template <int FORM, int TX, int TY, int NC, int CK, int NS, int MINB>
+// WB: staged bins per pulse (the launch passes the same value as its last
+// argument, shared with the first-generation kernels); MINB: blocks per SM
+// the register allocation is sized for.
+template <int FORM, int TX, int TY, int NC, int CK, int NS, int WB, int MINB>
 __global__ void __launch_bounds__((NC + 1) * 32, MINB)
 bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
       const CUtensorMap *__restrict__ tmaps, int *__restrict__ work_counter,
-      int *__restrict__ err, int WB) {
+      int *__restrict__ err, int /* window, = WB */) {
     constexpr int NCT = NC * 32;
     constexpr int M = TX * TY / NCT;
     constexpr int BX = TX / 8;  // 8 x 4 pixel blocks, one per warp and slot
@@ -168,6 +181,7 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
     extern __shared__ __align__(128) unsigned char dsm[];
     __shared__ CtlWS ctl;
     __shared__ StageHdr hdr[NS];
+    __shared__ double lat_tab[TY][4], lon_tab[TX][2];  // per-tile line / column factors of the ECEF
     PP *prm = reinterpret_cast<PP *>(dsm);
     float2 *samp0;
     {
@@ -204,6 +218,16 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
         const int ly0 = (ti / B.tiles_x) * TY;
 
         // ---- prologue (all threads) ----
+        static_assert(TX + TY <= (NC + 1) * 32, "one thread per table row");
+        if (tid < TY) {
+            const LineTrig L = line_trig(B, ly0 + tid);
+            lat_tab[tid][0] = L.slat;
+            lat_tab[tid][1] = L.clat;
+            lat_tab[tid][2] = L.re;
+            lat_tab[tid][3] = L.rez;
+        } else if (tid < TY + TX) {
+            col_trig(B, px0 + tid - TY, lon_tab[tid - TY][0], lon_tab[tid - TY][1]);
+        }
         if (tid == 0) {
             ctl.kmin = INT_MAX;
             ctl.kmax = INT_MIN;
@@ -227,7 +251,8 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                 azs[m] = aze[m] = 0;
                 if (px <= B.lastpix_eff && line < B.nlines) {
                     const double h = (double)B.dem[(long long)line * B.dem_ld + px];
-                    pixel_ecef(B, line, px, h, X[m][0], X[m][1], X[m][2]);
+                    pixel_ecef_from(lat_tab[y][0], lat_tab[y][1], lat_tab[y][2], lat_tab[y][3],
+                                    lon_tab[x][0], lon_tab[x][1], h, X[m][0], X[m][1], X[m][2]);
                     pixel_window(B, pixel_azoff(B, B.coef + 3 * line, px), azs[m], aze[m]);
                     if (aze[m] > azs[m]) {
                         k0 = min(k0, azs[m]);
@@ -582,7 +607,9 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                         dwa[m] += S;
                         cph[m] = fmaf(Kr, S, cph[m]);
                     }
-                    // edge chunks add the exact azimuth-window test of every term
+                    // edge chunks add the exact azimuth-window test of every term;
+                    // the quadratics and the floor run on pixel pairs (f32x2)
+                    static_assert(M % 2 == 0, "pixel pairs");
                     auto terms = [&](auto masked) {
                         constexpr bool MASKED = decltype(masked)::value;
                         int ja[M], nj[M];
@@ -591,32 +618,52 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                             ja[m] = max(azs[m] - k0, 0);
                             nj[m] = max(min(aze[m] - k0, nk) - ja[m], 0);
                         }
-                        float f = -jc;
-#pragma unroll 2
-                        for (int j = 0; j < nk; ++j, f += 1.f) {
+                        uint64_t t0[M / 2], t1[M / 2], t2[M / 2], q0[M / 2], q1[M / 2], q2[M / 2];
+#pragma unroll
+                        for (int e = 0; e < M / 2; ++e) {
+                            t0[e] = f2_pack(T0[2 * e], T0[2 * e + 1]);
+                            t1[e] = f2_pack(T1[2 * e], T1[2 * e + 1]);
+                            t2[e] = f2_pack(T2[2 * e], T2[2 * e + 1]);
+                            q0[e] = f2_pack(P0[2 * e], P0[2 * e + 1]);
+                            q1[e] = f2_pack(P1[2 * e], P1[2 * e + 1]);
+                            q2[e] = f2_pack(P2[2 * e], P2[2 * e + 1]);
+                        }
+                        const uint64_t mag = f2_pack(kFloorMagic, kFloorMagic);
+                        const uint64_t one = f2_pack(1.f, 1.f);
+                        uint64_t ff = f2_pack(-jc, -jc);
+#pragma unroll 4
+                        for (int j = 0; j < nk; ++j) {
                             const float2 *row = win + j * WB;
 #pragma unroll
-                            for (int m = 0; m < M; ++m) {
-                                const float t = fmaf(fmaf(T2[m], f, T1[m]), f, T0[m]);
-                                const float ph = fmaf(fmaf(P2[m], f, P1[m]), f, P0[m]);
-                                const float tm = __fadd_rd(t, kFloorMagic);
-                                const float fr = t - (tm - kFloorMagic);
-                                // proven in range by the producer; clamped for memory safety
-                                const unsigned ic = min((unsigned)(__float_as_int(tm) - kFloorMagicBits),
-                                                        (unsigned)(WB - 2));
-                                const float2 s0 = row[ic], s1 = row[ic + 1];
-                                float vr = fmaf(fr, s1.x - s0.x, s0.x);
-                                float vi = fmaf(fr, s1.y - s0.y, s0.y);
-                                if constexpr (MASKED) {
-                                    const bool ok = (unsigned)(j - ja[m]) < (unsigned)nj[m];
-                                    vr = ok ? vr : 0.f;
-                                    vi = ok ? vi : 0.f;
+                            for (int e = 0; e < M / 2; ++e) {
+                                const uint64_t t = f2_fma(f2_fma(t2[e], ff, t1[e]), ff, t0[e]);
+                                const uint64_t ph = f2_fma(f2_fma(q2[e], ff, q1[e]), ff, q0[e]);
+                                const uint64_t tm = f2_add_rm(t, mag);
+                                const uint64_t fr = f2_sub(t, f2_sub(tm, mag));
+                                float tmv[2], frv[2], phv[2];
+                                f2_unpack(tm, tmv[0], tmv[1]);
+                                f2_unpack(fr, frv[0], frv[1]);
+                                f2_unpack(ph, phv[0], phv[1]);
+#pragma unroll
+                                for (int h2 = 0; h2 < 2; ++h2) {
+                                    const int m = 2 * e + h2;
+                                    // proven in the window by the producer; bounded for memory safety
+                                    const unsigned ic = tap_index<WB>(tmv[h2]);
+                                    const float2 s0 = row[ic], s1 = row[ic + 1];
+                                    float vr = fmaf(frv[h2], s1.x - s0.x, s0.x);
+                                    float vi = fmaf(frv[h2], s1.y - s0.y, s0.y);
+                                    if constexpr (MASKED) {
+                                        const bool ok = (unsigned)(j - ja[m]) < (unsigned)nj[m];
+                                        vr = ok ? vr : 0.f;
+                                        vi = ok ? vi : 0.f;
+                                    }
+                                    float sn, cs;
+                                    __sincosf(phv[h2], &sn, &cs);
+                                    accr[m] = fmaf(vr, cs, fmaf(-vi, sn, accr[m]));
+                                    acci[m] = fmaf(vr, sn, fmaf(vi, cs, acci[m]));
                                 }
-                                float sn, cs;
-                                __sincosf(ph, &sn, &cs);
-                                accr[m] = fmaf(vr, cs, fmaf(-vi, sn, accr[m]));
-                                acci[m] = fmaf(vr, sn, fmaf(vi, cs, acci[m]));
                             }
+                            ff = f2_add(ff, one);
                         }
                     };
                     if (h.interior) terms(std::false_type{});
@@ -654,8 +701,7 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                                 const float tm = __fadd_rd(t, kFloorMagic);
                                 const float fr = t - (tm - kFloorMagic);
                                 // proven in range by the producer; clamped for memory safety
-                                const unsigned ic = min((unsigned)(__float_as_int(tm) - kFloorMagicBits),
-                                                        (unsigned)(WB - 2));
+                                const unsigned ic = tap_index<WB>(tm);
                                 const float2 s0 = row[ic], s1 = row[ic + 1];
                                 const float vr = fmaf(fr, s1.x - s0.x, s0.x);
                                 const float vi = fmaf(fr, s1.y - s0.y, s0.y);

@@ -16,22 +16,42 @@ __device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a,
 __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
 
-// Pixel ECEF on WGS-84 (sentinel/azimuth_compress.cu:117-131).
-__device__ __forceinline__ void pixel_ecef(const BurstDev &B, int line, int pix, double hgt,
-                                           double &x, double &y, double &z) {
+// Pixel ECEF on WGS-84 (sentinel/azimuth_compress.cu:117-131), split into
+// the factors that depend on the line only and on the column only, so that a
+// tile can evaluate each sine and cosine once; pixel_ecef composes them with
+// the same operations in the same order.
+struct LineTrig {
+    double slat, clat, re, rez;  // sin, cos of the latitude; prime-vertical radius; re - re*e2
+};
+__device__ __forceinline__ LineTrig line_trig(const BurstDev &B, int line) {
     const double a = 6378137.0;
     const double e2 = 0.0066943799901499996;
     const double lat = dadd(B.firstlat, dmul((double)(line + B.firstline), B.deltalat));
     const double rlat = dmul(lat, B.deg2rad);
+    LineTrig L;
+    sincos(rlat, &L.slat, &L.clat);
+    L.re = ddiv(a, __dsqrt_rn(dsub(1.0, dmul(dmul(e2, L.slat), L.slat))));
+    L.rez = dsub(L.re, dmul(L.re, e2));
+    return L;
+}
+__device__ __forceinline__ void col_trig(const BurstDev &B, int pix, double &slon, double &clon) {
     const double rlon = dmul(dadd(B.firstlon, dmul((double)pix, B.deltalon)), B.deg2rad);
-    double slat, clat, slon, clon;
-    sincos(rlat, &slat, &clat);
     sincos(rlon, &slon, &clon);
-    const double re = ddiv(a, __dsqrt_rn(dsub(1.0, dmul(dmul(e2, slat), slat))));
+}
+__device__ __forceinline__ void pixel_ecef_from(double slat, double clat, double re, double rez,
+                                                double slon, double clon, double hgt, double &x,
+                                                double &y, double &z) {
     const double rh = dadd(re, hgt);
     x = dmul(dmul(rh, clat), clon);
     y = dmul(dmul(rh, clat), slon);
-    z = dmul(dadd(dsub(re, dmul(re, e2)), hgt), slat);
+    z = dmul(dadd(rez, hgt), slat);
+}
+__device__ __forceinline__ void pixel_ecef(const BurstDev &B, int line, int pix, double hgt,
+                                           double &x, double &y, double &z) {
+    const LineTrig L = line_trig(B, line);
+    double slon, clon;
+    col_trig(B, pix, slon, clon);
+    pixel_ecef_from(L.slat, L.clat, L.re, L.rez, slon, clon, hgt, x, y, z);
 }
 
 // azoff of one pixel from its line's parabola (azimuth_compress.cu:169-175),

@@ -276,7 +276,7 @@ cudaError_t launch_fma_peak(int fp64, int blocks, int iters, void *sink, cudaStr
      "bp_tiles<" #F "," #TXv "x" #TYv ",threads " #NTv ",chunk " #CKv ",window " #WBv ">"},
 #define SRG_WS_ENTRY(F, TXv, TYv, NCv, CKv, NSv, WBv, MBv)                                      \
     {F, {TXv, TYv, (NCv + 1) * 32, CKv, WBv}, ws_smem_bytes<F, CKv, NSv>(WBv),                  \
-     (const void *)bp_ws<F, TXv, TYv, NCv, CKv, NSv, MBv>,                                      \
+     (const void *)bp_ws<F, TXv, TYv, NCv, CKv, NSv, WBv, MBv>,                                 \
      "bp_ws<" #F "," #TXv "x" #TYv ",consumer warps " #NCv ",chunk " #CKv ",stages " #NSv       \
      ",window " #WBv ",min blocks " #MBv ">"},
 
