@@ -226,9 +226,10 @@ def e2e_dropin(torch, wl, steps, form):
     return dt, h2d, d2h
 
 
-def time_plan(torch, plan, steps, warmup, stream, stages=None):
+def time_plan(torch, plan, steps, warmup, stream, stages=None, label="timed"):
     """K passes of a scene plan on `stream` (graph replay), or of chosen
-    stages; returns ms per pass (CUDA events on the stream)."""
+    stages; returns ms per pass (CUDA events on the stream).  The timed
+    passes sit in an NVTX range named `label` (for ncu --nvtx-include)."""
     sp = stream.cuda_stream
     run = (lambda: plan.run(sp)) if stages is None else (lambda: plan.run_stages(stages, sp))
     for _ in range(warmup):
@@ -236,10 +237,12 @@ def time_plan(torch, plan, steps, warmup, stream, stages=None):
     torch.cuda.synchronize()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(steps)]
+    torch.cuda.nvtx.range_push(label)
     for e0, e1 in ev:
         e0.record(stream)
         run()
         e1.record(stream)
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     plan.sync(sp)
     return sum(e0.elapsed_time(e1) for e0, e1 in ev) / steps
@@ -336,7 +339,10 @@ def main():
     ap.add_argument("--workload", default="c3", choices=["c1", "c3"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shapes", default=None,
+                    help="SPLIT,FP64 kernel shape indices (srg_tile_config); default: tuned")
     args = ap.parse_args()
+    pinned = [int(x) for x in args.shapes.split(",")] if args.shapes else None
     rank, world, local = dist_env()
     if args.impl == "reference" and rank != 0:
         return  # the reference arm runs on rank 0 only
@@ -377,17 +383,25 @@ def main():
     tuned = {}
     if args.workload == "c3":
         plan = wl.plan
-        tuned["split"] = plan.tune(iters=2)
+        if pinned:
+            plan.set_form(_lib.FORM_SPLIT, pinned[0])
+            tuned["split"] = (pinned[0], None)
+        else:
+            tuned["split"] = plan.tune(iters=2)
         with ClockSampler(local) as clk:
             if world > 1:
                 dist.barrier()
-            s_ms = time_plan(torch, plan, args.steps, args.warmup, stream)
+            s_ms = time_plan(torch, plan, args.steps, args.warmup, stream, label="timed_split")
             if world > 1:
                 dist.barrier()
         s_kern = time_plan(torch, plan, args.steps, 1, stream, stages=2)
         split_raster = wl.raster.clone()
-        plan.set_form(_lib.FORM_FP64)
-        tuned["fp64"] = plan.tune(iters=1)
+        if pinned:
+            plan.set_form(_lib.FORM_FP64, pinned[1])
+            tuned["fp64"] = (pinned[1], None)
+        else:
+            plan.set_form(_lib.FORM_FP64)
+            tuned["fp64"] = plan.tune(iters=1)
         d_ms = time_plan(torch, plan, max(3, args.steps // 3), 1, stream)
         d_kern = d_ms
         perr = raster_phase_error(torch, split_raster, wl.raster)

@@ -246,6 +246,31 @@ int srg_forward_project_device(const srg_burst_desc *b, const float *refl,
                                int64_t refl_ld, const double *satvel,
                                double antenna_m, void *stream);
 
+/* ---- Interferogram formation (replaces the crossmul program,
+ * int/crossmul.f90:95-185, which SRG runs on pairs of .geo files) ----
+ * Each line of both images (scaled by `scale`) is upsampled 2x across by
+ * FFT (zero-padded to nnn = the first power of two >= na, spectrum halves
+ * moved to the ends of a 2*nnn array, inverse FFT, / nnn / 2); the images are
+ * cross-multiplied (slc1 * conj(slc2)) and their powers kept; pairs of
+ * upsampled samples are summed, then `looksdn` lines down and `looksac`
+ * samples across; the amplitude pair is square-rooted (|slc1|, |slc2|).  With
+ * `mask` != 0 an output sample is zeroed when |sum of the unscaled input over
+ * its look window| <= 1e-6 in either image (the reference's default 'y').
+ * Inputs: [nlines][ld] complex64 (device); nlines plays the reference's
+ * <valid_lines>.  Outputs: [nlines/looksdn][na/looksac] complex64 (device).
+ * Enqueued on `stream`; FFTs by cuFFT (the reference uses FFTW in single
+ * precision, so results agree to FP32 rounding, not bit for bit). */
+int srg_crossmul_device(const float *slc1, const float *slc2, long long ld, int na, int nlines,
+                        int looksac, int looksdn, float scale, int mask, float *igram,
+                        float *amp, void *stream);
+/* Sequential pairs (k, k+1), k = 0..n-2, of a stack of n images (device
+ * pointer arrays on the host), each image transformed once; igrams[k] and
+ * amps[k] receive pair k.  No reference counterpart (the reference runs the
+ * crossmul program once per pair). */
+int srg_crossmul_stack_device(const float *const *slcs, int n, long long ld, int na, int nlines,
+                              int looksac, int looksdn, float scale, int mask,
+                              float *const *igrams, float *const *amps, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -90,6 +90,11 @@ _SIGS = {
     "srg_tile_config_name": (C.c_char_p, [C.c_int]),
     "srg_forward_project_device": (C.c_int, [C.POINTER(BurstDesc), C.c_void_p, C.c_int64, C.c_void_p,
                                              C.c_double, C.c_void_p]),
+    "srg_crossmul_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong, C.c_int, C.c_int, C.c_int,
+                                      C.c_int, C.c_float, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "srg_crossmul_stack_device": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_longlong, C.c_int,
+                                            C.c_int, C.c_int, C.c_int, C.c_float, C.c_int,
+                                            C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_void_p]),
     "srg_azimuth_compress": (C.c_int, [
         _fp, _dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
         C.c_double, C.c_double, C.c_double, C.c_double, _dp, _dp, _dp, _dp, C.c_int,

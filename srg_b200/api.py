@@ -233,6 +233,68 @@ def forward_project(db: DeviceBurst, refl, satvel, antenna: float = 10.0, stream
                                            C.c_void_p(_stream_ptr(stream))))
 
 
+def _xm_check(t, na):
+    import torch
+    if t.dtype != torch.complex64 or t.dim() != 2 or t.stride(1) != 1 or not t.is_cuda:
+        raise ValueError("images must be 2-D complex64 CUDA tensors with unit column stride")
+
+
+def crossmul(slc1, slc2, looksac: int = 1, looksdn: Optional[int] = None, scale: float = 1.0,
+             mask: bool = True, nvalid: Optional[int] = None, stream=None, sync: bool = True):
+    """Interferogram and amplitude images of two co-registered device images
+    (srg_crossmul_device; the reference's int/crossmul.f90).  Returns
+    (igram, amp), complex64 [nvalid // looksdn][na // looksac] on the device."""
+    import torch
+    looksdn = looksac if looksdn is None else looksdn
+    nd, na = slc1.shape
+    nvalid = nd if nvalid is None else nvalid
+    for t in (slc1, slc2):
+        _xm_check(t, na)
+    if slc2.shape != slc1.shape or slc2.stride(0) != slc1.stride(0):
+        raise ValueError("images must have the same shape and row stride")
+    shape = (nvalid // looksdn, na // looksac)
+    ig = torch.empty(shape, dtype=torch.complex64, device=slc1.device)
+    am = torch.empty_like(ig)
+    st = _stream_ptr(stream)
+    check(lib().srg_crossmul_device(
+        C.c_void_p(slc1.data_ptr()), C.c_void_p(slc2.data_ptr()), slc1.stride(0), na, nvalid,
+        looksac, looksdn, scale, int(bool(mask)), C.c_void_p(ig.data_ptr()), C.c_void_p(am.data_ptr()),
+        C.c_void_p(st)))
+    if sync:
+        check(lib().srg_sync_check(C.c_void_p(st)))
+    return ig, am
+
+
+def crossmul_stack(slcs, looksac: int = 1, looksdn: Optional[int] = None, scale: float = 1.0,
+                   mask: bool = True, stream=None, sync: bool = True, outs=None):
+    """Interferograms of the sequential pairs (k, k+1) of a list of device
+    images (srg_crossmul_stack_device: each image transformed once).
+    Returns ([igram_k], [amp_k]); `outs` may supply them."""
+    import torch
+    looksdn = looksac if looksdn is None else looksdn
+    nd, na = slcs[0].shape
+    for t in slcs:
+        _xm_check(t, na)
+        if t.shape != slcs[0].shape or t.stride(0) != slcs[0].stride(0):
+            raise ValueError("images must have the same shape and row stride")
+    shape = (nd // looksdn, na // looksac)
+    if outs is None:
+        igs = [torch.empty(shape, dtype=torch.complex64, device=slcs[0].device) for _ in slcs[1:]]
+        ams = [torch.empty_like(g) for g in igs]
+    else:
+        igs, ams = outs
+    n = len(slcs)
+    pin = (C.c_void_p * n)(*[t.data_ptr() for t in slcs])
+    pig = (C.c_void_p * (n - 1))(*[t.data_ptr() for t in igs])
+    pam = (C.c_void_p * (n - 1))(*[t.data_ptr() for t in ams])
+    st = _stream_ptr(stream)
+    check(lib().srg_crossmul_stack_device(pin, n, slcs[0].stride(0), na, nd, looksac, looksdn, scale,
+                                          int(bool(mask)), pig, pam, C.c_void_p(st)))
+    if sync:
+        check(lib().srg_sync_check(C.c_void_p(st)))
+    return igs, ams
+
+
 class Scene:
     """A reusable plan over device bursts (srg_scene_*): azimuth centres,
     one persistent backprojection launch for all bursts and the ordered merge

@@ -8,7 +8,7 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsrg_bp.so")
-SOURCES = ["capi.cu", "kernels.cu", "noalloc.cu", "scene.cu"]
+SOURCES = ["capi.cu", "kernels.cu", "noalloc.cu", "scene.cu", "crossmul.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -34,7 +34,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         return LIB
     cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
            "-Xcompiler", "-Wall", "-o", LIB + ".tmp",
-           *[os.path.join(CSRC, s) for s in SOURCES]]
+           *[os.path.join(CSRC, s) for s in SOURCES], "-lcufft"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     subprocess.run(cmd, check=True)

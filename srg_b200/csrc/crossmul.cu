@@ -1,0 +1,265 @@
+// crossmul.cu -- interferograms of co-registered complex64 images on the GPU.
+//
+// Follows int/crossmul.f90:95-185 line for line in what it computes; the
+// layout is the GPU's: every output line of every pair is independent, so the
+// images are transformed whole (one batched FFT per image and direction,
+// cuFFT) and one fused kernel forms the cross products, the two-sample
+// reclaim, the looks down and across, the square-rooted amplitudes and the
+// zero-input mask.  Per image:
+//   1. in * scale, zero-padded from na to nnn = the first 2^i >= na (i >= 1)
+//      (crossmul.f90:69-73, 128-135);
+//   2. forward FFT of nnn points (FFTW sign -1, unnormalised);
+//   3. spectrum bins [0, nnn/2) to [0, nnn/2) and [nnn/2, nnn) to
+//      [2nnn - nnn/2, 2nnn) of a zeroed 2nnn array (crossmul.f90:136-137);
+//   4. inverse FFT of 2nnn points (sign +1), / nnn / 2 (crossmul.f90:139-141).
+// Per pair and output sample (line L, column j), with u1, u2 the upsampled
+// lines: igram = sum_k sum_i (u1 conj(u2))[2c] + (u1 conj(u2))[2c+1],
+// c = j looksac + k, i over the looksdn input lines of L (crossmul.f90:155-172);
+// amp likewise with (|u1|^2, |u2|^2), then (sqrt re, sqrt im) (:173); both
+// zeroed where |sum of the raw input over the look window| <= 1e-6 in either
+// image (crossmul.f90:112-125, 176-184).  Sums run in the reference's order
+// (reclaim, then down, then across) in FP32 as the reference's complex*8.
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <mutex>
+#include <vector>
+
+#include "../../include/srg_bp.h"
+#include "host_internal.h"
+
+using namespace srg;
+using namespace srg::detail;
+
+namespace {
+
+#define CKC(call)                                                                      \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess)                                                         \
+            return fail(SRG_E_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));   \
+    } while (0)
+#define CKF(call)                                                                      \
+    do {                                                                               \
+        cufftResult r_ = (call);                                                       \
+        if (r_ != CUFFT_SUCCESS) return fail(SRG_E_CUDA, "%s failed: cufft %d", #call, (int)r_); \
+    } while (0)
+
+// in * scale, zero-padded to nnn, for nl lines
+__global__ void pad_scale_kernel(const float2 *__restrict__ in, long long ld, int na, int nnn, int nl,
+                                 float scale, float2 *__restrict__ out) {
+    const long long total = (long long)nl * nnn;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int l = (int)(i / nnn), n = (int)(i - (long long)l * nnn);
+        float2 v = make_float2(0.f, 0.f);
+        if (n < na) {
+            const float2 x = in[(long long)l * ld + n];
+            v = make_float2(x.x * scale, x.y * scale);
+        }
+        out[i] = v;
+    }
+}
+
+// nnn-point spectrum -> 2nnn array with the upper half of the bins at the top
+__global__ void spread_kernel(const float2 *__restrict__ X, int nnn, int nl, float2 *__restrict__ up) {
+    const int n2 = 2 * nnn, h = nnn / 2;
+    const long long total = (long long)nl * n2;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int l = (int)(i / n2), m = (int)(i - (long long)l * n2);
+        float2 v = make_float2(0.f, 0.f);
+        if (m < h) v = X[(long long)l * nnn + m];
+        else if (m >= n2 - h) v = X[(long long)l * nnn + (m - nnn)];
+        up[i] = v;
+    }
+}
+
+__device__ __forceinline__ float2 cmul_conj(float2 a, float2 b) {  // a * conj(b)
+    return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+
+// one thread per output sample (L, j)
+__global__ void crossmul_looks_kernel(const float2 *__restrict__ up1, const float2 *__restrict__ up2,
+                                      const float2 *__restrict__ in1, const float2 *__restrict__ in2,
+                                      long long ld, int nnn, int nout_lines, int nout_cols,
+                                      int looksac, int looksdn, int mask, float2 *__restrict__ igram,
+                                      float2 *__restrict__ amp) {
+    const long long total = (long long)nout_lines * nout_cols;
+    const float inv = 1.f / (float)nnn;  // a power of two: same as the reference's division
+    const int n2 = 2 * nnn;
+    for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < total;
+         o += (long long)gridDim.x * blockDim.x) {
+        const int L = (int)(o / nout_cols), j = (int)(o - (long long)L * nout_cols);
+        float2 ig = make_float2(0.f, 0.f), am = make_float2(0.f, 0.f);
+        float2 m1 = make_float2(0.f, 0.f), m2 = make_float2(0.f, 0.f);
+        for (int k = 0; k < looksac; ++k) {
+            const int c = j * looksac + k;
+            float2 gd = make_float2(0.f, 0.f), ad = make_float2(0.f, 0.f);
+            float2 s1 = make_float2(0.f, 0.f), s2 = make_float2(0.f, 0.f);
+            for (int i = 0; i < looksdn; ++i) {
+                const long long l = (long long)L * looksdn + i;
+                const float2 *u1 = up1 + l * n2, *u2 = up2 + l * n2;
+                float2 a0 = u1[2 * c], a1 = u1[2 * c + 1], b0 = u2[2 * c], b1 = u2[2 * c + 1];
+                a0 = make_float2(a0.x * inv * 0.5f, a0.y * inv * 0.5f);
+                a1 = make_float2(a1.x * inv * 0.5f, a1.y * inv * 0.5f);
+                b0 = make_float2(b0.x * inv * 0.5f, b0.y * inv * 0.5f);
+                b1 = make_float2(b1.x * inv * 0.5f, b1.y * inv * 0.5f);
+                const float2 g0 = cmul_conj(a0, b0), g1 = cmul_conj(a1, b1);
+                gd.x += g0.x + g1.x;
+                gd.y += g0.y + g1.y;
+                ad.x += (a0.x * a0.x + a0.y * a0.y) + (a1.x * a1.x + a1.y * a1.y);
+                ad.y += (b0.x * b0.x + b0.y * b0.y) + (b1.x * b1.x + b1.y * b1.y);
+                if (mask) {
+                    const float2 x1 = in1[l * ld + c], x2 = in2[l * ld + c];
+                    s1.x += x1.x;
+                    s1.y += x1.y;
+                    s2.x += x2.x;
+                    s2.y += x2.y;
+                }
+            }
+            ig.x += gd.x;
+            ig.y += gd.y;
+            am.x += ad.x;
+            am.y += ad.y;
+            m1.x += s1.x;
+            m1.y += s1.y;
+            m2.x += s2.x;
+            m2.y += s2.y;
+        }
+        am = make_float2(sqrtf(am.x), sqrtf(am.y));
+        if (mask && (hypotf(m1.x, m1.y) <= 1.e-6f || hypotf(m2.x, m2.y) <= 1.e-6f)) {
+            ig = make_float2(0.f, 0.f);
+            am = make_float2(0.f, 0.f);
+        }
+        igram[o] = ig;
+        amp[o] = am;
+    }
+}
+
+struct Plan {
+    int n = 0, batch = 0;
+    cufftHandle h = 0;
+    bool ok = false;
+};
+
+struct XmCtx {
+    std::mutex mu;
+    Plan fwd, inv;
+    DevBuf pad, upA, upB;
+};
+XmCtx g_xm[64];
+
+int plan_for(Plan &p, int n, int batch) {
+    if (p.ok && p.n == n && p.batch == batch) return SRG_OK;
+    if (p.ok) cufftDestroy(p.h);
+    p.ok = false;
+    CKF(cufftPlan1d(&p.h, n, CUFFT_C2C, batch));
+    p.n = n;
+    p.batch = batch;
+    p.ok = true;
+    return SRG_OK;
+}
+
+int grid_for(long long n) {
+    long long g = (n + 255) / 256;
+    return (int)std::min<long long>(g, 148LL * 32);
+}
+
+// upsampled lines of one image into `up` (nl x 2nnn)
+int upsample(XmCtx &x, const float2 *in, long long ld, int na, int nnn, int nl, float scale,
+             float2 *up, cudaStream_t st) {
+    float2 *pad = static_cast<float2 *>(x.pad.p);
+    pad_scale_kernel<<<grid_for((long long)nl * nnn), 256, 0, st>>>(in, ld, na, nnn, nl, scale, pad);
+    CKC(cudaGetLastError());
+    CKF(cufftSetStream(x.fwd.h, st));
+    CKF(cufftExecC2C(x.fwd.h, reinterpret_cast<cufftComplex *>(pad),
+                     reinterpret_cast<cufftComplex *>(pad), CUFFT_FORWARD));
+    spread_kernel<<<grid_for((long long)nl * 2 * nnn), 256, 0, st>>>(pad, nnn, nl, up);
+    CKC(cudaGetLastError());
+    CKF(cufftSetStream(x.inv.h, st));
+    CKF(cufftExecC2C(x.inv.h, reinterpret_cast<cufftComplex *>(up),
+                     reinterpret_cast<cufftComplex *>(up), CUFFT_INVERSE));
+    return SRG_OK;
+}
+
+int check_args(long long ld, int na, int nlines, int looksac, int looksdn) {
+    if (na < 1 || ld < na || nlines < 1 || looksac < 1 || looksdn < 1)
+        return fail(SRG_E_ARG, "bad crossmul sizes: na=%d ld=%lld nlines=%d looks=%d x %d", na, ld,
+                    nlines, looksac, looksdn);
+    if (na / looksac < 1 || nlines / looksdn < 1)
+        return fail(SRG_E_ARG, "looks %d x %d exceed the image %d x %d", looksac, looksdn, na, nlines);
+    if (na > (1 << 24)) return fail(SRG_E_ARG, "line of %d samples exceeds 2^24", na);
+    return SRG_OK;
+}
+
+int fft_length(int na) {  // crossmul.f90:69-73: first 2^i >= na, i = 1..24
+    int n = 2;
+    while (n < na) n *= 2;
+    return n;
+}
+
+int run_stack(const float *const *slcs, int n, long long ld, int na, int nlines, int looksac,
+              int looksdn, float scale, int mask, float *const *igrams, float *const *amps,
+              void *stream) {
+    int rc = check_args(ld, na, nlines, looksac, looksdn);
+    if (rc) return rc;
+    if (n < 2 || !slcs || !igrams || !amps) return fail(SRG_E_ARG, "need >= 2 images and outputs");
+    for (int k = 0; k < n; ++k)
+        if (!slcs[k]) return fail(SRG_E_ARG, "null image %d", k);
+    for (int k = 0; k + 1 < n; ++k)
+        if (!igrams[k] || !amps[k]) return fail(SRG_E_ARG, "null output of pair %d", k);
+    int dev = 0;
+    CKC(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(SRG_E_ARG, "device %d out of range", dev);
+    XmCtx &x = g_xm[dev];
+    std::lock_guard<std::mutex> g(x.mu);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int nnn = fft_length(na);
+    const int nout_lines = nlines / looksdn, nout_cols = na / looksac;
+    const int nl = nout_lines * looksdn;
+    if ((rc = plan_for(x.fwd, nnn, nl)) || (rc = plan_for(x.inv, 2 * nnn, nl))) return rc;
+    const size_t up_bytes = (size_t)nl * 2 * nnn * sizeof(float2);
+    if ((rc = x.pad.ensure((size_t)nl * nnn * sizeof(float2))) || (rc = x.upA.ensure(up_bytes)) ||
+        (rc = x.upB.ensure(up_bytes)))
+        return rc;
+    float2 *cur = static_cast<float2 *>(x.upA.p), *nxt = static_cast<float2 *>(x.upB.p);
+    if ((rc = upsample(x, reinterpret_cast<const float2 *>(slcs[0]), ld, na, nnn, nl, scale, cur, st)))
+        return rc;
+    for (int k = 0; k + 1 < n; ++k) {
+        const float2 *a = reinterpret_cast<const float2 *>(slcs[k]);
+        const float2 *b = reinterpret_cast<const float2 *>(slcs[k + 1]);
+        if (b == a) {
+            CKC(cudaMemcpyAsync(nxt, cur, up_bytes, cudaMemcpyDeviceToDevice, st));
+        } else if ((rc = upsample(x, b, ld, na, nnn, nl, scale, nxt, st))) {
+            return rc;
+        }
+        crossmul_looks_kernel<<<grid_for((long long)nout_lines * nout_cols), 256, 0, st>>>(
+            cur, nxt, a, b, ld, nnn, nout_lines, nout_cols, looksac, looksdn, mask,
+            reinterpret_cast<float2 *>(igrams[k]), reinterpret_cast<float2 *>(amps[k]));
+        CKC(cudaGetLastError());
+        std::swap(cur, nxt);
+    }
+    return SRG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int srg_crossmul_device(const float *slc1, const float *slc2, long long ld, int na, int nlines,
+                        int looksac, int looksdn, float scale, int mask, float *igram, float *amp,
+                        void *stream) {
+    const float *s[2] = {slc1, slc2};
+    float *ig[1] = {igram};
+    float *am[1] = {amp};
+    return run_stack(s, 2, ld, na, nlines, looksac, looksdn, scale, mask, ig, am, stream);
+}
+
+int srg_crossmul_stack_device(const float *const *slcs, int n, long long ld, int na, int nlines,
+                              int looksac, int looksdn, float scale, int mask, float *const *igrams,
+                              float *const *amps, void *stream) {
+    return run_stack(slcs, n, ld, na, nlines, looksac, looksdn, scale, mask, igrams, amps, stream);
+}
+
+}  // extern "C"
