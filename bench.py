@@ -174,31 +174,36 @@ def phase_error(torch, wl):
             "amp_rel_rms": float(torch.sqrt((amp ** 2).mean())), "pixels": int(ph.numel())}
 
 
-def e2e_dropin(torch, wl, steps, form):
+def e2e_dropin(torch, wl, steps, form, separate=False):
     """End to end through azimuth_compress_ (the drop-in C ABI), one call per
     burst in acquisition order as the reference's driver makes them: burst
     lines in pinned host memory, the DEM and the .geo raster as files on tmpfs
-    (when it has room, else the temp dir).  Returns (s per step, h2d, d2h
-    bytes per step)."""
+    (when it has room, else the temp dir); `separate`: one .geo file per burst
+    (a stack of passes) instead of one scene raster.  Returns (s per step,
+    h2d, d2h bytes per step)."""
     from srg_b200 import api
     api.set_default_form(form)
     b0 = wl.bursts[0].b
     geo_bytes = b0.demlength * b0.demwidth * 8
     dem_bytes = b0.demlength * b0.demwidth * 2
+    nfiles = len(wl.bursts) if separate else 1
     tmp = None
     if os.path.isdir("/dev/shm"):
         st = os.statvfs("/dev/shm")
-        if st.f_bavail * st.f_frsize > 2 * (geo_bytes + dem_bytes):
+        if st.f_bavail * st.f_frsize > 2 * (nfiles * geo_bytes + dem_bytes):
             tmp = "/dev/shm"
     h2d = d2h = 0
     with tempfile.TemporaryDirectory(dir=tmp) as td:
         dem_path = os.path.join(td, "elevation.dem")
-        geo_path = os.path.join(td, "scene.geo")
         np.ascontiguousarray(b0.dem, np.int16).tofile(dem_path)
-        with open(geo_path, "wb") as f:
-            f.truncate(geo_bytes)
         fd_dem = os.open(dem_path, os.O_RDWR)
-        fd_geo = os.open(geo_path, os.O_RDWR)
+        fds = []
+        for i in range(nfiles):
+            geo_path = os.path.join(td, f"scene{i}.geo")
+            with open(geo_path, "wb") as f:
+                f.truncate(geo_bytes)
+            fds.append(os.open(geo_path, os.O_RDWR))
+        fd_of = (lambda i: fds[i]) if separate else (lambda i: fds[0])
         hosts = []
         try:
             for db in wl.bursts:
@@ -210,18 +215,19 @@ def e2e_dropin(torch, wl, steps, form):
                 ncols = max(0, min(lp, db.b.demwidth - 1) - fp + 1)
                 h2d += host.numel() * 8 + db.b.rawdatalines * 24 + nl * ncols * 2
                 d2h += nl * ncols * 8
-            for db, host in zip(wl.bursts, hosts):   # warm-up
-                api.azimuth_compress_files(db.b, fd_geo, fd_dem, burst=host.numpy())
+            for i, (db, host) in enumerate(zip(wl.bursts, hosts)):   # warm-up
+                api.azimuth_compress_files(db.b, fd_of(i), fd_dem, burst=host.numpy())
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             for _ in range(steps):
-                for db, host in zip(wl.bursts, hosts):
-                    api.azimuth_compress_files(db.b, fd_geo, fd_dem, burst=host.numpy())
+                for i, (db, host) in enumerate(zip(wl.bursts, hosts)):
+                    api.azimuth_compress_files(db.b, fd_of(i), fd_dem, burst=host.numpy())
             torch.cuda.synchronize()
             dt = (time.perf_counter() - t0) / steps
         finally:
             os.close(fd_dem)
-            os.close(fd_geo)
+            for fd in fds:
+                os.close(fd)
             del hosts
     return dt, h2d, d2h
 
@@ -246,6 +252,42 @@ def time_plan(torch, plan, steps, warmup, stream, stages=None, label="timed"):
     torch.cuda.synchronize()
     plan.sync(sp)
     return sum(e0.elapsed_time(e1) for e0, e1 in ev) / steps
+
+
+def stack_interferograms(torch, wl, s_slcs, d_slcs, stream, steps):
+    """Crossmul of the stack's sequential pairs (one stack call, timed with
+    CUDA events on `stream`), the interferometric phase error of the split
+    images against the FP64 images, and of the FP64 interferograms against
+    the injected deformation (4 pi / lambda times the pair's range change)."""
+    from srg_b200 import api
+    sp = stream.cuda_stream
+    outs = api.crossmul_stack(s_slcs, stream=sp)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(steps)]
+    for e0, e1 in ev:
+        e0.record(stream)
+        api.crossmul_stack(s_slcs, stream=sp, sync=False, outs=outs)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    ms = sum(e0.elapsed_time(e1) for e0, e1 in ev) / steps
+    igd, _ = api.crossmul_stack(d_slcs, stream=sp)
+    igs = torch.stack(outs[0]).to(torch.complex128)
+    igd = torch.stack(igd).to(torch.complex128)
+    amp = igd.abs()
+    rms = torch.sqrt((amp[amp > 0] ** 2).mean())
+    m = amp > 0.05 * rms
+    ph = torch.angle(igs[m] * igd[m].conj()) * 1e3
+    n = wl.extra["acquisitions"]
+    want = torch.from_numpy(wl.extra["range_change"]).to(igd.device, torch.float64)
+    want = want * (4.0 * np.pi / wl.extra["wvl"] / max(1, n - 1))
+    dt = torch.angle(igd * torch.exp(-1j * want)[None]) * 1e3
+    return {"ms_per_stack": ms, "pairs": n - 1, "looks": [1, 1],
+            "ifg_phase_error_vs_fp64": {"ph_rms_mrad": float(torch.sqrt((ph ** 2).mean())),
+                                        "ph_max_mrad": float(ph.abs().max()),
+                                        "pixels": int(ph.numel())},
+            "injected_deformation_phase_rms_mrad": float(torch.sqrt((want[m[0]] ** 2).mean()) * 1e3),
+            "fp64_ifg_vs_injected_deformation_rms_mrad": float(torch.sqrt((dt[m] ** 2).mean()))}
 
 
 def raster_phase_error(torch, a, ref):
@@ -336,7 +378,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c3", choices=["c1", "c3"])
+    ap.add_argument("--workload", default="c3", choices=["c1", "c3", "c4"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--shapes", default=None,
@@ -354,7 +396,7 @@ def main():
     torch.cuda.set_device(local)
     from srg_b200 import _lib, workloads
 
-    build = workloads.config3 if args.workload == "c3" else workloads.config1
+    build = {"c1": workloads.config1, "c3": workloads.config3, "c4": workloads.config4}[args.workload]
     if args.impl == "reference":
         wl = build(device=f"cuda:{local}")
         from srg_b200 import api
@@ -376,12 +418,13 @@ def main():
         print(json.dumps(line))
         return
 
-    wl = build(device=f"cuda:{local}", seed=(1003 if args.workload == "c3" else 1001) + rank)
+    wl = build(device=f"cuda:{local}", seed={"c1": 1001, "c3": 1003, "c4": 1004}[args.workload] + rank)
     stream = torch.cuda.Stream()
     fp32_peak = _lib.measure_fma_peak(False)
     fp64_peak = _lib.measure_fma_peak(True)
     tuned = {}
-    if args.workload == "c3":
+    ifg = None
+    if args.workload in ("c3", "c4"):
         plan = wl.plan
         if pinned:
             plan.set_form(_lib.FORM_SPLIT, pinned[0])
@@ -395,7 +438,10 @@ def main():
             if world > 1:
                 dist.barrier()
         s_kern = time_plan(torch, plan, args.steps, 1, stream, stages=2)
-        split_raster = wl.raster.clone()
+        if wl.raster is not None:
+            split_out = wl.raster.clone()
+        else:
+            split_out = torch.stack([db.out for db in wl.bursts])
         if pinned:
             plan.set_form(_lib.FORM_FP64, pinned[1])
             tuned["fp64"] = (pinned[1], None)
@@ -404,10 +450,18 @@ def main():
             tuned["fp64"] = plan.tune(iters=1)
         d_ms = time_plan(torch, plan, max(3, args.steps // 3), 1, stream)
         d_kern = d_ms
-        perr = raster_phase_error(torch, split_raster, wl.raster)
-        del split_raster
+        if wl.raster is not None:
+            perr = raster_phase_error(torch, split_out, wl.raster)
+        else:
+            fp64_out = torch.stack([db.out for db in wl.bursts])
+            perr = raster_phase_error(torch, split_out, fp64_out)
+            ifg = stack_interferograms(torch, wl, list(split_out), list(fp64_out), stream,
+                                       max(3, args.steps))
+            del fp64_out
+        del split_out
         plan.set_form(_lib.FORM_SPLIT, tuned["split"][0])
-        launches = 3  # azimuth centres, backprojection, merge (one graph per pass)
+        # azimuth centres, backprojection (and the ordered merge): one graph per pass
+        launches = 3 if wl.raster is not None else 2
     else:
         with ClockSampler(local) as clk:
             if world > 1:
@@ -424,7 +478,8 @@ def main():
         t = torch.tensor([s_ms, d_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         s_ms, d_ms = float(t[0]), float(t[1])
-    e2e_s, h2d, d2h = e2e_dropin(torch, wl, args.e2e_steps, _lib.FORM_SPLIT)
+    e2e_s, h2d, d2h = e2e_dropin(torch, wl, args.e2e_steps, _lib.FORM_SPLIT,
+                                 separate=args.workload == "c4")
     terms_all = wl.terms * world
     value = terms_all / (s_ms * 1e-3) / 1e9
     fp64_value = terms_all / (d_ms * 1e-3) / 1e9
@@ -443,19 +498,24 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": s_ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 (split; FP64 orbit/ECEF/reference range)",
-        "data": ("synthetic, seeded: complex Gaussian clutter + forward-projected point targets"
-                 if args.workload == "c3" else "synthetic, seeded: forward-projected scatterers"),
+        "data": {"c3": "synthetic, seeded: complex Gaussian clutter + forward-projected point targets",
+                 "c4": "synthetic, seeded: forward-projected scatterers + point targets, Mogi "
+                       "deformation, repeat-pass baselines",
+                 "c1": "synthetic, seeded: forward-projected scatterers"}[args.workload],
         "config": {"workload": wl.description, "bursts": len(wl.bursts),
                    "terms_per_step_per_gpu": wl.terms,
                    "l2": "range lines of every burst > 126 MB L2; no flush between steps",
                    "parallelism": f"replicas x{world} (one workload per GPU)",
                    "kernel_shapes": {k: _lib.tile_config_name(v[0]) for k, v in tuned.items()},
-                   "step": ("one graph replay: azimuth centres of every line, one persistent "
-                            "backprojection launch for all bursts, ordered merge into the scene raster")
-                   if args.workload == "c3" else "azimuth centres + backprojection of one burst"},
+                   "step": {"c3": "one graph replay: azimuth centres of every line, one persistent "
+                                  "backprojection launch for all bursts, ordered merge into the scene raster",
+                            "c4": "one graph replay: azimuth centres of every pass, one persistent "
+                                  "backprojection launch for all passes onto the common grid",
+                            "c1": "azimuth centres + backprojection of one burst"}[args.workload]},
         "fp64_form": {"value": fp64_value, "ms_per_step": d_ms, "kernel_ms": d_kern,
                       "split_over_fp64": value / fp64_value},
         "phase_error_vs_fp64": perr,
+        **({"crossmul": ifg} if ifg is not None else {}),
         "roofline": {"bound": "fp32-issue", "achieved": achieved, "peak": fp32_peak,
                      "unit": "TFLOP/s", "frac": achieved / fp32_peak,
                      "traffic": traffic, "flops_per_term": FLOPS_PER_TERM,
@@ -466,7 +526,8 @@ def main():
         "cpu_baseline": cpu,
         "e2e": {"value": terms_all / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "s_per_step": e2e_s,
-                "path": "azimuth_compress_ (33-arg C ABI), pinned host burst, tmpfs DEM/.geo"},
+                "path": "azimuth_compress_ (33-arg C ABI), pinned host burst, tmpfs DEM/.geo"
+                        + (" (one .geo per pass)" if args.workload == "c4" else "")},
         "gpu_launches": launches * args.steps,
         "clocks": clk.summary(),
         "setup_s": wl.setup_s,

@@ -238,13 +238,16 @@ int srg_tile_config(int idx, int *tile_x, int *tile_y, int *threads, int *chunk,
 const char *srg_tile_config_name(int idx);
 
 /* Synthetic-scene support: forward-project a per-pixel reflectivity field
- * (complex64, [nlines][dem_ld-aligned W] of the burst's grid, device) into
+ * (complex64, [nlines][refl_ld] of the burst's grid rows, device) into
  * the burst's range lines (accumulates into burst, device), with a
  * sinc^2 azimuth antenna pattern of length `antenna_m`, a linear range
- * response and FP64 geometry.  Atomic accumulation: not bit-reproducible. */
+ * response and FP64 geometry.  `range_offset` (nullable, float metres,
+ * [nlines][refl_ld], device) lengthens each scatterer's range, e.g. by its
+ * line-of-sight surface motion.  Atomic accumulation: not bit-reproducible.
+ * No reference counterpart (the reference processes recorded data). */
 int srg_forward_project_device(const srg_burst_desc *b, const float *refl,
                                int64_t refl_ld, const double *satvel,
-                               double antenna_m, void *stream);
+                               double antenna_m, const float *range_offset, void *stream);
 
 /* ---- Interferogram formation (replaces the crossmul program,
  * int/crossmul.f90:95-185, which SRG runs on pairs of .geo files) ----

@@ -89,7 +89,7 @@ _SIGS = {
     "srg_tile_config": (C.c_int, [C.c_int, _ip, _ip, _ip, _ip, _ip]),
     "srg_tile_config_name": (C.c_char_p, [C.c_int]),
     "srg_forward_project_device": (C.c_int, [C.POINTER(BurstDesc), C.c_void_p, C.c_int64, C.c_void_p,
-                                             C.c_double, C.c_void_p]),
+                                             C.c_double, C.c_void_p, C.c_void_p]),
     "srg_crossmul_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong, C.c_int, C.c_int, C.c_int,
                                       C.c_int, C.c_float, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "srg_crossmul_stack_device": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_longlong, C.c_int,

@@ -225,11 +225,19 @@ def merge(dst, src, stream=None) -> None:
                                  C.c_void_p(_stream_ptr(stream))))
 
 
-def forward_project(db: DeviceBurst, refl, satvel, antenna: float = 10.0, stream=None) -> None:
-    """Accumulate the echo of a per-pixel reflectivity field into db.burst."""
+def forward_project(db: DeviceBurst, refl, satvel, antenna: float = 10.0, stream=None,
+                    range_offset=None) -> None:
+    """Accumulate the echo of a per-pixel reflectivity field into db.burst;
+    range_offset: optional float32 tensor of the same shape as refl (metres
+    added to each scatterer's range)."""
     d = db.desc()
+    ro = 0
+    if range_offset is not None:
+        if range_offset.shape != refl.shape or range_offset.stride(0) != refl.stride(0):
+            raise ValueError("range_offset must match refl's shape and row stride")
+        ro = range_offset.data_ptr()
     check(lib().srg_forward_project_device(C.byref(d), C.c_void_p(refl.data_ptr()), refl.stride(0),
-                                           C.c_void_p(satvel.data_ptr()), antenna,
+                                           C.c_void_p(satvel.data_ptr()), antenna, C.c_void_p(ro),
                                            C.c_void_p(_stream_ptr(stream))))
 
 

@@ -503,7 +503,8 @@ int srg_pulse_orbit_device(const double *times, int P, const double *timeorbit, 
 }
 
 int srg_forward_project_device(const srg_burst_desc *b, const float *refl, int64_t refl_ld,
-                               const double *satvel, double antenna_m, void *stream) {
+                               const double *satvel, double antenna_m, const float *range_offset,
+                               void *stream) {
     if (!b || !refl || !satvel) return fail(SRG_E_ARG, "bad arguments");
     int rc = validate_desc(*b);
     if (rc) return rc;
@@ -512,7 +513,7 @@ int srg_forward_project_device(const srg_burst_desc *b, const float *refl, int64
     if (rc) return rc;
     BurstDev B = make_burst_dev(*b, nullptr);
     CK(launch_forward_project(B, reinterpret_cast<const float2 *>(refl), refl_ld, satvel,
-                              antenna_m, static_cast<cudaStream_t>(stream)));
+                              antenna_m, range_offset, static_cast<cudaStream_t>(stream)));
     return SRG_OK;
 }
 

@@ -177,7 +177,8 @@ __global__ void pulse_orbit_kernel(const double *times, int P, Orbit o, double *
 // to the two range bins around R of every pulse (the adjoint of linear
 // interpolation).  FP64 geometry; atomic accumulation.
 __global__ void forward_project_kernel(BurstDev B, const float2 *refl, long long refl_ld,
-                                       const double *satvel, double antenna) {
+                                       const double *satvel, double antenna,
+                                       const float *range_offset) {
     const int nx = B.lastpix_eff - B.firstpix + 1;
     const long long npix = (long long)nx * B.nlines;
     const double pi = 3.141592653589793;
@@ -189,17 +190,20 @@ __global__ void forward_project_kernel(BurstDev B, const float2 *refl, long long
     if (a.x == 0.f && a.y == 0.f) return;
     double X[3];
     pixel_ecef(B, line, px, (double)B.dem[(long long)line * B.dem_ld + px], X[0], X[1], X[2]);
+    // extra two-way path of the scatterer (e.g. surface motion along the line of sight)
+    const double dR = range_offset ? (double)range_offset[(long long)line * refl_ld + px] : 0.0;
     const double wvl = 2.0 / B.K;
     float2 *out = const_cast<float2 *>(B.burst);
     for (int k = 0; k < B.P; ++k) {
         const double *s = B.satloc + 3 * k;
         const double dx = X[0] - s[0], dy = X[1] - s[1], dz = X[2] - s[2];
-        const double R = sqrt(dx * dx + dy * dy + dz * dz);
+        const double R0 = sqrt(dx * dx + dy * dy + dz * dz);
+        const double R = R0 + dR;
         const double r = (R - B.rngstart) * B.inv_dmrg;
         if (!(r >= 0.0 && r < (double)(B.S - 1))) continue;
         const double *v = satvel + 3 * k;
         const double vn = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
-        const double spsi = (dx * v[0] + dy * v[1] + dz * v[2]) / (vn * R);
+        const double spsi = (dx * v[0] + dy * v[1] + dz * v[2]) / (vn * R0);
         const double arg = pi * antenna * spsi / wvl;
         const double sc = fabs(arg) < 1e-12 ? 1.0 : sin(arg) / arg;
         const double w = sc * sc;
@@ -347,11 +351,12 @@ cudaError_t launch_pulse_orbit(const double *times, int P, const Orbit &o, doubl
 }
 
 cudaError_t launch_forward_project(const BurstDev &B, const float2 *refl, long long refl_ld,
-                                   const double *satvel, double antenna, cudaStream_t st) {
+                                   const double *satvel, double antenna, const float *range_offset,
+                                   cudaStream_t st) {
     const long long npix = (long long)(B.lastpix_eff - B.firstpix + 1) * B.nlines;
     if (npix <= 0) return cudaSuccess;
     forward_project_kernel<<<(int)((npix + 127) / 128), 128, 0, st>>>(B, refl, refl_ld, satvel,
-                                                                       antenna);
+                                                                       antenna, range_offset);
     return cudaGetLastError();
 }
 

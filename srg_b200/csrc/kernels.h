@@ -48,7 +48,8 @@ cudaError_t launch_merge(float2 *dst, long long dst_ld, const float2 *src, long 
 cudaError_t launch_pulse_orbit(const double *times, int P, const Orbit &o, double *pos,
                                double *vel, cudaStream_t st);
 cudaError_t launch_forward_project(const BurstDev &B, const float2 *refl, long long refl_ld,
-                                   const double *satvel, double antenna, cudaStream_t st);
+                                   const double *satvel, double antenna, const float *range_offset,
+                                   cudaStream_t st);
 
 cudaError_t launch_fma_peak(int fp64, int blocks, int iters, void *sink, cudaStream_t st);
 

@@ -362,8 +362,10 @@ def make_geometry(*, pulses: int, samples: int, width: int, length: int, spacing
                   centre_height: float = 0.0, aperture: Optional[int] = None,
                   angc0: float = 0.0, angc1: float = 0.0, quantise: bool = True,
                   grid_centre: Optional[tuple] = None, orbit: Optional[CircularOrbit] = None,
-                  along_offset: float = 0.0) -> Burst:
-    """Orbit, pulses and grid of one burst; samples are left zero."""
+                  along_offset: float = 0.0, position_offset=None) -> Burst:
+    """Orbit, pulses and grid of one burst; samples are left zero.
+    along_offset (s) shifts the pulse times along the orbit; position_offset
+    (ECEF metres) displaces every state vector (a repeat-pass baseline)."""
     if orbit is None:
         inc = math.radians(ORBIT_INCL_DEG)
         u0 = math.asin(math.sin(math.radians(lat0)) / math.sin(inc))
@@ -375,6 +377,8 @@ def make_geometry(*, pulses: int, samples: int, width: int, length: int, spacing
     t0 = math.floor((tstart - 30.0) / SV_SPACING) * SV_SPACING + SV_SPACING
     timeorbit = t0 + SV_SPACING * np.arange(11, dtype=np.float64)
     xx, vv = orbit.state(timeorbit)
+    if position_offset is not None:
+        xx = xx + np.asarray(position_offset, np.float64)[None, :]
     ptime = tstart + np.arange(pulses, dtype=np.float64) * dtaz
     sx, sv = interp_pulses(timeorbit, xx, vv, ptime)
     if quantise:
@@ -414,6 +418,48 @@ def grid_ecef(b: Burst, lines, pixels, heights):
     lat = b.firstlat + np.asarray(lines, np.float64) * b.deltalat
     lon = b.firstlon + np.asarray(pixels, np.float64) * b.deltalon
     return llh_to_ecef(lat, lon, np.asarray(heights, np.float64))
+
+
+def grid_centre(b: Burst):
+    """(lat, lon) of the grid's centre pixel."""
+    return (b.firstlat + 0.5 * (b.demlength - 1) * b.deltalat,
+            b.firstlon + 0.5 * (b.demwidth - 1) * b.deltalon)
+
+
+def baseline_frame(b: Burst):
+    """Unit vector normal to both the line of sight to the grid centre and
+    the velocity at mid-burst (the direction of a perpendicular baseline),
+    and the orbital speed (m/s)."""
+    clat, clon = grid_centre(b)
+    h = float(b.dem[b.demlength // 2, b.demwidth // 2]) if b.dem is not None else 0.0
+    p = llh_to_ecef(clat, clon, h)
+    los = p - b.xyz_mid
+    los /= np.linalg.norm(los)
+    v = np.asarray(b.vel_mid, np.float64)
+    e = np.cross(los, v / np.linalg.norm(v))
+    return e / np.linalg.norm(e), float(np.linalg.norm(v))
+
+
+def mogi_range_change(b: Burst, depth: float = 3000.0, los_max: float = 0.10) -> np.ndarray:
+    """Range change (m, float32 [demlength][demwidth]) of every grid pixel due
+    to a Mogi point source `depth` metres below the ellipsoid under the grid
+    centre: surface displacement u = C (x - s) / |x - s|^3 (the point-source
+    field of an elastic half-space, Mogi 1958), projected on the unit vector
+    from the pixel to the mid-burst satellite position, negated (uplift toward
+    the radar shortens the range), scaled so that max |change| = los_max."""
+    L, W = b.demlength, b.demwidth
+    clat, clon = grid_centre(b)
+    src = llh_to_ecef(clat, clon, -depth)
+    lat = b.firstlat + np.arange(L, dtype=np.float64)[:, None] * b.deltalat
+    lon = b.firstlon + np.arange(W, dtype=np.float64)[None, :] * b.deltalon
+    P = llh_to_ecef(np.broadcast_to(lat, (L, W)), np.broadcast_to(lon, (L, W)),
+                    b.dem.astype(np.float64))
+    d = P - src
+    u = d / (np.linalg.norm(d, axis=-1, keepdims=True) ** 3)
+    s = np.asarray(b.xyz_mid, np.float64) - P
+    s /= np.linalg.norm(s, axis=-1, keepdims=True)
+    dr = -(u * s).sum(-1)
+    return (dr * (los_max / np.abs(dr).max())).astype(np.float32)
 
 
 # --------------------------------------------------------------------------

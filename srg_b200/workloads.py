@@ -32,6 +32,7 @@ class Workload:
     description: str
     raster: object = None    # scene raster (device) the bursts merge into, if any
     grid: object = None      # scene.SceneGrid of a multi-burst scene
+    extra: dict = dataclasses.field(default_factory=dict)  # workload-specific arrays
 
     def descs_bytes(self):
         """Bytes a host-resident copy of the step inputs/outputs moves."""
@@ -146,4 +147,67 @@ def config3(device="cuda", seed: int = 1003, ntargets: int = 200, target_db: flo
     host_dem = dem_dev.cpu().numpy()
     for b in bursts:
         b.dem = host_dem
+    return wl
+
+
+def config4(device="cuda", seed: int = 1004, acquisitions: int = 32, bperp_max: float = 150.0,
+            along_max: float = 5.0, los_max: float = 0.10, depth: float = 3000.0,
+            ntargets: int = 200, target_db: float = 30.0, form=None) -> Workload:
+    """Repeat-pass stack: `acquisitions` passes over the config-1 footprint
+    (1,500 pulses x 21,000 bins each, common 2,400 x 1,200 grid at 1e-4 deg
+    over the volcano DEM).  Pass k has its state vectors displaced by a
+    perpendicular baseline drawn from U[-bperp_max, bperp_max] m and its pulse
+    times shifted by an along-track offset from U[-along_max, along_max] m;
+    the scene (one circular Gaussian scatterer per grid pixel plus point
+    targets at +30 dB, identical in every pass) has moved by k/(n-1) of a Mogi
+    source's range change (depth 3 km below the summit, max 10 cm of line of
+    sight).  All passes form one scene plan without a raster: one batched
+    backprojection launch writes every pass's image on the common grid."""
+    import torch
+    from . import _lib
+    t0 = time.time()
+    base = scene.config1_geometry(seed=seed)
+    rng = np.random.default_rng(seed)
+    e_perp, speed = scene.baseline_frame(base)
+    bperp = rng.uniform(-bperp_max, bperp_max, acquisitions)
+    along = rng.uniform(-along_max, along_max, acquisitions)
+    bperp[0] = along[0] = 0.0  # the first pass is the reference orbit
+    drange = scene.mogi_range_change(base, depth=depth, los_max=los_max)
+    L, W = base.demlength, base.demwidth
+    dem_t = torch.from_numpy(np.ascontiguousarray(base.dem)).to(device)
+    refl = _reflectivity(torch, (L, W), seed, device)
+    amp = 10.0 ** (target_db / 20.0)
+    lines = rng.integers(0, L, ntargets)
+    pix = rng.integers(0, W, ntargets)
+    refl[torch.from_numpy(lines).to(device), torch.from_numpy(pix).to(device)] = amp
+    dr_t = torch.from_numpy(drange).to(device)
+    dbs = []
+    for k in range(acquisitions):
+        b = scene.make_geometry(pulses=base.rawdatalines, samples=base.samples, width=W, length=L,
+                                spacing=abs(base.deltalat), centre_height=1000.0,
+                                grid_centre=scene.grid_centre(base),
+                                position_offset=bperp[k] * e_perp, along_offset=along[k] / speed)
+        # the common grid, to the bit
+        b.firstlat, b.firstlon, b.latlons = base.firstlat, base.firstlon, base.latlons.copy()
+        b.dem = base.dem
+        bt = torch.zeros((b.rawdatalines, b.samples), dtype=torch.complex64, device=device)
+        db = api.to_device(b, device=device, burst_tensor=bt, dem_tensor=dem_t)
+        rows = slice(db.firstline, db.firstline + db.nlines)
+        offs = (dr_t[rows] * (k / max(1, acquisitions - 1))).contiguous()
+        satvel = torch.from_numpy(np.ascontiguousarray(b.satvel)).to(device)
+        api.forward_project(db, refl[rows], satvel, range_offset=offs)
+        dbs.append(db)
+    torch.cuda.synchronize(device)
+    sc = api.Scene(dbs, raster=None, form=_lib.FORM_SPLIT if form is None else form)
+    terms = sc.terms()
+    wl = Workload("c4", dbs, [], terms, time.time() - t0,
+                  f"repeat-pass stack: {acquisitions} passes of 1500 x 21000 complex64 "
+                  f"({sum(db.burst.numel() * 8 for db in dbs) / 1e9:.2f} GB) onto a common "
+                  f"{W}x{L} grid at 1e-4 deg, perpendicular baselines U[+-{bperp_max:g} m], "
+                  f"along-track U[+-{along_max:g} m], Mogi source {depth / 1000:g} km deep, "
+                  f"{los_max * 100:g} cm max LOS growing linearly; then crossmul of "
+                  f"{acquisitions - 1} sequential pairs")
+    wl.plan = sc
+    wl.extra = {"range_change": drange, "bperp": bperp, "along": along,
+                "wvl": base.wvl, "acquisitions": acquisitions}
     return wl
