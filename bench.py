@@ -324,6 +324,18 @@ class quiet_stdout:
         os.close(self.null)
 
 
+def combine_ranks(torch, dist, device, maxes, sums):
+    """Max over ranks of `maxes` and sum over ranks of `sums` (lists of
+    numbers); identity without a process group (dist None)."""
+    if dist is None:
+        return list(maxes), list(sums)
+    t = torch.tensor([float(x) for x in maxes], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    u = torch.tensor([float(x) for x in sums], dtype=torch.float64, device=device)
+    dist.all_reduce(u, op=dist.ReduceOp.SUM)
+    return t.tolist(), u.tolist()
+
+
 def reference_cpu_sample(wl, budget_s: float = 15.0):
     """Time the reference CPU backprojection (oracle/_ref, compiled from the
     reference sources, unmodified) end to end on a slab of grid lines of the
@@ -474,13 +486,12 @@ def main():
         d_ms, d_kern, _ = time_steps(torch, wl, _lib.FORM_FP64, max(3, args.steps // 2),
                                      args.warmup, stream)
         perr = phase_error(torch, wl)
-    if world > 1:
-        t = torch.tensor([s_ms, d_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        s_ms, d_ms = float(t[0]), float(t[1])
     e2e_s, h2d, d2h = e2e_dropin(torch, wl, args.e2e_steps, _lib.FORM_SPLIT,
                                  separate=args.workload == "c4")
-    terms_all = wl.terms * world
+    # whole job: the slowest rank's times, every rank's terms and bytes
+    (s_ms, d_ms, e2e_s), (terms_all, h2d, d2h) = combine_ranks(
+        torch, dist if world > 1 else None, "cuda", [s_ms, d_ms, e2e_s], [wl.terms, h2d, d2h])
+    terms_all, h2d, d2h = int(terms_all), int(h2d), int(d2h)
     value = terms_all / (s_ms * 1e-3) / 1e9
     fp64_value = terms_all / (d_ms * 1e-3) / 1e9
     achieved = FLOPS_PER_TERM * wl.terms / (s_kern * 1e-3) / 1e12
