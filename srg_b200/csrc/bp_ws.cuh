@@ -206,7 +206,16 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
     uint32_t issued = 0, issued_par = 0;  // producer lane 0: stages with a TMA issued this tile
 
     for (;;) {
-        if (tid == 0) ctl.item = atomicAdd(work_counter, 1);
+        if (tid == 0) {
+            ctl.item = atomicAdd(work_counter, 1);
+            ctl.kmin = INT_MAX;
+            ctl.kmax = INT_MIN;
+            ctl.azs_max = INT_MIN;
+            ctl.aze_min = INT_MAX;
+            ctl.bmin = INT_MAX;
+            ctl.bmax = INT_MIN;
+            ctl.dmax_bits = 0;
+        }
         __syncthreads();
         const int item = ctl.item;
         if (item >= total_tiles) break;
@@ -217,29 +226,13 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
         const int px0 = B.firstpix + (ti % B.tiles_x) * TX;
         const int ly0 = (ti / B.tiles_x) * TY;
 
-        // ---- prologue (all threads) ----
-        static_assert(TX + TY <= (NC + 1) * 32, "one thread per table row");
-        if (tid < TY) {
-            const LineTrig L = line_trig(B, ly0 + tid);
-            lat_tab[tid][0] = L.slat;
-            lat_tab[tid][1] = L.clat;
-            lat_tab[tid][2] = L.re;
-            lat_tab[tid][3] = L.rez;
-        } else if (tid < TY + TX) {
-            col_trig(B, px0 + tid - TY, lon_tab[tid - TY][0], lon_tab[tid - TY][1]);
-        }
-        if (tid == 0) {
-            ctl.kmin = INT_MAX;
-            ctl.kmax = INT_MIN;
-            ctl.azs_max = INT_MIN;
-            ctl.aze_min = INT_MAX;
-            ctl.bmin = INT_MAX;
-            ctl.bmax = INT_MIN;
-            ctl.dmax_bits = 0;
-        }
-        __syncthreads();
+        // ---- prologue ----
+        // Phase A: consumers solve their pixels' aperture windows; the producer
+        // warp, idle until the tile's pulse range is known, builds the tile's
+        // line / column ECEF factors and the tile-centre position.
         double X[M][3];
         int azs[M], aze[M];
+        short hgt[M];
         if (!producer) {
             int k0 = INT_MAX, k1 = INT_MIN, smax = INT_MIN, emin = INT_MAX;
 #pragma unroll
@@ -249,10 +242,9 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                 const int px = px0 + x, line = ly0 + y;
                 X[m][0] = X[m][1] = X[m][2] = 0.0;
                 azs[m] = aze[m] = 0;
+                hgt[m] = 0;
                 if (px <= B.lastpix_eff && line < B.nlines) {
-                    const double h = (double)B.dem[(long long)line * B.dem_ld + px];
-                    pixel_ecef_from(lat_tab[y][0], lat_tab[y][1], lat_tab[y][2], lat_tab[y][3],
-                                    lon_tab[x][0], lon_tab[x][1], h, X[m][0], X[m][1], X[m][2]);
+                    hgt[m] = B.dem[(long long)line * B.dem_ld + px];
                     pixel_window(B, pixel_azoff(B, B.coef + 3 * line, px), azs[m], aze[m]);
                     if (aze[m] > azs[m]) {
                         k0 = min(k0, azs[m]);
@@ -272,6 +264,29 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                 atomicMax(&ctl.azs_max, smax);
                 atomicMin(&ctl.aze_min, emin);
             }
+        } else {
+            for (int r = lane; r < TY + TX; r += 32) {
+                if (r < TY) {
+                    const LineTrig L = line_trig(B, ly0 + r);
+                    lat_tab[r][0] = L.slat;
+                    lat_tab[r][1] = L.clat;
+                    lat_tab[r][2] = L.re;
+                    lat_tab[r][3] = L.rez;
+                } else {
+                    col_trig(B, px0 + r - TY, lon_tab[r - TY][0], lon_tab[r - TY][1]);
+                }
+            }
+            __syncwarp();
+            if (lane == 0) {
+                // tile-centre pixel (inside the tile, so its factors are in the tables)
+                const int cx = min(max(px0 + TX / 2, B.firstpix), B.lastpix_eff);
+                const int cy = min(ly0 + TY / 2, B.nlines - 1);
+                const int ty = cy - ly0, tx = cx - px0;
+                pixel_ecef_from(lat_tab[ty][0], lat_tab[ty][1], lat_tab[ty][2], lat_tab[ty][3],
+                                lon_tab[tx][0], lon_tab[tx][1],
+                                (double)B.dem[(long long)cy * B.dem_ld + cx], ctl.xc[0], ctl.xc[1],
+                                ctl.xc[2]);
+            }
         }
         __syncthreads();
         const int kmin = ctl.kmin, kmax = ctl.kmax;
@@ -289,28 +304,38 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
             __syncthreads();
             continue;
         }
-        if (tid == 0) {
-            const int cx = min(max(px0 + TX / 2, B.firstpix), B.lastpix_eff);
-            const int cy = min(ly0 + TY / 2, B.nlines - 1);
-            double xc[3];
-            pixel_ecef(B, cy, cx, (double)B.dem[(long long)cy * B.dem_ld + cx], xc[0], xc[1], xc[2]);
-            ctl.xc[0] = xc[0];
-            ctl.xc[1] = xc[1];
-            ctl.xc[2] = xc[2];
+        // Phase B: consumers place their formed pixels; the producer's lane 0
+        // derives the ranges and look vectors of the tile centre at the first
+        // and last pulse and the compensated seed of the look vector.
+        if (!producer) {
+#pragma unroll
+            for (int m = 0; m < M; ++m) {
+                if (aze[m] > azs[m]) {
+                    const int bi = warp + NC * m;
+                    const int x = 8 * (bi % BX) + (lane & 7), y = 4 * (bi / BX) + (lane >> 3);
+                    pixel_ecef_from(lat_tab[y][0], lat_tab[y][1], lat_tab[y][2], lat_tab[y][3],
+                                    lon_tab[x][0], lon_tab[x][1], (double)hgt[m], X[m][0], X[m][1],
+                                    X[m][2]);
+                }
+            }
+        } else if (lane == 0) {
+            const double xc[3] = {ctl.xc[0], ctl.xc[1], ctl.xc[2]};
             const double *s0 = B.satloc + 3 * kmin;
             const double *s1 = B.satloc + 3 * (kmax - 1);
             const double u0 = xc[0] - s0[0], u1 = xc[1] - s0[1], u2 = xc[2] - s0[2];
             const double r0 = sqrt(u0 * u0 + u1 * u1 + u2 * u2);
             const double v0 = xc[0] - s1[0], v1 = xc[1] - s1[1], v2 = xc[2] - s1[2];
+            const double r1 = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
             ctl.rc0 = r0;
-            ctl.rc1 = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
-            const double uu[3] = {u0 / r0, u1 / r0, u2 / r0};
+            ctl.rc1 = r1;
+            const double i0 = 1.0 / r0, i1 = 1.0 / r1;
+            const double uu[3] = {u0 * i0, u1 * i0, u2 * i0};
             ctl.ua[0] = uu[0];
             ctl.ua[1] = uu[1];
             ctl.ua[2] = uu[2];
-            ctl.ub[0] = v0 / ctl.rc1;
-            ctl.ub[1] = v1 / ctl.rc1;
-            ctl.ub[2] = v2 / ctl.rc1;
+            ctl.ub[0] = v0 * i1;
+            ctl.ub[1] = v1 * i1;
+            ctl.ub[2] = v2 * i1;
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
                 const float hi = __double2float_rn(uu[c]);
@@ -324,8 +349,13 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
         if (!producer) {
             int lb0 = INT_MAX, lb1 = INT_MIN;
             float dmx = 0.f;
-            const double *s0 = B.satloc + 3 * kmin;
-            const double *s1 = B.satloc + 3 * (kmax - 1);
+            // bin offsets of the pixel from the tile centre at the tile's first and
+            // last pulse, to second order in d = x - x_c (error < 1e-4 m at
+            // |d| < 1 km; the window keeps a bin of margin on both sides)
+            const float ua0 = (float)ctl.ua[0], ua1 = (float)ctl.ua[1], ua2 = (float)ctl.ua[2];
+            const float ub0 = (float)ctl.ub[0], ub1 = (float)ctl.ub[1], ub2 = (float)ctl.ub[2];
+            const float h0 = (float)(0.5 / ctl.rc0), h1 = (float)(0.5 / ctl.rc1);
+            const float invd = B.inv_dmrg_f;
 #pragma unroll
             for (int m = 0; m < M; ++m) {
                 accr[m] = acci[m] = 0.f;
@@ -333,28 +363,25 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                 d[m][0] = d[m][1] = d[m][2] = 0.f;
                 dd[m] = cph[m] = whi[m] = dwa[m] = 0.f;
                 if (aze[m] > azs[m]) {
-                    const double a0 = X[m][0] - s0[0], a1 = X[m][1] - s0[1], a2 = X[m][2] - s0[2];
-                    const double c0 = X[m][0] - s1[0], c1 = X[m][1] - s1[1], c2 = X[m][2] - s1[2];
-                    const double e0 = (sqrt(a0 * a0 + a1 * a1 + a2 * a2) - ctl.rc0) * B.inv_dmrg;
-                    const double e1 = (sqrt(c0 * c0 + c1 * c1 + c2 * c2) - ctl.rc1) * B.inv_dmrg;
-                    lb0 = min(lb0, (int)floor(fmin(e0, e1)));
-                    lb1 = max(lb1, (int)ceil(fmax(e0, e1)));
-                    const double q0 = X[m][0] - ctl.xc[0], q1 = X[m][1] - ctl.xc[1],
-                                 q2 = X[m][2] - ctl.xc[2];
-                    dmx = fmaxf(dmx, (float)sqrt(q0 * q0 + q1 * q1 + q2 * q2) * 1.0001f);
-                    if (FORM == FORM_SPLIT) {
-                        float dh[3], dl[3];
+                    float dh[3], dl[3];
 #pragma unroll
-                        for (int q = 0; q < 3; ++q) {
-                            const double dv = X[m][q] - ctl.xc[q];
-                            dh[q] = __double2float_rn(dv);
-                            dl[q] = __double2float_rn(dv - (double)dh[q]);
-                            d[m][q] = dh[q];
-                        }
-                        dd[m] = fmaf(dh[0], dh[0], fmaf(dh[1], dh[1], dh[2] * dh[2]));
+                    for (int q = 0; q < 3; ++q) {
+                        const double dv = X[m][q] - ctl.xc[q];
+                        dh[q] = __double2float_rn(dv);
+                        dl[q] = __double2float_rn(dv - (double)dh[q]);
+                        d[m][q] = dh[q];
+                    }
+                    dd[m] = fmaf(dh[0], dh[0], fmaf(dh[1], dh[1], dh[2] * dh[2]));
+                    const float wa = fmaf(dh[0], ua0, fmaf(dh[1], ua1, dh[2] * ua2));
+                    const float wb = fmaf(dh[0], ub0, fmaf(dh[1], ub1, dh[2] * ub2));
+                    const float e0 = fmaf(fmaf(-wa, wa, dd[m]), h0, wa) * invd;
+                    const float e1 = fmaf(fmaf(-wb, wb, dd[m]), h1, wb) * invd;
+                    lb0 = min(lb0, (int)floorf(fminf(e0, e1)));
+                    lb1 = max(lb1, (int)ceilf(fmaxf(e0, e1)));
+                    dmx = fmaxf(dmx, sqrtf(dd[m]) * 1.0001f);
+                    if (FORM == FORM_SPLIT)
                         cph[m] = (float)kTwoPi * seed_phase(dh, dl, ctl.seed_hi, ctl.seed_lo, B.K_hi,
                                                             B.K_lo, &whi[m], &dwa[m]);
-                    }
                 }
             }
             lb0 = warp_min(lb0);
@@ -425,7 +452,8 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                 const double f = (double)(k - kmin) * span;
                 const double gx = ex - (uax + f * dux), gy = ey - (uay + f * duy),
                              gz = ez - (uaz + f * duz);
-                const float dev = act ? (float)(sqrt(gx * gx + gy * gy + gz * gz) * dev_scale) : 0.f;
+                const float dev =
+                    act ? sqrtf((float)(gx * gx + gy * gy + gz * gz)) * (float)dev_scale * 1.0001f : 0.f;
                 const int lo = __reduce_min_sync(0xffffffffu, act ? (int)floor(rbabs) : INT_MAX);
                 const int hi = __reduce_max_sync(0xffffffffu, act ? (int)ceil(rbabs) : INT_MIN);
                 const int devmax = __reduce_max_sync(0xffffffffu, __float_as_int(dev));
@@ -449,8 +477,9 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                     hv.dmx = __double2float_rn(__shfl_sync(0xffffffffu, nx - ex, nk / 2));
                     hv.dmy = __double2float_rn(__shfl_sync(0xffffffffu, ny - ey, nk / 2));
                     hv.dmz = __double2float_rn(__shfl_sync(0xffffffffu, nz - ez, nk / 2));
-                    hv.inv2R = __double2float_rn(0.5 / Rmid);
-                    hv.c2 = __double2float_rn(0.5 / (Rmid * Rmid));
+                    const float rm = (float)Rmid;
+                    hv.inv2R = 0.5f / rm;
+                    hv.c2 = hv.inv2R / rm;
                 }
                 hv.poly = 0;
                 hv.r0 = hv.r1 = hv.r2 = hv.p0 = hv.p1 = hv.p2 = 0.f;
@@ -514,7 +543,7 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                         __int_as_float(__reduce_max_sync(0xffffffffu, __float_as_int(act ? err : 0.f)));
                     hv.poly = (nk >= 3 && (double)resmax * kTwoPi * B.K < kPolyTolRad) ? 1 : 0;
                 }
-                if (!mbar_wait_backoff(&ctl.empty[s], (r & 1) ^ 1)) {
+                if (!mbar_wait_bounded(&ctl.empty[s], (r & 1) ^ 1)) {
                     ctl.abort = 1;
                     break;
                 }

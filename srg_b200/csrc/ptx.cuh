@@ -86,19 +86,6 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
     return false;
 }
 
-// Bounded wait that backs off between polls (for a warp that is usually
-// ahead and would otherwise take issue slots from the warps it waits for).
-// At most kSpinLimit polls of at most 256 ns each.
-__device__ __forceinline__ bool mbar_wait_backoff(uint64_t *bar, uint32_t parity) {
-    uint32_t ns = 32;
-    for (uint32_t i = 0; i < kSpinLimit; ++i) {
-        if (mbar_try_wait(bar, parity)) return true;
-        __nanosleep(ns);
-        ns = ns < 256 ? 2 * ns : 256;
-    }
-    return false;
-}
-
 // 2D tiled TMA load of box {box_x, box_y} at element coordinates (x, y) into
 // shared memory, completing on `bar` (byte count set by the caller).  The
 // tensor map lives in global memory, written by the host before launch.
