@@ -90,6 +90,14 @@ constexpr double kPolyTolRad = 1e-4;
 // rounded toward -inf leaves floor(t) in the low mantissa bits.
 constexpr float kFloorMagic = 12582912.f;
 constexpr int kFloorMagicBits = 0x4B400000;
+// Width (pixels across) of the block of 32 pixels a warp owns per slot.  The
+// two taps of a lane are 8-byte words of one staged row; lanes of a half-warp
+// whose bins differ by a multiple of 16 share shared-memory banks, so narrow
+// blocks (fewer range bins per half-warp) conflict less.
+#ifndef SRG_PIX_BLOCK_X
+#define SRG_PIX_BLOCK_X 4
+#endif
+constexpr int kPixBlockX = SRG_PIX_BLOCK_X;
 
 // Per-pulse parameters of one chunk (split: 2 x float4; FP64: satloc + pad).
 template <int FORM>
@@ -172,8 +180,10 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
       int *__restrict__ err, int /* window, = WB */) {
     constexpr int NCT = NC * 32;
     constexpr int M = TX * TY / NCT;
-    constexpr int BX = TX / 8;  // 8 x 4 pixel blocks, one per warp and slot
-    static_assert(TX % 8 == 0 && TY % 4 == 0 && (TX / 8) * (TY / 4) == NC * M, "tile / warp map");
+    // each warp and slot covers a PBX x PBY block of pixels (PBY = 32 / PBX)
+    constexpr int PBX = (TY % (32 / kPixBlockX) == 0) ? kPixBlockX : 8, PBY = 32 / PBX;
+    constexpr int BX = TX / PBX;
+    static_assert(TX % PBX == 0 && TY % PBY == 0 && (TX / PBX) * (TY / PBY) == NC * M, "tile / warp map");
     static_assert(CK < 32, "the producer warp covers CK + 1 pulses");
     static_assert(NS >= 2 && NS <= 4, "stage ring");
     using PP = PulseParams<FORM>;
@@ -200,14 +210,18 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
         }
         fence_barrier_init();
         ctl.abort = 0;
+        // Later items are claimed by the producer once it has issued a tile's
+        // last chunk, so the atomic's latency hides behind the consumers' last
+        // chunks (claiming a whole tile ahead would unbalance the tail).
+        ctl.item = atomicAdd(work_counter, 1);
     }
     __syncthreads();
     uint32_t gchunk = 0;  // chunks issued/consumed by this CTA so far (uniform)
     uint32_t issued = 0, issued_par = 0;  // producer lane 0: stages with a TMA issued this tile
+    int b = 0;  // burst of the current item (items grow, so the search resumes here)
 
     for (;;) {
         if (tid == 0) {
-            ctl.item = atomicAdd(work_counter, 1);
             ctl.kmin = INT_MAX;
             ctl.kmax = INT_MIN;
             ctl.azs_max = INT_MIN;
@@ -219,7 +233,6 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
         __syncthreads();
         const int item = ctl.item;
         if (item >= total_tiles) break;
-        int b = 0;
         while (b + 1 < nbursts && bursts[b + 1].tile_base <= item) ++b;
         const BurstDev &B = bursts[b];
         const int ti = item - B.tile_base;
@@ -238,7 +251,7 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
 #pragma unroll
             for (int m = 0; m < M; ++m) {
                 const int bi = warp + NC * m;
-                const int x = 8 * (bi % BX) + (lane & 7), y = 4 * (bi / BX) + (lane >> 3);
+                const int x = PBX * (bi % BX) + lane % PBX, y = PBY * (bi / BX) + lane / PBX;
                 const int px = px0 + x, line = ly0 + y;
                 X[m][0] = X[m][1] = X[m][2] = 0.0;
                 azs[m] = aze[m] = 0;
@@ -295,11 +308,13 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
 #pragma unroll
                 for (int m = 0; m < M; ++m) {
                     const int bi = warp + NC * m;
-                    const int x = 8 * (bi % BX) + (lane & 7), y = 4 * (bi / BX) + (lane >> 3);
+                    const int x = PBX * (bi % BX) + lane % PBX, y = PBY * (bi / BX) + lane / PBX;
                     const int px = px0 + x, line = ly0 + y;
                     if (px <= B.lastpix_eff && line < B.nlines)
                         B.out[(long long)line * B.out_ld + (px - B.out_pix0)] = make_float2(0.f, 0.f);
                 }
+            } else if (lane == 0) {
+                ctl.item = atomicAdd(work_counter, 1);
             }
             __syncthreads();
             continue;
@@ -312,7 +327,7 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
             for (int m = 0; m < M; ++m) {
                 if (aze[m] > azs[m]) {
                     const int bi = warp + NC * m;
-                    const int x = 8 * (bi % BX) + (lane & 7), y = 4 * (bi / BX) + (lane >> 3);
+                    const int x = PBX * (bi % BX) + lane % PBX, y = PBY * (bi / BX) + lane / PBX;
                     pixel_ecef_from(lat_tab[y][0], lat_tab[y][1], lat_tab[y][2], lat_tab[y][3],
                                     lon_tab[x][0], lon_tab[x][1], (double)hgt[m], X[m][0], X[m][1],
                                     X[m][2]);
@@ -583,6 +598,7 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                     mbar_arrive(&ctl.full[s]);
                 }
             }
+            if (lane == 0) ctl.item = atomicAdd(work_counter, 1);
         } else {
             // ---- consumer warps ----
             for (int c = 0; c < nchunks; ++c) {
@@ -660,6 +676,10 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                         const uint64_t mag = f2_pack(kFloorMagic, kFloorMagic);
                         const uint64_t one = f2_pack(1.f, 1.f);
                         uint64_t ff = f2_pack(-jc, -jc);
+                        // pair accumulators: sum vr cs, sum vi sn, sum (vr sn + vi cs)
+                        uint64_t aR[M / 2], aM[M / 2], aI[M / 2];
+#pragma unroll
+                        for (int e = 0; e < M / 2; ++e) aR[e] = aM[e] = aI[e] = 0ull;
 #pragma unroll 4
                         for (int j = 0; j < nk; ++j) {
                             const float2 *row = win + j * WB;
@@ -673,26 +693,40 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                                 f2_unpack(tm, tmv[0], tmv[1]);
                                 f2_unpack(fr, frv[0], frv[1]);
                                 f2_unpack(ph, phv[0], phv[1]);
+                                float vr[2], vi[2], sn[2], cs[2];
 #pragma unroll
                                 for (int h2 = 0; h2 < 2; ++h2) {
                                     const int m = 2 * e + h2;
                                     // proven in the window by the producer; bounded for memory safety
                                     const unsigned ic = tap_index<WB>(tmv[h2]);
                                     const float2 s0 = row[ic], s1 = row[ic + 1];
-                                    float vr = fmaf(frv[h2], s1.x - s0.x, s0.x);
-                                    float vi = fmaf(frv[h2], s1.y - s0.y, s0.y);
+                                    vr[h2] = fmaf(frv[h2], s1.x - s0.x, s0.x);
+                                    vi[h2] = fmaf(frv[h2], s1.y - s0.y, s0.y);
                                     if constexpr (MASKED) {
                                         const bool ok = (unsigned)(j - ja[m]) < (unsigned)nj[m];
-                                        vr = ok ? vr : 0.f;
-                                        vi = ok ? vi : 0.f;
+                                        vr[h2] = ok ? vr[h2] : 0.f;
+                                        vi[h2] = ok ? vi[h2] : 0.f;
                                     }
-                                    float sn, cs;
-                                    __sincosf(phv[h2], &sn, &cs);
-                                    accr[m] = fmaf(vr, cs, fmaf(-vi, sn, accr[m]));
-                                    acci[m] = fmaf(vr, sn, fmaf(vi, cs, acci[m]));
+                                    __sincosf(phv[h2], &sn[h2], &cs[h2]);
                                 }
+                                const uint64_t VR = f2_pack(vr[0], vr[1]), VI = f2_pack(vi[0], vi[1]);
+                                const uint64_t SN = f2_pack(sn[0], sn[1]), CS = f2_pack(cs[0], cs[1]);
+                                aR[e] = f2_fma(VR, CS, aR[e]);
+                                aM[e] = f2_fma(VI, SN, aM[e]);
+                                aI[e] = f2_fma(VI, CS, f2_fma(VR, SN, aI[e]));
                             }
                             ff = f2_add(ff, one);
+                        }
+#pragma unroll
+                        for (int e = 0; e < M / 2; ++e) {
+                            float r0, r1, m0, m1, i0, i1;
+                            f2_unpack(aR[e], r0, r1);
+                            f2_unpack(aM[e], m0, m1);
+                            f2_unpack(aI[e], i0, i1);
+                            accr[2 * e] += r0 - m0;
+                            accr[2 * e + 1] += r1 - m1;
+                            acci[2 * e] += i0;
+                            acci[2 * e + 1] += i1;
                         }
                     };
                     if (h.interior) terms(std::false_type{});
@@ -843,7 +877,7 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
 #pragma unroll
                 for (int m = 0; m < M; ++m) {
                     const int bi = warp + NC * m;
-                    const int x = 8 * (bi % BX) + (lane & 7), y = 4 * (bi / BX) + (lane >> 3);
+                    const int x = PBX * (bi % BX) + lane % PBX, y = PBY * (bi / BX) + lane / PBX;
                     const int px = px0 + x, line = ly0 + y;
                     if (px <= B.lastpix_eff && line < B.nlines) {
                         float2 o = make_float2(0.f, 0.f);
