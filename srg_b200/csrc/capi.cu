@@ -10,8 +10,9 @@
 // [firstpix, min(lastpix, W-1)] of the DEM rows is read (the only columns the
 // sum touches) and only that box of the output rows is merged, row by row with
 // pread/pwrite on the descriptors (instead of an fdopen() stream that is never
-// flushed or closed), by several host threads; the DEM read overlaps the
-// upload of the burst.
+// flushed or closed), by a persistent pool of host threads; the DEM read and
+// the azimuth centres overlap the upload of the burst, and the merge of each
+// block of rows starts as soon as that block is copied back.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
@@ -30,6 +31,7 @@
 
 #include "../../include/srg_bp.h"
 #include "host_internal.h"
+#include "host_pool.h"
 #include "kernels.h"
 
 using namespace srg;
@@ -238,6 +240,22 @@ void ensure_attrs(DevCtx &c, int idx) {
 
 int kernel_index(const KernelEntry *e) { return (int)(e - kKernels); }
 
+int ensure_dropin(DevCtx &c) {
+    if (c.dropin_ready) return SRG_OK;
+    CK(cudaStreamCreateWithFlags(&c.s_main, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c.s_copy, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&c.ev_burst, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c.ev_flags, cudaEventDisableTiming));
+    for (int i = 0; i < DevCtx::kOutBlocks; ++i)
+        CK(cudaEventCreateWithFlags(&c.ev_blk[i], cudaEventDisableTiming));
+    if (cudaMallocHost(&c.host_flags, 64) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(SRG_E_NOMEM, "pinned error word allocation failed");
+    }
+    c.dropin_ready = true;
+    return SRG_OK;
+}
+
 }  // namespace detail
 }  // namespace srg
 
@@ -246,8 +264,12 @@ using namespace srg::detail;
 namespace {
 
 // Core: launch the tiled kernel over n prepared bursts.
+// Azimuth centres (for descriptors without them) and one backprojection
+// launch over `descs` on `st`; with `before_sum` the launch also waits for
+// that event (the azimuth centres need no range lines, so they may overlap
+// the upload the event marks).
 int run_bursts(DevCtx &c, const srg_burst_desc *descs, int n, const srg_bp_options &o,
-               cudaStream_t st) {
+               cudaStream_t st, cudaEvent_t before_sum = nullptr) {
     const KernelEntry *ke = pick_kernel(o.form, o.tile_cfg);
     if (!ke) return fail(SRG_E_ARG, "no kernel for form %d shape %d", o.form, o.tile_cfg);
     const int TX = ke->shape.tx, TY = ke->shape.ty;
@@ -305,6 +327,7 @@ int run_bursts(DevCtx &c, const srg_burst_desc *descs, int n, const srg_bp_optio
     if (per_sm < 1) return fail(SRG_E_UNSUPPORTED, "kernel shape %d does not fit an SM", idx);
     const int grid = std::min(total, per_sm * c.sms);
     int *flags = static_cast<int *>(c.flags.p);
+    if (before_sum) CK(cudaStreamWaitEvent(st, before_sum, 0));
     CK(launch_tiles(*ke, grid, smem, st, static_cast<const BurstDev *>(c.bursts.p), n, total,
                     static_cast<const CUtensorMap *>(c.tmaps.p), flags, flags + 1));
     // host vectors hb/hm were copied from pageable memory: the copies are
@@ -323,34 +346,6 @@ int check_flags(DevCtx &c, cudaStream_t st) {
     return SRG_OK;
 }
 
-// Host threads for the row-wise DEM read and merge of one burst: enough to
-// hide the per-call latency of pread/pwrite, at least 256 rows each.
-int row_threads(int rows) {
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    return std::max(1, std::min({(int)std::min(hw, 16u), rows / 256, 16}));
-}
-
-// Start fn(r0, r1) over `nthr` contiguous blocks of [0, rows) on host threads
-// (a block whose thread cannot be started runs on the caller's); join() waits.
-struct RowPool {
-    std::vector<std::thread> th;
-    template <class F>
-    void start(int rows, int nthr, F fn) {
-        for (int t = 0; t < nthr; ++t) {
-            const int r0 = (int)((long long)rows * t / nthr), r1 = (int)((long long)rows * (t + 1) / nthr);
-            try {
-                th.emplace_back(fn, r0, r1);
-            } catch (...) {
-                fn(r0, r1);
-            }
-        }
-    }
-    void join() {
-        for (auto &x : th) x.join();
-        th.clear();
-    }
-    ~RowPool() { join(); }
-};
 }  // namespace
 
 extern "C" {
@@ -580,7 +575,8 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     int rc = get_ctx(o.device, &c);
     if (rc) return rc;
     std::lock_guard<std::mutex> g(c->mu);
-    cudaStream_t st = 0;
+    if ((rc = ensure_dropin(*c))) return rc;
+    cudaStream_t st = c->s_main;
     const int fp_eff = std::max(fp, 0);
     const int lp_eff = std::min(lp, W - 1);
     const int ncols = lp_eff >= fp_eff ? lp_eff - fp_eff + 1 : 0;
@@ -603,32 +599,34 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     if ((rc = c->in_burst.ensure(bbytes)) || (rc = c->in_sat.ensure(24 * (size_t)rawdatalines)) ||
         (rc = c->in_dem.ensure(dem_bytes)) || (rc = c->out.ensure(win_bytes)))
         return rc;
-    // DEM box of rows [fl, fl + nl) (azimuth_compress.cu:399-408), read by host
-    // threads while the burst uploads; bytes past the end of the file read as 0
+    HostPool &pool = HostPool::get();
+    // the range lines upload on their own stream; the orbit, the DEM box and
+    // the azimuth centres (which need no range lines) proceed meanwhile
+    CK(cudaMemcpyAsync(c->in_burst.p, burstdata, bbytes, cudaMemcpyHostToDevice, c->s_copy));
+    CK(cudaEventRecord(c->ev_burst, c->s_copy));
+    CK(cudaMemcpyAsync(c->in_sat.p, satloc, 24 * (size_t)rawdatalines, cudaMemcpyHostToDevice, st));
+    // DEM box of rows [fl, fl + nl) (azimuth_compress.cu:399-408), read by the
+    // pool's threads; bytes past the end of the file read as 0
     int16_t *slab = static_cast<int16_t *>(c->host_stage);
-    std::atomic<int> dem_err{0};
-    const int nthr = row_threads(nl);
-    RowPool readers;
-    readers.start(nl, nthr, [&](int r0, int r1) {
+    std::atomic<int> io_err{0};
+    const int ntask = std::max(1, std::min(nl, 4 * HostPool::threads()));
+    pool.run(ntask, [&](int t) {
         const size_t want = (size_t)ncols * 2;
-        for (int r = r0; r < r1; ++r) {
+        for (int r = (int)((long long)nl * t / ntask); r < (int)((long long)nl * (t + 1) / ntask); ++r) {
             char *dst = reinterpret_cast<char *>(slab + (size_t)r * ncols);
             const ssize_t got = pread(fddem, dst, want, ((off_t)(fl + r) * W + fp_eff) * 2);
             if (got < 0) {
-                dem_err = 1;
+                io_err = 1;
                 return;
             }
             if ((size_t)got < want) std::memset(dst + got, 0, want - (size_t)got);
         }
     });
-    cudaError_t e1 = cudaMemcpyAsync(c->in_burst.p, burstdata, bbytes, cudaMemcpyHostToDevice, st);
-    cudaError_t e2 = cudaSuccess;
-    if (e1 == cudaSuccess)
-        e2 = cudaMemcpyAsync(c->in_sat.p, satloc, 24 * (size_t)rawdatalines, cudaMemcpyHostToDevice, st);
-    readers.join();
-    CK(e1);
-    CK(e2);
-    if (dem_err) return fail(SRG_E_IO, "DEM read failed (fd %d)", fddem);
+    if (io_err) {
+        cudaStreamSynchronize(c->s_copy);
+        cudaStreamSynchronize(st);
+        return fail(SRG_E_IO, "DEM read failed (fd %d)", fddem);
+    }
     CK(cudaMemcpyAsync(c->in_dem.p, slab, dem_bytes, cudaMemcpyHostToDevice, st));
 
     srg_burst_desc d{};
@@ -671,21 +669,47 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     d.angc0 = angc0;
     d.angc1 = angc1;
     d.prf = prf;
-    rc = run_bursts(*c, &d, 1, o, st);
-    if (rc) return rc;
-    // the kernel wrote every pixel of the box: bring back only the box
+    rc = run_bursts(*c, &d, 1, o, st, c->ev_burst);
+    if (rc) {
+        cudaStreamSynchronize(c->s_copy);
+        cudaStreamSynchronize(st);
+        return rc;
+    }
+    // the error word, then the output box in row blocks: the merge of a block
+    // starts as soon as that block is back
+    CK(cudaMemcpyAsync(c->host_flags, c->flags.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaEventRecord(c->ev_flags, st));
     float *win = static_cast<float *>(c->host_stage);
-    CK(cudaMemcpyAsync(win, c->out.p, win_bytes, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    CK(cudaGetLastError());
-    rc = check_flags(*c, st);
-    if (rc) return rc;
+    const int nblk = std::min(nl, (int)DevCtx::kOutBlocks);
+    for (int k = 0; k < nblk; ++k) {
+        const int r0 = (int)((long long)nl * k / nblk), r1 = (int)((long long)nl * (k + 1) / nblk);
+        const size_t off = (size_t)r0 * ncols * 2, n = (size_t)(r1 - r0) * ncols * 8;
+        CK(cudaMemcpyAsync(win + off, static_cast<float *>(c->out.p) + off, n, cudaMemcpyDeviceToHost,
+                           st));
+        CK(cudaEventRecord(c->ev_blk[k], st));
+    }
+    CK(cudaEventSynchronize(c->ev_flags));
+    if (c->host_flags[1]) {
+        const int word = c->host_flags[1];
+        cudaStreamSynchronize(st);
+        cudaMemsetAsync(static_cast<int *>(c->flags.p) + 1, 0, sizeof(int), st);
+        cudaStreamSynchronize(st);
+        return fail(SRG_E_TIMEOUT, "device error word 0x%x (TMA wait timed out)", word);
+    }
 
     // merge into the .geo rows (azimuth_compress.cu:510-537); pixels outside
     // the box are never replaced, so only the box is read and written
-    std::atomic<int> io_err{0};
-    RowPool mergers;
-    mergers.start(nl, nthr, [&](int r0, int r1) {
+    std::atomic<int> cuda_err{0};
+    const int per_blk = std::max(1, ntask / nblk);
+    pool.run(nblk * per_blk, [&](int t) {
+        const int k = t / per_blk, part = t % per_blk;
+        if (cudaEventSynchronize(c->ev_blk[k]) != cudaSuccess) {
+            cuda_err = 1;
+            return;
+        }
+        const int b0 = (int)((long long)nl * k / nblk), b1 = (int)((long long)nl * (k + 1) / nblk);
+        const int r0 = b0 + (int)((long long)(b1 - b0) * part / per_blk);
+        const int r1 = b0 + (int)((long long)(b1 - b0) * (part + 1) / per_blk);
         std::vector<float> cur(2 * (size_t)ncols);
         const ssize_t want = (ssize_t)ncols * 8;
         for (int r = r0; r < r1; ++r) {
@@ -711,7 +735,9 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
             }
         }
     });
-    mergers.join();
+    CK(cudaStreamSynchronize(st));
+    CK(cudaGetLastError());
+    if (cuda_err) return fail(SRG_E_CUDA, "copy of the output box failed");
     if (io_err == 1) return fail(SRG_E_IO, "output read failed (fd %d)", fdout);
     if (io_err == 2) return fail(SRG_E_IO, "output write failed (fd %d)", fdout);
     return SRG_OK;

@@ -56,11 +56,20 @@ struct DevCtx {
     DevBuf in_burst, in_sat, in_dem, out;  // drop-in staging
     void *host_stage = nullptr;            // pinned host staging (drop-in entry)
     size_t host_cap = 0;
+    // drop-in entry: its own streams (the burst upload overlaps the azimuth
+    // centres), events of the row blocks copied back, a pinned error word
+    static constexpr int kOutBlocks = 16;
+    bool dropin_ready = false;
+    cudaStream_t s_main = nullptr, s_copy = nullptr;
+    cudaEvent_t ev_burst = nullptr, ev_flags = nullptr, ev_blk[kOutBlocks] = {};
+    int *host_flags = nullptr;
     bool attrs_done[64] = {};
 };
 
 // Per-device context (sets the device current).
 int get_ctx(int device, DevCtx **out);
+// Streams, events and pinned error word of the drop-in entry (made once).
+int ensure_dropin(DevCtx &c);
 // Kernel entry for a form and shape index (-1: the default of that form).
 const KernelEntry *pick_kernel(int form, int cfg);
 int kernel_index(const KernelEntry *e);
