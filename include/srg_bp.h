@@ -274,6 +274,27 @@ int srg_crossmul_stack_device(const float *const *slcs, int n, long long ld, int
                               int looksac, int looksdn, float scale, int mask,
                               float *const *igrams, float *const *amps, void *stream);
 
+/* ---- Range compression (replaces the range loop of sentinel/processsub.f90:86-123) ----
+ * The chirp replica of the decoded pulse parameters (processsub.f90:101-107:
+ * t = (j-1)/samplefreq in FP32, phase = 2 pi startfreq t + pi ramprate t^2 in
+ * FP64, each sample rounded to complex64 and divided by npts, npts =
+ * int(pulselength * samplefreq) in FP32), written zero-padded to n complex
+ * samples into `replica` (host); *npts_out receives npts. */
+int srg_range_replica(float samplefreq, float startfreq, float ramprate, float pulselength,
+                      float *replica, int n, int *npts_out);
+/* Range-compress `nlines` decoded echo lines ([nlines][ld_in] complex64 on
+ * the device, the 10-word line header already stripped, nsamps <= 32768
+ * samples each): zero-pad to 32,768, forward FFT, times the conjugate of the
+ * replica's 32,768-point spectrum, inverse FFT (unnormalised, as FFTW's), and
+ * write the first nvalid = nsamps - npts samples of each line to `out`
+ * ([nlines][ld_out] complex64, device; *nvalid_out receives nvalid).
+ * Enqueued on `stream`; FFTs by cuFFT (the reference uses FFTW in single
+ * precision: results agree to FP32 rounding, not bit for bit). */
+int srg_range_compress_device(const float *lines, long long ld_in, int nlines, int nsamps,
+                              float samplefreq, float startfreq, float ramprate,
+                              float pulselength, float *out, long long ld_out, int *nvalid_out,
+                              void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -95,6 +95,11 @@ _SIGS = {
     "srg_crossmul_stack_device": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_longlong, C.c_int,
                                             C.c_int, C.c_int, C.c_int, C.c_float, C.c_int,
                                             C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_void_p]),
+    "srg_range_replica": (C.c_int, [C.c_float, C.c_float, C.c_float, C.c_float, C.c_void_p, C.c_int,
+                                    _ip]),
+    "srg_range_compress_device": (C.c_int, [C.c_void_p, C.c_longlong, C.c_int, C.c_int, C.c_float,
+                                            C.c_float, C.c_float, C.c_float, C.c_void_p, C.c_longlong,
+                                            _ip, C.c_void_p]),
     "srg_azimuth_compress": (C.c_int, [
         _fp, _dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
         C.c_double, C.c_double, C.c_double, C.c_double, _dp, _dp, _dp, _dp, C.c_int,

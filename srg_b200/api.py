@@ -303,6 +303,42 @@ def crossmul_stack(slcs, looksac: int = 1, looksdn: Optional[int] = None, scale:
     return igs, ams
 
 
+def range_replica(samplefreq: float, startfreq: float, ramprate: float, pulselength: float,
+                  n: int = 32768):
+    """The reference's chirp replica (complex64 [n], zero-padded) and npts."""
+    rep = np.zeros(n, np.complex64)
+    npts = C.c_int()
+    check(lib().srg_range_replica(samplefreq, startfreq, ramprate, pulselength,
+                                  C.c_void_p(rep.ctypes.data), n, C.byref(npts)))
+    return rep, int(npts.value)
+
+
+def range_compress(lines, samplefreq: float, startfreq: float, ramprate: float, pulselength: float,
+                   nsamps: Optional[int] = None, out=None, stream=None, sync: bool = True):
+    """Range-compress decoded echo lines (complex64 CUDA tensor [nlines][>= nsamps],
+    line headers stripped) with the chirp of the given pulse parameters
+    (srg_range_compress_device).  Returns the [nlines][nvalid] complex64 tensor
+    (or writes into `out`, whose rows must hold nvalid samples)."""
+    import torch
+    if lines.dtype != torch.complex64 or lines.dim() != 2 or lines.stride(1) != 1 or not lines.is_cuda:
+        raise ValueError("lines must be a 2-D complex64 CUDA tensor with unit column stride")
+    nlines = lines.shape[0]
+    nsamps = lines.shape[1] if nsamps is None else nsamps
+    _, npts = range_replica(samplefreq, startfreq, ramprate, pulselength)
+    nvalid = nsamps - npts
+    if out is None:
+        out = torch.empty((nlines, max(nvalid, 1)), dtype=torch.complex64, device=lines.device)
+    nv = C.c_int()
+    st = _stream_ptr(stream)
+    check(lib().srg_range_compress_device(C.c_void_p(lines.data_ptr()), lines.stride(0), nlines, nsamps,
+                                          samplefreq, startfreq, ramprate, pulselength,
+                                          C.c_void_p(out.data_ptr()), out.stride(0), C.byref(nv),
+                                          C.c_void_p(st)))
+    if sync:
+        check(lib().srg_sync_check(C.c_void_p(st)))
+    return out
+
+
 class Scene:
     """A reusable plan over device bursts (srg_scene_*): azimuth centres,
     one persistent backprojection launch for all bursts and the ordered merge
