@@ -119,61 +119,6 @@ def load_traffic(kernel: str, workload: str):
 # our arm
 
 
-def time_steps(torch, wl, form, steps, warmup, stream, tile_cfg=-1):
-    """K steps of [azimuth centres + backprojection] on `stream`; returns
-    (ms per step, ms per backprojection launch, launches per step)."""
-    from srg_b200 import api
-    db = wl.bursts
-    coefs = [torch.empty_like(c) for c in wl.coefs]
-    for _ in range(warmup):
-        for b, c in zip(db, coefs):
-            api.line_centres(b, stream=stream.cuda_stream, out=c, sync=False)
-        api.backproject(db, form=form, stream=stream.cuda_stream, coefs=coefs, tile_cfg=tile_cfg)
-    torch.cuda.synchronize()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
-           torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
-    with torch.cuda.stream(stream):
-        for e0, e1, e2 in ev:
-            e0.record(stream)
-            for b, c in zip(db, coefs):
-                api.line_centres(b, stream=stream.cuda_stream, out=c, sync=False)
-            e1.record(stream)
-            api.backproject(db, form=form, stream=stream.cuda_stream, coefs=coefs, sync=False,
-                            tile_cfg=tile_cfg)
-            e2.record(stream)
-    torch.cuda.synchronize()
-    from srg_b200 import _lib
-    _lib.check(_lib.lib().srg_sync_check(None))
-    step_ms = sum(e0.elapsed_time(e2) for e0, _, e2 in ev) / steps
-    kern_ms = sum(e1.elapsed_time(e2) for _, e1, e2 in ev) / steps
-    launches = len(db) + 1
-    return step_ms, kern_ms, launches
-
-
-def phase_error(torch, wl):
-    """Split vs FP64 outputs of the same scene: RMS / max phase error (mrad)
-    and RMS amplitude relative error over pixels above 5 % of RMS amplitude."""
-    from srg_b200 import _lib, api
-    outs = {}
-    for form in (_lib.FORM_FP64, _lib.FORM_SPLIT):
-        api.backproject(wl.bursts, form=form, coefs=wl.coefs)
-        outs[form] = [db.out.clone() for db in wl.bursts]
-    ph, amp = [], []
-    for f, s in zip(outs[_lib.FORM_FP64], outs[_lib.FORM_SPLIT]):
-        f = f.to(torch.complex128)
-        s = s.to(torch.complex128)
-        a = f.abs()
-        rms = torch.sqrt((a[a > 0] ** 2).mean())
-        m = a > 0.05 * rms
-        ph.append(torch.angle(s[m] * f[m].conj()))
-        amp.append((s[m].abs() - a[m]).abs() / a[m])
-    ph = torch.cat(ph) * 1e3
-    amp = torch.cat(amp)
-    return {"ph_rms_mrad": float(torch.sqrt((ph ** 2).mean())),
-            "ph_max_mrad": float(ph.abs().max()),
-            "amp_rel_rms": float(torch.sqrt((amp ** 2).mean())), "pixels": int(ph.numel())}
-
-
 def e2e_dropin(torch, wl, steps, form, separate=False):
     """End to end through azimuth_compress_ (the drop-in C ABI), one call per
     burst in acquisition order as the reference's driver makes them: burst
@@ -290,6 +235,37 @@ def stack_interferograms(torch, wl, s_slcs, d_slcs, stream, steps):
             "fp64_ifg_vs_injected_deformation_rms_mrad": float(torch.sqrt((dt[m] ** 2).mean()))}
 
 
+def oversampled_lines(torch, wl, stream):
+    """Configuration 2: the config-1 burst on 2x-oversampled range lines
+    (8-tap windowed-sinc half samples, then the backprojection's linear
+    interpolation on the finer line).  Keeps the plain-line FP64 output for
+    the comparison with configuration 1, swaps the workload's bursts for the
+    oversampled ones and times the oversampling."""
+    from srg_b200 import _lib, api
+    plain = []
+    for db, c in zip(wl.bursts, wl.coefs):
+        api.backproject([db], form=_lib.FORM_FP64, coefs=[c])
+        plain.append(db.out.clone())
+    api.oversample2(wl.bursts[0], stream=stream.cuda_stream)  # warm-up
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    bursts = [api.oversample2(db, stream=stream.cuda_stream, sync=False) for db in wl.bursts]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wl.bursts = bursts
+    wl.terms = api.count_terms(bursts)
+    wl.description += ("; range lines oversampled 2x (8-tap Hann-windowed sinc half samples) "
+                       "before the linear interpolation")
+    return {"oversample_ms": e0.elapsed_time(e1), "plain_fp64": plain}
+
+
+def vs_plain_lines(torch, wl, plain):
+    """FP64 images of the oversampled lines against those of the plain lines."""
+    from srg_b200 import _lib, api
+    api.backproject(wl.bursts, form=_lib.FORM_FP64, coefs=wl.coefs)
+    return raster_phase_error(torch, torch.cat([db.out for db in wl.bursts]), torch.cat(plain))
+
+
 def raster_phase_error(torch, a, ref):
     a = a.to(torch.complex128)
     r = ref.to(torch.complex128)
@@ -390,7 +366,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c3", choices=["c1", "c3", "c4"])
+    ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c4"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--shapes", default=None,
@@ -408,7 +384,8 @@ def main():
     torch.cuda.set_device(local)
     from srg_b200 import _lib, workloads
 
-    build = {"c1": workloads.config1, "c3": workloads.config3, "c4": workloads.config4}[args.workload]
+    build = {"c1": workloads.config1, "c2": workloads.config1, "c3": workloads.config3,
+             "c4": workloads.config4}[args.workload]
     if args.impl == "reference":
         wl = build(device=f"cuda:{local}")
         from srg_b200 import api
@@ -430,62 +407,58 @@ def main():
         print(json.dumps(line))
         return
 
-    wl = build(device=f"cuda:{local}", seed={"c1": 1001, "c3": 1003, "c4": 1004}[args.workload] + rank)
+    wl = build(device=f"cuda:{local}",
+               seed={"c1": 1001, "c2": 1001, "c3": 1003, "c4": 1004}[args.workload] + rank)
+
     stream = torch.cuda.Stream()
+    c2 = oversampled_lines(torch, wl, stream) if args.workload == "c2" else None
     fp32_peak = _lib.measure_fma_peak(False)
     fp64_peak = _lib.measure_fma_peak(True)
     tuned = {}
     ifg = None
-    if args.workload in ("c3", "c4"):
-        plan = wl.plan
-        if pinned:
-            plan.set_form(_lib.FORM_SPLIT, pinned[0])
-            tuned["split"] = (pinned[0], None)
-        else:
-            tuned["split"] = plan.tune(iters=2)
-        with ClockSampler(local) as clk:
-            if world > 1:
-                dist.barrier()
-            s_ms = time_plan(torch, plan, args.steps, args.warmup, stream, label="timed_split")
-            if world > 1:
-                dist.barrier()
-        s_kern = time_plan(torch, plan, args.steps, 1, stream, stages=2)
-        if wl.raster is not None:
-            split_out = wl.raster.clone()
-        else:
-            split_out = torch.stack([db.out for db in wl.bursts])
-        if pinned:
-            plan.set_form(_lib.FORM_FP64, pinned[1])
-            tuned["fp64"] = (pinned[1], None)
-        else:
-            plan.set_form(_lib.FORM_FP64)
-            tuned["fp64"] = plan.tune(iters=1)
-        d_ms = time_plan(torch, plan, max(3, args.steps // 3), 1, stream)
-        d_kern = d_ms
-        if wl.raster is not None:
-            perr = raster_phase_error(torch, split_out, wl.raster)
-        else:
-            fp64_out = torch.stack([db.out for db in wl.bursts])
-            perr = raster_phase_error(torch, split_out, fp64_out)
+    if getattr(wl, "plan", None) is None:  # single bursts: a plan without a scene raster
+        from srg_b200 import api
+        wl.plan = api.Scene(wl.bursts, raster=None, form=_lib.FORM_SPLIT)
+    plan = wl.plan
+    if pinned:
+        plan.set_form(_lib.FORM_SPLIT, pinned[0])
+        tuned["split"] = (pinned[0], None)
+    else:
+        tuned["split"] = plan.tune(iters=2)
+    with ClockSampler(local) as clk:
+        if world > 1:
+            dist.barrier()
+        s_ms = time_plan(torch, plan, args.steps, args.warmup, stream, label="timed_split")
+        if world > 1:
+            dist.barrier()
+    s_kern = time_plan(torch, plan, args.steps, 1, stream, stages=2)
+    if wl.raster is not None:
+        split_out = wl.raster.clone()
+    else:
+        split_out = torch.stack([db.out for db in wl.bursts])
+    if pinned:
+        plan.set_form(_lib.FORM_FP64, pinned[1])
+        tuned["fp64"] = (pinned[1], None)
+    else:
+        plan.set_form(_lib.FORM_FP64)
+        tuned["fp64"] = plan.tune(iters=1)
+    d_ms = time_plan(torch, plan, max(3, args.steps // 3), 1, stream)
+    d_kern = d_ms
+    if wl.raster is not None:
+        perr = raster_phase_error(torch, split_out, wl.raster)
+    else:
+        fp64_out = torch.stack([db.out for db in wl.bursts])
+        perr = raster_phase_error(torch, split_out, fp64_out)
+        if "range_change" in wl.extra:
             ifg = stack_interferograms(torch, wl, list(split_out), list(fp64_out), stream,
                                        max(3, args.steps))
-            del fp64_out
-        del split_out
-        plan.set_form(_lib.FORM_SPLIT, tuned["split"][0])
-        # azimuth centres, backprojection (and the ordered merge): one graph per pass
-        launches = 3 if wl.raster is not None else 2
-    else:
-        with ClockSampler(local) as clk:
-            if world > 1:
-                dist.barrier()
-            torch.cuda.synchronize()
-            s_ms, s_kern, launches = time_steps(torch, wl, _lib.FORM_SPLIT, args.steps,
-                                                args.warmup, stream)
-            if world > 1:
-                dist.barrier()
-        d_ms, d_kern, _ = time_steps(torch, wl, _lib.FORM_FP64, max(3, args.steps // 2),
-                                     args.warmup, stream)
-        perr = phase_error(torch, wl)
+        del fp64_out
+    del split_out
+    plan.set_form(_lib.FORM_SPLIT, tuned["split"][0])
+    # azimuth centres, backprojection (and the ordered merge): one graph per pass
+    launches = 3 if wl.raster is not None else 2
+    if c2 is not None:
+        c2["vs_config1_fp64"] = vs_plain_lines(torch, wl, c2.pop("plain_fp64"))
     e2e_s, h2d, d2h = e2e_dropin(torch, wl, args.e2e_steps, _lib.FORM_SPLIT,
                                  separate=args.workload == "c4")
     # whole job: the slowest rank's times, every rank's terms and bytes
@@ -512,7 +485,8 @@ def main():
         "data": {"c3": "synthetic, seeded: complex Gaussian clutter + forward-projected point targets",
                  "c4": "synthetic, seeded: forward-projected scatterers + point targets, Mogi "
                        "deformation, repeat-pass baselines",
-                 "c1": "synthetic, seeded: forward-projected scatterers"}[args.workload],
+                 "c1": "synthetic, seeded: forward-projected scatterers",
+                 "c2": "synthetic, seeded: forward-projected scatterers"}[args.workload],
         "config": {"workload": wl.description, "bursts": len(wl.bursts),
                    "terms_per_step_per_gpu": wl.terms,
                    "l2": "range lines of every burst > 126 MB L2; no flush between steps",
@@ -522,10 +496,14 @@ def main():
                                   "backprojection launch for all bursts, ordered merge into the scene raster",
                             "c4": "one graph replay: azimuth centres of every pass, one persistent "
                                   "backprojection launch for all passes onto the common grid",
-                            "c1": "azimuth centres + backprojection of one burst"}[args.workload]},
+                            "c1": "one graph replay: azimuth centres of every line, one "
+                                  "backprojection launch",
+                            "c2": "one graph replay: azimuth centres of every line, one "
+                                  "backprojection launch (lines oversampled once, beforehand)"}[args.workload]},
         "fp64_form": {"value": fp64_value, "ms_per_step": d_ms, "kernel_ms": d_kern,
                       "split_over_fp64": value / fp64_value},
         "phase_error_vs_fp64": perr,
+        **({"oversampled_lines": c2} if c2 is not None else {}),
         **({"crossmul": ifg} if ifg is not None else {}),
         "roofline": {"bound": "fp32-issue", "achieved": achieved, "peak": fp32_peak,
                      "unit": "TFLOP/s", "frac": achieved / fp32_peak,

@@ -295,6 +295,19 @@ int srg_range_compress_device(const float *lines, long long ld_in, int nlines, i
                               float pulselength, float *out, long long ld_out, int *nvalid_out,
                               void *stream);
 
+/* ---- Finer range lines (no reference counterpart: the reference
+ * interpolates the original line linearly) ----
+ * 2x oversampling of range lines for the backprojection's linear
+ * interpolation: out[2i] = in[i]; out[2i+1] = 8-tap Hann-windowed sinc at the
+ * half-sample point (taps from srg_oversample_taps, unit DC gain, FP32);
+ * samples beyond the line read as 0.  in: [nlines][ld_in] complex64 with
+ * nsamps samples, out: [nlines][ld_out] complex64 with 2*nsamps - 1 samples
+ * (device).  A burst so oversampled is backprojected with S' = 2*nsamps - 1,
+ * dmrg' = dmrg / 2 and the same rngstart and rngend. */
+void srg_oversample_taps(float taps[4]);
+int srg_oversample_range_device(const float *in, long long ld_in, int nlines, int nsamps,
+                                float *out, long long ld_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -100,6 +100,9 @@ _SIGS = {
     "srg_range_compress_device": (C.c_int, [C.c_void_p, C.c_longlong, C.c_int, C.c_int, C.c_float,
                                             C.c_float, C.c_float, C.c_float, C.c_void_p, C.c_longlong,
                                             _ip, C.c_void_p]),
+    "srg_oversample_taps": (None, [C.c_void_p]),
+    "srg_oversample_range_device": (C.c_int, [C.c_void_p, C.c_longlong, C.c_int, C.c_int, C.c_void_p,
+                                              C.c_longlong, C.c_void_p]),
     "srg_azimuth_compress": (C.c_int, [
         _fp, _dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
         C.c_double, C.c_double, C.c_double, C.c_double, _dp, _dp, _dp, _dp, C.c_int,

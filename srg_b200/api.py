@@ -339,6 +339,37 @@ def range_compress(lines, samplefreq: float, startfreq: float, ramprate: float, 
     return out
 
 
+def oversample_taps():
+    """The 4 half-sample taps (each used on both sides) of srg_oversample_range_device."""
+    h = np.zeros(4, np.float32)
+    lib().srg_oversample_taps(C.c_void_p(h.ctypes.data))
+    return h
+
+
+def oversample2(db: DeviceBurst, stream=None, sync: bool = True) -> DeviceBurst:
+    """A copy of a device burst with its range lines oversampled 2x
+    (srg_oversample_range_device) and the burst geometry adjusted: 2S - 1
+    samples at dmrg / 2 over the same [rngstart, rngend].  The copy shares the
+    satloc, DEM and output tensors of `db`."""
+    import copy
+    import torch
+    P, S = db.b.rawdatalines, db.b.samples
+    ld = 2 * S  # even row length keeps each row 16-byte aligned for TMA
+    out = torch.empty((P, ld), dtype=torch.complex64, device=db.burst.device)
+    st = _stream_ptr(stream)
+    check(lib().srg_oversample_range_device(C.c_void_p(db.burst.data_ptr()), db.burst.stride(0), P, S,
+                                            C.c_void_p(out.data_ptr()), ld, C.c_void_p(st)))
+    if sync:
+        check(lib().srg_sync_check(C.c_void_p(st)))
+    b2 = copy.copy(db.b)
+    b2.pulses = P
+    b2.burst = np.zeros((0, 2 * S - 1), np.complex64)  # shape only: the samples live on the device
+    b2.dmrg = db.b.dmrg / 2.0
+    return DeviceBurst(b=b2, burst=out[:, :2 * S - 1], satloc=db.satloc, dem=db.dem, out=db.out,
+                       firstline=db.firstline, nlines=db.nlines, firstpix=db.firstpix,
+                       lastpix=db.lastpix, out_pix0=db.out_pix0)
+
+
 class Scene:
     """A reusable plan over device bursts (srg_scene_*): azimuth centres,
     one persistent backprojection launch for all bursts and the ordered merge

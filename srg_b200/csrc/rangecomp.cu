@@ -166,3 +166,76 @@ int srg_range_compress_device(const float *lines, long long ld_in, int nlines, i
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// 2x oversampling of range lines (a finer line for the linear interpolation of
+// the backprojection): even output samples are the input samples, odd ones an
+// 8-tap Hann-windowed sinc at the half-sample point (taps normalised to unit
+// DC gain, FP32); samples beyond the line read as 0.  2*nsamps - 1 samples
+// per line.  No reference counterpart: the reference interpolates the
+// original line linearly.
+namespace {
+
+__global__ void oversample2_kernel(const float2 *__restrict__ in, long long ld_in, int nlines, int nsamps,
+                                   float2 *__restrict__ out, long long ld_out, float h0, float h1,
+                                   float h2, float h3) {
+    const int nout = 2 * nsamps - 1;
+    const long long total = (long long)nlines * nout;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int l = (int)(i / nout), m = (int)(i - (long long)l * nout);
+        const float2 *row = in + (long long)l * ld_in;
+        float2 v;
+        if ((m & 1) == 0) {
+            v = row[m >> 1];
+        } else {
+            const int k = m >> 1;  // between samples k and k+1
+            const float h[4] = {h0, h1, h2, h3};
+            float re = 0.f, im = 0.f;
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                const int a = k - t, b = k + 1 + t;
+                const float2 sa = a >= 0 ? row[a] : make_float2(0.f, 0.f);
+                const float2 sb = b < nsamps ? row[b] : make_float2(0.f, 0.f);
+                re = fmaf(h[t], sa.x + sb.x, re);
+                im = fmaf(h[t], sa.y + sb.y, im);
+            }
+            v = make_float2(re, im);
+        }
+        out[(long long)l * ld_out + m] = v;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+void srg_oversample_taps(float taps[4]) {
+    const double pi = 4.0 * std::atan2(1.0, 1.0);
+    double h[4], s = 0.0;
+    for (int t = 0; t < 4; ++t) {
+        const double x = t + 0.5;
+        const double sinc = std::sin(pi * x) / (pi * x);
+        const double win = 0.5 * (1.0 + std::cos(pi * x / 4.0));
+        h[t] = sinc * win;
+        s += 2.0 * h[t];
+    }
+    for (int t = 0; t < 4; ++t) taps[t] = (float)(h[t] / s);
+}
+
+int srg_oversample_range_device(const float *in, long long ld_in, int nlines, int nsamps, float *out,
+                                long long ld_out, void *stream) {
+    if (!in || !out || nlines < 1 || nsamps < 2 || ld_in < nsamps || ld_out < 2LL * nsamps - 1)
+        return fail(SRG_E_ARG, "bad oversampling sizes: nlines=%d nsamps=%d ld_in=%lld ld_out=%lld",
+                    nlines, nsamps, ld_in, ld_out);
+    float h[4];
+    srg_oversample_taps(h);
+    const long long total = (long long)nlines * (2LL * nsamps - 1);
+    oversample2_kernel<<<grid_of(total), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        reinterpret_cast<const float2 *>(in), ld_in, nlines, nsamps, reinterpret_cast<float2 *>(out),
+        ld_out, h[0], h[1], h[2], h[3]);
+    CKR(cudaGetLastError());
+    return SRG_OK;
+}
+
+}  // extern "C"
