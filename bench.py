@@ -370,7 +370,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--shapes", default=None,
-                    help="SPLIT,FP64 kernel shape indices (srg_tile_config); default: tuned")
+                    help="SPLIT,FP64 kernel shape indices (srg_tile_config; -1: the form's "
+                         "default shape); default: tuned")
     args = ap.parse_args()
     pinned = [int(x) for x in args.shapes.split(",")] if args.shapes else None
     rank, world, local = dist_env()
@@ -422,7 +423,7 @@ def main():
     plan = wl.plan
     if pinned:
         plan.set_form(_lib.FORM_SPLIT, pinned[0])
-        tuned["split"] = (pinned[0], None)
+        tuned["split"] = (plan.shape(), None)
     else:
         tuned["split"] = plan.tune(iters=2)
     with ClockSampler(local) as clk:
@@ -438,7 +439,7 @@ def main():
         split_out = torch.stack([db.out for db in wl.bursts])
     if pinned:
         plan.set_form(_lib.FORM_FP64, pinned[1])
-        tuned["fp64"] = (pinned[1], None)
+        tuned["fp64"] = (plan.shape(), None)
     else:
         plan.set_form(_lib.FORM_FP64)
         tuned["fp64"] = plan.tune(iters=1)

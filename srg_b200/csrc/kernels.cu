@@ -269,7 +269,8 @@ cudaError_t launch_fma_peak(int fp64, int blocks, int iters, void *sink, cudaStr
     X(FORM_SPLIT, 32, 8, 4, 24, 3, 128, 3)  \
     X(FORM_SPLIT, 16, 16, 4, 16, 3, 96, 3)  \
     X(FORM_SPLIT, 32, 16, 4, 16, 3, 144, 2)  \
-    X(FORM_SPLIT, 16, 16, 4, 31, 2, 128, 3)
+    X(FORM_SPLIT, 16, 16, 4, 31, 2, 128, 3)  \
+    X(FORM_SPLIT, 32, 8, 4, 16, 2, 256, 3)
 
 #define SRG_WS_FP64_SHAPES(X)               \
     X(FORM_FP64, 32, 4, 4, 16, 2, 128, 3)   \
