@@ -266,6 +266,23 @@ def vs_plain_lines(torch, wl, plain):
     return raster_phase_error(torch, torch.cat([db.out for db in wl.bursts]), torch.cat(plain))
 
 
+def pinned_h2d_gbs(torch, mib: int = 256, reps: int = 5) -> float:
+    """Host-to-device copy bandwidth from pinned memory (GB/s), the bound of
+    the end-to-end path, whose step uploads every burst's range lines."""
+    n = mib * 1024 * 1024 // 8
+    h = torch.ones(n, dtype=torch.complex64).pin_memory()
+    d = torch.empty(n, dtype=torch.complex64, device="cuda")
+    d.copy_(h, non_blocking=True)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        d.copy_(h, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    return reps * n * 8 / (e0.elapsed_time(e1) * 1e-3) / 1e9
+
+
 def raster_phase_error(torch, a, ref):
     a = a.to(torch.complex128)
     r = ref.to(torch.complex128)
@@ -462,6 +479,7 @@ def main():
         c2["vs_config1_fp64"] = vs_plain_lines(torch, wl, c2.pop("plain_fp64"))
     e2e_s, h2d, d2h = e2e_dropin(torch, wl, args.e2e_steps, _lib.FORM_SPLIT,
                                  separate=args.workload == "c4")
+    h2d_gbs = pinned_h2d_gbs(torch)
     # whole job: the slowest rank's times, every rank's terms and bytes
     (s_ms, d_ms, e2e_s), (terms_all, h2d, d2h) = combine_ranks(
         torch, dist if world > 1 else None, "cuda", [s_ms, d_ms, e2e_s], [wl.terms, h2d, d2h])
@@ -516,6 +534,8 @@ def main():
         "cpu_baseline": cpu,
         "e2e": {"value": terms_all / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "s_per_step": e2e_s,
+                "pinned_h2d_gbs": h2d_gbs,
+                "h2d_bound_s_per_step": h2d / world / (h2d_gbs * 1e9),
                 "path": "azimuth_compress_ (33-arg C ABI), pinned host burst, tmpfs DEM/.geo"
                         + (" (one .geo per pass)" if args.workload == "c4" else "")},
         "gpu_launches": launches * args.steps,

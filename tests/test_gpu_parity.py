@@ -188,3 +188,46 @@ def test_config0_point_targets(torch_cuda, orc):
         win = np.abs(spl[li - 2:li + 3, pix - 2:pix + 3])
         assert np.unravel_index(np.argmax(win), win.shape) == (2, 2)
         assert abs(np.angle(spl[li, pix])) < 0.1
+
+
+def test_dropin_sequential_bursts_merge_like_the_oracle(torch_cuda, orc):
+    """Three bursts over one grid and one DEM (different samples and
+    apertures, so their formed line bands overlap without coinciding), merged
+    in call order into one .geo file through azimuth_compress_ (the scene
+    loop of backprojectgpusub.f90): the same file as the oracle's entry
+    called the same way (later bursts overwrite earlier ones)."""
+    base = mini_case("slope")
+    bursts = [base]
+    for seed, ap in ((21, 64), (22, 160)):
+        b = scene.mini_fixture(seed=seed, dem_kind="slope", aperture=ap)
+        b.dem = base.dem
+        bursts.append(b)
+    rng = np.random.default_rng(5)
+    init = (rng.standard_normal((base.demlength, base.demwidth)) +
+            1j * rng.standard_normal((base.demlength, base.demwidth))).astype(np.complex64)
+
+    def run(fn):
+        with tempfile.TemporaryDirectory() as td:
+            dem_path, geo_path = os.path.join(td, "e.dem"), os.path.join(td, "s.geo")
+            np.ascontiguousarray(base.dem, np.int16).tofile(dem_path)
+            init.tofile(geo_path)
+            fd_dem, fd_geo = os.open(dem_path, os.O_RDWR), os.open(geo_path, os.O_RDWR)
+            try:
+                for b in bursts:
+                    O.call_33(fn, b, fd_geo, fd_dem)
+                    import ctypes
+                    ctypes.CDLL(None).fflush(None)
+            finally:
+                os.close(fd_dem)
+                os.close(fd_geo)
+            return np.fromfile(geo_path, np.complex64).reshape(base.demlength, base.demwidth)
+
+    ref = run(orc.lib.srg_oracle_azimuth_compress_)
+    api.set_default_form(_lib.FORM_FP64)
+    try:
+        got = run(_lib.lib().azimuth_compress_)
+    finally:
+        api.set_default_form(_lib.FORM_SPLIT)
+    assert np.array_equal(got != init, ref != init)
+    assert (ref != init).sum() > 0
+    assert rel_err(got, ref) < FP64_REL
