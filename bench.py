@@ -473,8 +473,9 @@ def main():
         del fp64_out
     del split_out
     plan.set_form(_lib.FORM_SPLIT, tuned["split"][0])
-    # azimuth centres, backprojection (and the ordered merge): one graph per pass
-    launches = 3 if wl.raster is not None else 2
+    # azimuth centres, work-list mask and compaction, backprojection (and the
+    # ordered merge): one graph per pass
+    launches = 5 if wl.raster is not None else 4
     if c2 is not None:
         c2["vs_config1_fp64"] = vs_plain_lines(torch, wl, c2.pop("plain_fp64"))
     e2e_s, h2d, d2h = e2e_dropin(torch, wl, args.e2e_steps, _lib.FORM_SPLIT,
@@ -511,13 +512,14 @@ def main():
                    "l2": "range lines of every burst > 126 MB L2; no flush between steps",
                    "parallelism": f"replicas x{world} (one workload per GPU)",
                    "kernel_shapes": {k: _lib.tile_config_name(v[0]) for k, v in tuned.items()},
-                   "step": {"c3": "one graph replay: azimuth centres of every line, one persistent "
-                                  "backprojection launch for all bursts, ordered merge into the scene raster",
-                            "c4": "one graph replay: azimuth centres of every pass, one persistent "
-                                  "backprojection launch for all passes onto the common grid",
-                            "c1": "one graph replay: azimuth centres of every line, one "
+                   "step": {"c3": "one graph replay: azimuth centres of every line, work list of the "
+                                  "tiles with a formed pixel, one persistent backprojection launch for "
+                                  "all bursts, ordered merge into the scene raster",
+                            "c4": "one graph replay: azimuth centres of every pass, work list, one "
+                                  "persistent backprojection launch for all passes onto the common grid",
+                            "c1": "one graph replay: azimuth centres of every line, work list, one "
                                   "backprojection launch",
-                            "c2": "one graph replay: azimuth centres of every line, one "
+                            "c2": "one graph replay: azimuth centres of every line, work list, one "
                                   "backprojection launch (lines oversampled once, beforehand)"}[args.workload]},
         "fp64_form": {"value": fp64_value, "ms_per_step": d_ms, "kernel_ms": d_kern,
                       "split_over_fp64": value / fp64_value},

@@ -144,7 +144,7 @@ template <int FORM, int TX, int TY, int NT, int CK>
 __global__ void __launch_bounds__(NT)
 bp_tiles(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
          const CUtensorMap *__restrict__ tmaps, int *__restrict__ work_counter,
-         int *__restrict__ err, int WB) {
+         int *__restrict__ err, int WB, const int *__restrict__ tile_list) {
     using PM = PixelMap<TX, TY, NT>;
     constexpr int M = PM::M;
     static_assert(CK <= 32, "one warp prepares a chunk");
@@ -168,16 +168,19 @@ bp_tiles(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
     }
     __syncthreads();
     uint32_t phase = 0;
+    // work items index the list of tiles with a formed pixel when there is one
+    const int nitems = tile_list ? tile_list[0] : total_tiles;
 
     for (;;) {
         if (tid == 0) ctl.item = atomicAdd(work_counter, 1);
         __syncthreads();
         const int item = ctl.item;
-        if (item >= total_tiles) break;
+        if (item >= nitems) break;
+        const int tile = tile_list ? tile_list[1 + item] : item;
         int b = 0;
-        while (b + 1 < nbursts && bursts[b + 1].tile_base <= item) ++b;
+        while (b + 1 < nbursts && bursts[b + 1].tile_base <= tile) ++b;
         const BurstDev &B = bursts[b];
-        const int ti = item - B.tile_base;
+        const int ti = tile - B.tile_base;
         const int px0 = B.firstpix + (ti % B.tiles_x) * TX;
         const int ly0 = (ti / B.tiles_x) * TY;
 

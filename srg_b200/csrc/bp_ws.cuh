@@ -177,7 +177,7 @@ template <int FORM, int TX, int TY, int NC, int CK, int NS, int WB, int MINB>
 __global__ void __launch_bounds__((NC + 1) * 32, MINB)
 bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
       const CUtensorMap *__restrict__ tmaps, int *__restrict__ work_counter,
-      int *__restrict__ err, int /* window, = WB */) {
+      int *__restrict__ err, int /* window, = WB */, const int *__restrict__ tile_list) {
     constexpr int NCT = NC * 32;
     constexpr int M = TX * TY / NCT;
     // each warp and slot covers a PBX x PBY block of pixels (PBY = 32 / PBX)
@@ -216,9 +216,11 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
         ctl.item = atomicAdd(work_counter, 1);
     }
     __syncthreads();
+    // work items index the list of tiles with a formed pixel when there is one
+    const int nitems = tile_list ? tile_list[0] : total_tiles;
     uint32_t gchunk = 0;  // chunks issued/consumed by this CTA so far (uniform)
     uint32_t issued = 0, issued_par = 0;  // producer lane 0: stages with a TMA issued this tile
-    int b = 0;  // burst of the current item (items grow, so the search resumes here)
+    int b = 0;  // burst of the current tile (tiles grow, so the search resumes here)
 
     for (;;) {
         if (tid == 0) {
@@ -232,10 +234,11 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
         }
         __syncthreads();
         const int item = ctl.item;
-        if (item >= total_tiles) break;
-        while (b + 1 < nbursts && bursts[b + 1].tile_base <= item) ++b;
+        if (item >= nitems) break;
+        const int tile = tile_list ? tile_list[1 + item] : item;
+        while (b + 1 < nbursts && bursts[b + 1].tile_base <= tile) ++b;
         const BurstDev &B = bursts[b];
-        const int ti = item - B.tile_base;
+        const int ti = tile - B.tile_base;
         const int px0 = B.firstpix + (ti % B.tiles_x) * TX;
         const int ly0 = (ti / B.tiles_x) * TY;
 
@@ -562,6 +565,18 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                     ctl.abort = 1;
                     break;
                 }
+                // The copy first: the stage's header and pulse parameters are
+                // written while it is in flight.  expect_tx arms the byte count
+                // without arriving; the phase still needs all 32 lane arrivals
+                // below, which follow those writes.
+                if (lane == 0 && use_tma) {
+                    if (c == 0) fence_tensormap_acquire(tmaps + B.tmap);
+                    fence_proxy_async_shared();
+                    mbar_expect_tx(&ctl.full[s], (uint32_t)(WB * CK * 8));
+                    tma_load_2d(samp0 + (size_t)s * CK * WB, tmaps + B.tmap, &ctl.full[s], x0, k0);
+                    issued |= 1u << s;
+                    issued_par = (issued_par & ~(1u << s)) | ((r & 1u) << s);
+                }
                 if constexpr (FORM == FORM_FP64) {
                     if (lane < CK) {
                         double *q = prm[s * CK + lane].s;
@@ -587,16 +602,7 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                     }
                 }
                 __syncwarp();
-                if (lane == 0 && use_tma) {
-                    if (c == 0) fence_tensormap_acquire(tmaps + B.tmap);
-                    fence_proxy_async_shared();
-                    mbar_arrive_expect_tx(&ctl.full[s], (uint32_t)(WB * CK * 8));
-                    tma_load_2d(samp0 + (size_t)s * CK * WB, tmaps + B.tmap, &ctl.full[s], x0, k0);
-                    issued |= 1u << s;
-                    issued_par = (issued_par & ~(1u << s)) | ((r & 1u) << s);
-                } else {
-                    mbar_arrive(&ctl.full[s]);
-                }
+                mbar_arrive(&ctl.full[s]);
             }
             if (lane == 0) ctl.item = atomicAdd(work_counter, 1);
         } else {

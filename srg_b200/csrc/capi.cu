@@ -292,7 +292,7 @@ int run_bursts(DevCtx &c, const srg_burst_desc *descs, int n, const srg_bp_optio
     std::vector<CUtensorMap> hm(n);
     double *coef_base = static_cast<double *>(c.coef.p);
     size_t coef_off = 0;
-    int total = 0;
+    int total = 0, max_burst_tiles = 0;
     for (int i = 0; i < n; ++i) {
         const srg_burst_desc &d = descs[i];
         const double *coef = d.coef;
@@ -312,10 +312,13 @@ int run_bursts(DevCtx &c, const srg_burst_desc *descs, int n, const srg_bp_optio
         B.tiles_y = (B.nlines + TY - 1) / TY;
         B.tile_base = total;
         total += B.tiles_x * B.tiles_y;
+        max_burst_tiles = std::max(max_burst_tiles, B.tiles_x * B.tiles_y);
         if (make_tmap(B, ke->shape.window, ke->shape.chunk, &hm[i]) == 0) B.tmap = i;
         hb[i] = B;
     }
     if (total == 0) return SRG_OK;
+    rc = c.tiles.ensure(tile_list_bytes(total));
+    if (rc) return rc;
     CK(cudaMemcpyAsync(c.bursts.p, hb.data(), sizeof(BurstDev) * n, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(c.tmaps.p, hm.data(), sizeof(CUtensorMap) * n, cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(c.flags.p, 0, sizeof(int), st));  // work counter only
@@ -328,8 +331,11 @@ int run_bursts(DevCtx &c, const srg_burst_desc *descs, int n, const srg_bp_optio
     const int grid = std::min(total, per_sm * c.sms);
     int *flags = static_cast<int *>(c.flags.p);
     if (before_sum) CK(cudaStreamWaitEvent(st, before_sum, 0));
-    CK(launch_tiles(*ke, grid, smem, st, static_cast<const BurstDev *>(c.bursts.p), n, total,
-                    static_cast<const CUtensorMap *>(c.tmaps.p), flags, flags + 1));
+    const BurstDev *d_bursts = static_cast<const BurstDev *>(c.bursts.p);
+    CK(launch_tile_list(d_bursts, n, max_burst_tiles, total, TX, TY, c.tiles.p, st));
+    CK(launch_tiles(*ke, grid, smem, st, d_bursts, n, total,
+                    static_cast<const CUtensorMap *>(c.tmaps.p), flags, flags + 1,
+                    static_cast<const int *>(c.tiles.p)));
     // host vectors hb/hm were copied from pageable memory: the copies are
     // complete (staged) when cudaMemcpyAsync returns for pageable sources.
     return SRG_OK;

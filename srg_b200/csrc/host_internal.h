@@ -52,6 +52,7 @@ struct DevCtx {
     DevBuf bursts;    // BurstDev[]
     DevBuf tmaps;     // CUtensorMap[]
     DevBuf coef;      // doubles
+    DevBuf tiles;     // work list of the backprojection (tile_list_bytes)
     DevBuf orbit;     // state vectors
     DevBuf in_burst, in_sat, in_dem, out;  // drop-in staging
     void *host_stage = nullptr;            // pinned host staging (drop-in entry)

@@ -227,6 +227,113 @@ __global__ void forward_project_kernel(BurstDev B, const float2 *refl, long long
 // Calibration: FMA issue-rate peak.  Every thread runs 8 independent FMA
 // chains (enough to cover the pipeline latency at full occupancy); the
 // result is written so the work cannot be elided.
+// ---------------------------------------------------------------------------
+// Work list of the backprojection: the tiles that can hold a formed pixel.
+// A pixel is formed only where its line's azimuth-centre parabola lies inside
+// (ap2, P - ap2) (pixel_azoff, azimuth_compress.cu:169-175); a burst's grid
+// limits span more lines than its pulses see, and on the IW scene 72 % of the
+// tiles have no formed pixel.  Without the list every persistent CTA claims
+// those tiles too and runs their prologue only to write zeros.
+//
+// The mask is conservative: a tile is dropped only when, on every one of its
+// lines, the parabola over the tile's columns stays outside the interval by
+// 1e-3 pulse (its extremes over [arg(first column), arg(last column)] are at
+// the ends or the vertex; the column arguments are the same rounded quotients
+// pixel_azoff forms, monotonic in the column).  A dropped tile's pixels get
+// the zeros the backprojection writes for unformed pixels.  One warp per tile.
+__device__ __forceinline__ double azoff_fit(const double *c, double arg) {
+    return dadd(dadd(dmul(dmul(c[0], arg), arg), dmul(c[1], arg)), c[2]);
+}
+
+__global__ void __launch_bounds__(256) tile_mask_kernel(const BurstDev *__restrict__ bursts, int tx,
+                                                        int ty, unsigned char *__restrict__ mask,
+                                                        int *__restrict__ seg_count) {
+    const BurstDev &B = bursts[blockIdx.y];
+    const int lane = threadIdx.x & 31;
+    const int ti = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (ti >= B.tiles_x * B.tiles_y) return;
+    const int px0 = B.firstpix + (ti % B.tiles_x) * tx;
+    const int ly0 = (ti / B.tiles_x) * ty;
+    const int px1 = min(px0 + tx - 1, B.lastpix_eff);
+    const int nl = min(ty, B.nlines - ly0);
+    bool keep = false;
+    if (lane < nl) {
+        const double *c = B.coef + 3 * (ly0 + lane);
+        const float den = (float)(B.lastpix - B.firstpix);
+        const double a0 = dsub(dmul((double)__fdiv_rn((float)(px0 - B.firstpix), den), 2.0), 1.0);
+        const double a1 = dsub(dmul((double)__fdiv_rn((float)(px1 - B.firstpix), den), 2.0), 1.0);
+        const double f0 = azoff_fit(c, a0), f1 = azoff_fit(c, a1);
+        double lo = fmin(f0, f1), hi = fmax(f0, f1);
+        if (c[0] != 0.0) {
+            const double v = -c[1] / (2.0 * c[0]);
+            if (v > a0 && v < a1) {
+                const double fv = azoff_fit(c, v);
+                lo = fmin(lo, fv);
+                hi = fmax(hi, fv);
+            }
+        }
+        const bool finite = isfinite(f0) && isfinite(f1) && isfinite(lo) && isfinite(hi);
+        keep = !finite || !(hi < (double)B.ap2 - 1e-3 || lo > (double)(B.P - B.ap2) + 1e-3);
+    }
+    keep = __any_sync(0xffffffffu, keep);
+    if (!keep && lane < tx && px0 + lane <= px1) {
+        for (int y = 0; y < nl; ++y)
+            B.out[(long long)(ly0 + y) * B.out_ld + (px0 + lane - B.out_pix0)] = make_float2(0.f, 0.f);
+    }
+    if (lane == 0) {
+        const int t = B.tile_base + ti;
+        mask[t] = keep ? 1 : 0;
+        if (keep) atomicAdd(seg_count + (t >> kTileSegShift), 1);
+    }
+}
+
+// Ordered compaction of the mask: block s writes the kept tiles of segment s
+// (kTileSeg tiles, 16 per thread) after those of the segments before it.
+// list[0] = number of kept tiles, list[1..] = their indices, ascending.
+__global__ void __launch_bounds__(256) tile_compact_kernel(const unsigned char *__restrict__ mask,
+                                                           const int *__restrict__ seg_count,
+                                                           int total, int *__restrict__ list) {
+    static_assert(kTileSeg == 256 * 16, "16 tiles per thread");
+    __shared__ int wsum[8];
+    __shared__ int base;
+    const int s = blockIdx.x, tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    if (w == 0) {
+        int acc = 0;
+        for (int i = lane; i < s; i += 32) acc += seg_count[i];
+#pragma unroll
+        for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) base = acc;
+    }
+    const int t0 = s * kTileSeg + tid * 16;
+    unsigned bits = 0;
+#pragma unroll
+    for (int k = 0; k < 16; ++k)
+        if (t0 + k < total && mask[t0 + k]) bits |= 1u << k;
+    const int cnt = __popc(bits);
+    int inc = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += v;
+    }
+    if (lane == 31) wsum[w] = inc;
+    __syncthreads();
+    int wbase = 0, btotal = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int v = wsum[i];
+        wbase += i < w ? v : 0;
+        btotal += v;
+    }
+    int pos = base + wbase + inc - cnt;
+    while (bits) {
+        const int k = __ffs(bits) - 1;
+        bits &= bits - 1;
+        list[1 + pos++] = t0 + k;
+    }
+    if (s == (int)gridDim.x - 1 && tid == 0) list[0] = base + btotal;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) fma_peak_kernel(T *sink, int iters, T a, T b) {
     T x[8];
@@ -294,10 +401,10 @@ const int kNumKernels = sizeof(kKernels) / sizeof(kKernels[0]);
 
 cudaError_t launch_tiles(const KernelEntry &e, int grid, size_t smem, cudaStream_t st,
                          const BurstDev *bursts, int nb, int total, const CUtensorMap *tmaps,
-                         int *counter, int *err) {
+                         int *counter, int *err, const int *tile_list) {
     int WB = e.shape.window;
     void *args[] = {(void *)&bursts, (void *)&nb, (void *)&total, (void *)&tmaps,
-                    (void *)&counter, (void *)&err, (void *)&WB};
+                    (void *)&counter, (void *)&err, (void *)&WB, (void *)&tile_list};
     return cudaLaunchKernel(e.fn, dim3(grid), dim3(e.shape.threads), args, smem, st);
 }
 
@@ -333,6 +440,22 @@ cudaError_t launch_line_centres_batch(const BurstDev *bursts, const CentreJob *j
                                       int total, cudaStream_t st) {
     if (total <= 0) return cudaSuccess;
     line_centres_batch_kernel<<<(total + 127) / 128, 128, 0, st>>>(bursts, jobs, n, total);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tile_list(const BurstDev *bursts, int nbursts, int max_burst_tiles, int total,
+                             int tx, int ty, void *scratch, cudaStream_t st) {
+    if (total <= 0 || nbursts <= 0 || max_burst_tiles <= 0 || tx > 32 || ty > 32)
+        return cudaErrorInvalidValue;
+    int *list = static_cast<int *>(scratch);
+    int *seg = tile_list_segments(scratch, total);
+    unsigned char *mask = tile_list_mask(scratch, total);
+    const int nseg = (total + kTileSeg - 1) / kTileSeg;
+    cudaError_t e = cudaMemsetAsync(seg, 0, sizeof(int) * nseg, st);
+    if (e != cudaSuccess) return e;
+    tile_mask_kernel<<<dim3((max_burst_tiles + 7) / 8, nbursts), 256, 0, st>>>(bursts, tx, ty, mask,
+                                                                                 seg);
+    tile_compact_kernel<<<nseg, 256, 0, st>>>(mask, seg, total, list);
     return cudaGetLastError();
 }
 

@@ -32,9 +32,30 @@ struct KernelEntry {
 extern const KernelEntry kKernels[];
 extern const int kNumKernels;
 
+// tile_list: the kept tiles from launch_tile_list (list[0] = count, list[1..]
+// = tile indices); nullptr = every tile in [0, total).
 cudaError_t launch_tiles(const KernelEntry &e, int grid, size_t smem, cudaStream_t st,
                          const BurstDev *bursts, int nb, int total, const CUtensorMap *tmaps,
-                         int *counter, int *err);
+                         int *counter, int *err, const int *tile_list = nullptr);
+
+// Work list of the backprojection (kernels.cu: tile_mask_kernel): the tiles
+// of tx x ty pixels that can hold a formed pixel, ascending, with the pixels
+// of the dropped tiles zeroed.  Scratch layout: list [total + 1] ints,
+// segment counts, mask [total] bytes.
+constexpr int kTileSegShift = 12;
+constexpr int kTileSeg = 1 << kTileSegShift;
+inline int *tile_list_segments(void *scratch, int total) {
+    return static_cast<int *>(scratch) + total + 1;
+}
+inline unsigned char *tile_list_mask(void *scratch, int total) {
+    return reinterpret_cast<unsigned char *>(tile_list_segments(scratch, total) +
+                                             (total + kTileSeg - 1) / kTileSeg);
+}
+inline size_t tile_list_bytes(int total) {
+    return sizeof(int) * ((size_t)total + 1 + (total + kTileSeg - 1) / kTileSeg) + (size_t)total;
+}
+cudaError_t launch_tile_list(const BurstDev *bursts, int nbursts, int max_burst_tiles, int total,
+                             int tx, int ty, void *scratch, cudaStream_t st);
 cudaError_t launch_line_centres(const BurstDev &B, const Orbit &o, const CentreParams &cp,
                                 double *coef, cudaStream_t st);
 cudaError_t launch_line_centres_batch(const BurstDev *bursts, const CentreJob *jobs, int n,

@@ -4,11 +4,13 @@
 // needs besides the caller's inputs and outputs: the burst descriptors, one
 // TMA descriptor per burst, the orbit state vectors and centre parameters of
 // every burst, the per-line azimuth-centre parabolas and the work counter.
-// A pass is four launches -- azimuth centres of every line of every burst
-// (one launch), the counter reset, the persistent backprojection (one
-// launch for all bursts) and, when a scene raster is given, the ordered
-// merge of every burst into it (one launch).  On a non-default stream the
+// A pass is a short chain of launches -- azimuth centres of every line of
+// every burst (one launch), the counter reset, the work list of tiles with a
+// formed pixel (a mask and an ordered compaction), the persistent
+// backprojection (one launch for all bursts) and, when a scene raster is
+// given, the ordered merge of every burst into it (one launch).  On a non-default stream the
 // first pass is captured into a CUDA graph and later passes replay it.
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -37,6 +39,9 @@ struct srg_scene {
     double *d_coef = nullptr;
     double *d_orbit = nullptr;
     int *d_flags = nullptr;          // [0] work counter, [1] error word, [2..3] u64 term counter
+    void *d_tiles = nullptr;         // work list of the backprojection (tile_list_bytes)
+    size_t tiles_cap = 0;
+    int max_burst_tiles = 0;
     cudaGraphExec_t graph = nullptr;
     cudaStream_t graph_stream = nullptr;
 };
@@ -76,7 +81,7 @@ void drop_graph(srg_scene *s) {
 int set_kernel(srg_scene *s, int idx) {
     const KernelEntry &ke = kKernels[idx];
     std::vector<CUtensorMap> hm(s->n);
-    int total = 0;
+    int total = 0, max_burst_tiles = 0;
     for (int i = 0; i < s->n; ++i) {
         BurstDev &B = s->hb[i];
         const int nx = B.lastpix_eff - B.firstpix + 1;
@@ -84,12 +89,23 @@ int set_kernel(srg_scene *s, int idx) {
         B.tiles_y = (B.nlines + ke.shape.ty - 1) / ke.shape.ty;
         B.tile_base = total;
         total += B.tiles_x * B.tiles_y;
+        max_burst_tiles = std::max(max_burst_tiles, B.tiles_x * B.tiles_y);
         std::memset(&hm[i], 0, sizeof(CUtensorMap));
         B.tmap = make_tmap(B, ke.shape.window, ke.shape.chunk, &hm[i]) == 0 ? i : -1;
     }
     SCK(cudaMemcpy(s->d_bursts, s->hb.data(), sizeof(BurstDev) * s->n, cudaMemcpyHostToDevice));
     SCK(cudaMemcpy(s->d_tmaps, hm.data(), sizeof(CUtensorMap) * s->n, cudaMemcpyHostToDevice));
+    const size_t need = tile_list_bytes(total);
+    if (need > s->tiles_cap) {
+        cudaFree(s->d_tiles);
+        s->d_tiles = nullptr;
+        s->tiles_cap = 0;
+        const int rc = alloc(&s->d_tiles, need);
+        if (rc) return rc;
+        s->tiles_cap = need;
+    }
     s->total_tiles = total;
+    s->max_burst_tiles = max_burst_tiles;
     s->kernel = idx;
     drop_graph(s);
     return SRG_OK;
@@ -111,8 +127,11 @@ int enqueue_backprojection(srg_scene *s, cudaStream_t st) {
     SCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ke.fn, ke.shape.threads, ke.smem));
     if (per_sm < 1) return fail(SRG_E_UNSUPPORTED, "kernel shape %d does not fit an SM", s->kernel);
     SCK(cudaMemsetAsync(s->d_flags, 0, sizeof(int), st));
+    SCK(launch_tile_list(s->d_bursts, s->n, s->max_burst_tiles, s->total_tiles, ke.shape.tx,
+                         ke.shape.ty, s->d_tiles, st));
     SCK(launch_tiles(ke, std::min(s->total_tiles, per_sm * c->sms), ke.smem, st, s->d_bursts, s->n,
-                     s->total_tiles, s->d_tmaps, s->d_flags, s->d_flags + 1));
+                     s->total_tiles, s->d_tmaps, s->d_flags, s->d_flags + 1,
+                     static_cast<const int *>(s->d_tiles)));
     return SRG_OK;
 }
 
@@ -375,6 +394,7 @@ void srg_scene_destroy(srg_scene *s) {
     cudaFree(s->d_coef);
     cudaFree(s->d_orbit);
     cudaFree(s->d_flags);
+    cudaFree(s->d_tiles);
     delete s;
 }
 

@@ -190,6 +190,29 @@ def test_config0_point_targets(torch_cuda, orc):
         assert abs(np.angle(spl[li, pix])) < 0.1
 
 
+@pytest.mark.parametrize("form", [_lib.FORM_FP64, _lib.FORM_SPLIT])
+def test_tiles_without_formed_pixels(torch_cuda, orc, form):
+    """A grid reaching far past the lines the pulses see: most tiles hold no
+    formed pixel and stay out of the kernel's work list.  Their pixels still
+    come out zero (the output starts filled with 7+7j) and the formed pixels
+    match the oracle."""
+    b = scene.mini_fixture(seed=31, length=400, width=96)
+    ref = oracle_gpu_form(orc, b)["out"]
+    rows = np.abs(ref).sum(axis=1) > 0
+    assert 0 < rows.sum() < 0.5 * len(rows)          # mostly unformed lines
+    db = api.to_device(b)
+    db.out.fill_(complex(7.0, 7.0))
+    api.backproject([db], form=form)
+    out = db.out.cpu().numpy()
+    assert not np.any(out == np.complex64(7 + 7j))
+    assert np.array_equal(out != 0, ref != 0)
+    if form == _lib.FORM_FP64:
+        assert rel_err(out, ref) < FP64_REL
+    else:
+        e = phase_amp_errors(out, ref)
+        assert e["ph_rms"] < SPLIT_PH_RMS_MRAD and e["amp_rms"] < SPLIT_AMP_RMS, e
+
+
 def test_dropin_sequential_bursts_merge_like_the_oracle(torch_cuda, orc):
     """Three bursts over one grid and one DEM (different samples and
     apertures, so their formed line bands overlap without coinciding), merged

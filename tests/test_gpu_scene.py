@@ -48,8 +48,12 @@ def test_scene_plan_matches_sequential_merge(torch_cuda, mini, form):
     st = torch.cuda.Stream()
     for rep in range(3):          # first pass captures the graph, then replays
         raster.zero_()
+        for db in dbs:            # every burst pixel is written by the pass, formed or not
+            db.out.fill_(complex(7.0, 7.0))
         sc.run(st.cuda_stream)
         sc.sync(st.cuda_stream)
+        for db in dbs:
+            assert not bool((db.out == complex(7.0, 7.0)).any())
         got = raster.cpu().numpy()
         assert np.array_equal(got != 0, geo != 0)
         if form == _lib.FORM_FP64:
