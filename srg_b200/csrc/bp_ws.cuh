@@ -565,6 +565,17 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                     ctl.abort = 1;
                     break;
                 }
+                // Range lines still in transfer: wait (bounded) until the rows
+                // of this chunk are in device memory.
+                if (B.ready) {
+                    const int rows_needed = min(k0 + CK, B.P);
+                    const int blocks = (rows_needed + B.ready_rows - 1) / B.ready_rows;
+                    if (!wait_word_at_least(B.ready, B.ready_base + blocks)) {
+                        if (lane == 0) atomicOr(err, ERR_UPLOAD_TIMEOUT);
+                        ctl.abort = 1;
+                        break;
+                    }
+                }
                 // The copy first: the stage's header and pulse parameters are
                 // written while it is in flight.  expect_tx arms the byte count
                 // without arriving; the phase still needs all 32 lane arrivals

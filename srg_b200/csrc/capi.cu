@@ -263,15 +263,27 @@ using namespace srg::detail;
 
 namespace {
 
+// Range lines that are still being copied in blocks of `rows` pulse rows:
+// the copy stream raises `*word` to base + n after the first n blocks.
+struct UploadGate {
+    const int *word;
+    int base, rows;
+};
+
 // Core: launch the tiled kernel over n prepared bursts.
 // Azimuth centres (for descriptors without them) and one backprojection
 // launch over `descs` on `st`; with `before_sum` the launch also waits for
 // that event (the azimuth centres need no range lines, so they may overlap
-// the upload the event marks).
+// the upload the event marks).  With `gate` (one burst), a warp-specialised
+// kernel starts at once and its producer waits for each chunk's rows instead;
+// the first-generation kernels still wait for `before_sum`.  `band`
+// (optional): see launch_tile_list.
 int run_bursts(DevCtx &c, const srg_burst_desc *descs, int n, const srg_bp_options &o,
-               cudaStream_t st, cudaEvent_t before_sum = nullptr) {
+               cudaStream_t st, cudaEvent_t before_sum = nullptr,
+               const UploadGate *gate = nullptr, int *band = nullptr) {
     const KernelEntry *ke = pick_kernel(o.form, o.tile_cfg);
     if (!ke) return fail(SRG_E_ARG, "no kernel for form %d shape %d", o.form, o.tile_cfg);
+    const bool gated = gate && n == 1 && std::strncmp(ke->name, "bp_ws", 5) == 0;
     const int TX = ke->shape.tx, TY = ke->shape.ty;
     // coefficient scratch
     size_t coef_total = 0;
@@ -314,6 +326,11 @@ int run_bursts(DevCtx &c, const srg_burst_desc *descs, int n, const srg_bp_optio
         total += B.tiles_x * B.tiles_y;
         max_burst_tiles = std::max(max_burst_tiles, B.tiles_x * B.tiles_y);
         if (make_tmap(B, ke->shape.window, ke->shape.chunk, &hm[i]) == 0) B.tmap = i;
+        if (gated) {
+            B.ready = gate->word;
+            B.ready_base = gate->base;
+            B.ready_rows = gate->rows;
+        }
         hb[i] = B;
     }
     if (total == 0) return SRG_OK;
@@ -330,9 +347,9 @@ int run_bursts(DevCtx &c, const srg_burst_desc *descs, int n, const srg_bp_optio
     if (per_sm < 1) return fail(SRG_E_UNSUPPORTED, "kernel shape %d does not fit an SM", idx);
     const int grid = std::min(total, per_sm * c.sms);
     int *flags = static_cast<int *>(c.flags.p);
-    if (before_sum) CK(cudaStreamWaitEvent(st, before_sum, 0));
+    if (before_sum && !gated) CK(cudaStreamWaitEvent(st, before_sum, 0));
     const BurstDev *d_bursts = static_cast<const BurstDev *>(c.bursts.p);
-    CK(launch_tile_list(d_bursts, n, max_burst_tiles, total, TX, TY, c.tiles.p, st));
+    CK(launch_tile_list(d_bursts, n, max_burst_tiles, total, TX, TY, c.tiles.p, st, band));
     CK(launch_tiles(*ke, grid, smem, st, d_bursts, n, total,
                     static_cast<const CUtensorMap *>(c.tmaps.p), flags, flags + 1,
                     static_cast<const int *>(c.tiles.p)));
@@ -603,13 +620,38 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     }
     const size_t bbytes = (size_t)rawdatalines * samplesPerBurst * 8;
     if ((rc = c->in_burst.ensure(bbytes)) || (rc = c->in_sat.ensure(24 * (size_t)rawdatalines)) ||
-        (rc = c->in_dem.ensure(dem_bytes)) || (rc = c->out.ensure(win_bytes)))
+        (rc = c->in_dem.ensure(dem_bytes)) || (rc = c->out.ensure(win_bytes)) ||
+        (rc = c->flags.ensure(64)))
         return rc;
     HostPool &pool = HostPool::get();
-    // the range lines upload on their own stream; the orbit, the DEM box and
-    // the azimuth centres (which need no range lines) proceed meanwhile
-    CK(cudaMemcpyAsync(c->in_burst.p, burstdata, bbytes, cudaMemcpyHostToDevice, c->s_copy));
+    // The range lines upload on their own stream in blocks of pulse rows; after
+    // each block the copy stream raises a device word, and the backprojection,
+    // launched without waiting for the whole upload, takes a chunk of pulses as
+    // soon as its rows are in.  The orbit, the DEM box and the azimuth centres
+    // (which need no range lines) proceed meanwhile.  The word only grows
+    // (call number x 16 + blocks), so a value left by an earlier call never
+    // satisfies a later one.
+    int *ready_word = static_cast<int *>(c->flags.p) + DevCtx::kReadyWord;
+    const int nup = std::min(rawdatalines, (int)DevCtx::kUploadBlocks);
+    const int up_rows = (rawdatalines + nup - 1) / nup;
+    c->upload_seq = c->upload_seq >= (1 << 26) ? 1 : c->upload_seq + 1;
+    const int ready_base = c->upload_seq * 16;
+    const size_t row_bytes = (size_t)samplesPerBurst * 8;
+    for (int k = 0; k < nup; ++k) {
+        const int r0 = k * up_rows, r1 = std::min(rawdatalines, r0 + up_rows);
+        if (r0 >= r1) {
+            c->host_flags[DevCtx::kReadyHost + k] = ready_base + nup;
+        } else {
+            CK(cudaMemcpyAsync(static_cast<char *>(c->in_burst.p) + r0 * row_bytes,
+                               reinterpret_cast<const char *>(burstdata) + r0 * row_bytes,
+                               (r1 - r0) * row_bytes, cudaMemcpyHostToDevice, c->s_copy));
+            c->host_flags[DevCtx::kReadyHost + k] = ready_base + k + 1;
+        }
+        CK(cudaMemcpyAsync(ready_word, c->host_flags + DevCtx::kReadyHost + k, sizeof(int),
+                           cudaMemcpyHostToDevice, c->s_copy));
+    }
     CK(cudaEventRecord(c->ev_burst, c->s_copy));
+    const UploadGate gate{ready_word, ready_base, up_rows};
     CK(cudaMemcpyAsync(c->in_sat.p, satloc, 24 * (size_t)rawdatalines, cudaMemcpyHostToDevice, st));
     // DEM box of rows [fl, fl + nl) (azimuth_compress.cu:399-408), read by the
     // pool's threads; bytes past the end of the file read as 0
@@ -675,73 +717,93 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     d.angc0 = angc0;
     d.angc1 = angc1;
     d.prf = prf;
-    rc = run_bursts(*c, &d, 1, o, st, c->ev_burst);
+    // rows of the kept tiles (the band): rows outside it have no formed pixel
+    int *band = static_cast<int *>(c->flags.p) + DevCtx::kBandWord;
+    CK(cudaMemsetAsync(band, 0x7f, sizeof(int), st));      // INT_MAX-like
+    CK(cudaMemsetAsync(band + 1, 0xff, sizeof(int), st));  // -1
+    rc = run_bursts(*c, &d, 1, o, st, c->ev_burst, &gate, band);
     if (rc) {
         cudaStreamSynchronize(c->s_copy);
         cudaStreamSynchronize(st);
         return rc;
     }
-    // the error word, then the output box in row blocks: the merge of a block
-    // starts as soon as that block is back
-    CK(cudaMemcpyAsync(c->host_flags, c->flags.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    // the error word and the band, then the band's rows in blocks: the merge of
+    // a block starts as soon as that block is back
+    CK(cudaMemcpyAsync(c->host_flags, c->flags.p, (DevCtx::kBandWord + 2) * sizeof(int),
+                       cudaMemcpyDeviceToHost, st));
     CK(cudaEventRecord(c->ev_flags, st));
+    CK(cudaEventSynchronize(c->ev_flags));
+    if (c->host_flags[1]) {
+        const int word = c->host_flags[1];
+        cudaStreamSynchronize(c->s_copy);
+        cudaStreamSynchronize(st);
+        cudaMemsetAsync(static_cast<int *>(c->flags.p) + 1, 0, sizeof(int), st);
+        cudaStreamSynchronize(st);
+        return fail(SRG_E_TIMEOUT, "device error word 0x%x (a bounded device wait gave up)", word);
+    }
+    const int band_lo = std::max(0, c->host_flags[DevCtx::kBandWord]);
+    const int band_hi = std::min(nl - 1, c->host_flags[DevCtx::kBandWord + 1]);
+    const int nband = band_hi >= band_lo ? band_hi - band_lo + 1 : 0;
     float *win = static_cast<float *>(c->host_stage);
-    const int nblk = std::min(nl, (int)DevCtx::kOutBlocks);
+    const int nblk = std::min(nband, (int)DevCtx::kOutBlocks);
     for (int k = 0; k < nblk; ++k) {
-        const int r0 = (int)((long long)nl * k / nblk), r1 = (int)((long long)nl * (k + 1) / nblk);
+        const int r0 = band_lo + (int)((long long)nband * k / nblk);
+        const int r1 = band_lo + (int)((long long)nband * (k + 1) / nblk);
         const size_t off = (size_t)r0 * ncols * 2, n = (size_t)(r1 - r0) * ncols * 8;
         CK(cudaMemcpyAsync(win + off, static_cast<float *>(c->out.p) + off, n, cudaMemcpyDeviceToHost,
                            st));
         CK(cudaEventRecord(c->ev_blk[k], st));
     }
-    CK(cudaEventSynchronize(c->ev_flags));
-    if (c->host_flags[1]) {
-        const int word = c->host_flags[1];
-        cudaStreamSynchronize(st);
-        cudaMemsetAsync(static_cast<int *>(c->flags.p) + 1, 0, sizeof(int), st);
-        cudaStreamSynchronize(st);
-        return fail(SRG_E_TIMEOUT, "device error word 0x%x (TMA wait timed out)", word);
-    }
 
     // merge into the .geo rows (azimuth_compress.cu:510-537); pixels outside
     // the box are never replaced, so only the box is read and written
     std::atomic<int> cuda_err{0};
-    const int per_blk = std::max(1, ntask / nblk);
-    pool.run(nblk * per_blk, [&](int t) {
+    const int per_blk = std::max(1, ntask / std::max(nblk, 1));
+    if (nblk > 0) pool.run(nblk * per_blk, [&](int t) {
         const int k = t / per_blk, part = t % per_blk;
         if (cudaEventSynchronize(c->ev_blk[k]) != cudaSuccess) {
             cuda_err = 1;
             return;
         }
-        const int b0 = (int)((long long)nl * k / nblk), b1 = (int)((long long)nl * (k + 1) / nblk);
+        const int b0 = band_lo + (int)((long long)nband * k / nblk);
+        const int b1 = band_lo + (int)((long long)nband * (k + 1) / nblk);
         const int r0 = b0 + (int)((long long)(b1 - b0) * part / per_blk);
         const int r1 = b0 + (int)((long long)(b1 - b0) * (part + 1) / per_blk);
         std::vector<float> cur(2 * (size_t)ncols);
-        const ssize_t want = (ssize_t)ncols * 8;
+        auto replaced = [](const float *v) { return std::fabs((double)v[0]) > 1.e-18; };
         for (int r = r0; r < r1; ++r) {
-            const off_t off = ((off_t)(fl + r) * W + fp_eff) * 8;
+            // only the span [i0, i1] of replaced pixels is read and written back
+            // (most rows of a burst's box have none: they are left untouched)
+            const float *o2 = win + 2 * (size_t)r * ncols;
+            int i0 = 0;
+            while (i0 < ncols && !replaced(o2 + 2 * i0)) ++i0;
+            if (i0 == ncols) continue;
+            int i1 = ncols - 1;
+            while (!replaced(o2 + 2 * i1)) --i1;
+            const ssize_t want = (ssize_t)(i1 - i0 + 1) * 8;
+            const off_t off = ((off_t)(fl + r) * W + fp_eff + i0) * 8;
             const ssize_t got = pread(fdout, cur.data(), want, off);
             if (got < 0) {
                 io_err = 1;
                 return;
             }
             if (got < want) std::memset(reinterpret_cast<char *>(cur.data()) + got, 0, want - got);
-            const float *o2 = win + 2 * (size_t)r * ncols;
-            bool changed = false;
-            for (int i = 0; i < ncols; ++i) {
-                if (std::fabs((double)o2[2 * i]) > 1.e-18) {
-                    cur[2 * i] = o2[2 * i];
-                    cur[2 * i + 1] = o2[2 * i + 1];
-                    changed = true;
+            for (int i = i0; i <= i1; ++i) {
+                if (replaced(o2 + 2 * i)) {
+                    cur[2 * (i - i0)] = o2[2 * i];
+                    cur[2 * (i - i0) + 1] = o2[2 * i + 1];
                 }
             }
-            if (changed && pwrite(fdout, cur.data(), want, off) != want) {
+            if (pwrite(fdout, cur.data(), want, off) != want) {
                 io_err = 2;
                 return;
             }
         }
     });
     CK(cudaStreamSynchronize(st));
+    // the upload may end after the last chunk that needed it: the caller's
+    // buffer stays in use until then
+    CK(cudaStreamSynchronize(c->s_copy));
     CK(cudaGetLastError());
     if (cuda_err) return fail(SRG_E_CUDA, "copy of the output box failed");
     if (io_err == 1) return fail(SRG_E_IO, "output read failed (fd %d)", fdout);

@@ -9,6 +9,7 @@ namespace srg {
 enum : int {
     ERR_TMA_TIMEOUT = 1,   // a bounded mbarrier wait for a TMA tile gave up
     ERR_BAD_BURST = 2,     // a work item referenced an inconsistent burst
+    ERR_UPLOAD_TIMEOUT = 4,  // a bounded wait for range lines still in transfer gave up
 };
 
 // Everything a kernel needs about one burst, prepared on the host.  Field
@@ -35,6 +36,11 @@ struct BurstDev {
     double inv_dmrg;
     float K_hi, K_lo;         // K as an unevaluated float sum
     float K_f, inv_dmrg_f;
+    // Range lines still uploading (the drop-in entry): null, or a device word
+    // that the copy stream raises to ready_base + n once the first
+    // n * ready_rows pulse rows are in device memory.
+    const int *ready;
+    int ready_base, ready_rows;
 };
 
 // Kernel shape of the tiled backprojection.

@@ -60,6 +60,11 @@ struct DevCtx {
     // drop-in entry: its own streams (the burst upload overlaps the azimuth
     // centres), events of the row blocks copied back, a pinned error word
     static constexpr int kOutBlocks = 16;
+    // flags words of the drop-in: [kBandWord, +1] first / last line of the kept
+    // tiles, [kReadyWord] rows-uploaded word; host_flags[kReadyHost + k] holds
+    // the value the copy stream writes after upload block k
+    static constexpr int kBandWord = 4, kReadyWord = 6, kReadyHost = 8, kUploadBlocks = 8;
+    int upload_seq = 0;
     bool dropin_ready = false;
     cudaStream_t s_main = nullptr, s_copy = nullptr;
     cudaEvent_t ev_burst = nullptr, ev_flags = nullptr, ev_blk[kOutBlocks] = {};

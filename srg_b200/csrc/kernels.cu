@@ -247,7 +247,8 @@ __device__ __forceinline__ double azoff_fit(const double *c, double arg) {
 
 __global__ void __launch_bounds__(256) tile_mask_kernel(const BurstDev *__restrict__ bursts, int tx,
                                                         int ty, unsigned char *__restrict__ mask,
-                                                        int *__restrict__ seg_count) {
+                                                        int *__restrict__ seg_count,
+                                                        int *__restrict__ band) {
     const BurstDev &B = bursts[blockIdx.y];
     const int lane = threadIdx.x & 31;
     const int ti = blockIdx.x * 8 + (threadIdx.x >> 5);
@@ -283,7 +284,13 @@ __global__ void __launch_bounds__(256) tile_mask_kernel(const BurstDev *__restri
     if (lane == 0) {
         const int t = B.tile_base + ti;
         mask[t] = keep ? 1 : 0;
-        if (keep) atomicAdd(seg_count + (t >> kTileSegShift), 1);
+        if (keep) {
+            atomicAdd(seg_count + (t >> kTileSegShift), 1);
+            if (band) {
+                atomicMin(band, ly0);
+                atomicMax(band + 1, ly0 + nl - 1);
+            }
+        }
     }
 }
 
@@ -444,7 +451,7 @@ cudaError_t launch_line_centres_batch(const BurstDev *bursts, const CentreJob *j
 }
 
 cudaError_t launch_tile_list(const BurstDev *bursts, int nbursts, int max_burst_tiles, int total,
-                             int tx, int ty, void *scratch, cudaStream_t st) {
+                             int tx, int ty, void *scratch, cudaStream_t st, int *band) {
     if (total <= 0 || nbursts <= 0 || max_burst_tiles <= 0 || tx > 32 || ty > 32)
         return cudaErrorInvalidValue;
     int *list = static_cast<int *>(scratch);
@@ -454,7 +461,7 @@ cudaError_t launch_tile_list(const BurstDev *bursts, int nbursts, int max_burst_
     cudaError_t e = cudaMemsetAsync(seg, 0, sizeof(int) * nseg, st);
     if (e != cudaSuccess) return e;
     tile_mask_kernel<<<dim3((max_burst_tiles + 7) / 8, nbursts), 256, 0, st>>>(bursts, tx, ty, mask,
-                                                                                 seg);
+                                                                                 seg, band);
     tile_compact_kernel<<<nseg, 256, 0, st>>>(mask, seg, total, list);
     return cudaGetLastError();
 }

@@ -41,7 +41,9 @@ cudaError_t launch_tiles(const KernelEntry &e, int grid, size_t smem, cudaStream
 // Work list of the backprojection (kernels.cu: tile_mask_kernel): the tiles
 // of tx x ty pixels that can hold a formed pixel, ascending, with the pixels
 // of the dropped tiles zeroed.  Scratch layout: list [total + 1] ints,
-// segment counts, mask [total] bytes.
+// segment counts, mask [total] bytes.  band (optional, preset to
+// {INT_MAX, -1}): lowered / raised to the first and last line of the kept
+// tiles (lines relative to each burst's first line).
 constexpr int kTileSegShift = 12;
 constexpr int kTileSeg = 1 << kTileSegShift;
 inline int *tile_list_segments(void *scratch, int total) {
@@ -55,7 +57,7 @@ inline size_t tile_list_bytes(int total) {
     return sizeof(int) * ((size_t)total + 1 + (total + kTileSeg - 1) / kTileSeg) + (size_t)total;
 }
 cudaError_t launch_tile_list(const BurstDev *bursts, int nbursts, int max_burst_tiles, int total,
-                             int tx, int ty, void *scratch, cudaStream_t st);
+                             int tx, int ty, void *scratch, cudaStream_t st, int *band = nullptr);
 cudaError_t launch_line_centres(const BurstDev &B, const Orbit &o, const CentreParams &cp,
                                 double *coef, cudaStream_t st);
 cudaError_t launch_line_centres_batch(const BurstDev *bursts, const CentreJob *jobs, int n,

@@ -93,6 +93,18 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
     return false;
 }
 
+// Bounded wait until the device word `word` reaches `target` (a value a copy
+// engine raises; read with acquire semantics); false when the limit ran out.
+__device__ __forceinline__ bool wait_word_at_least(const int *word, int target) {
+    for (uint32_t i = 0; i < kSpinLimit; ++i) {
+        int v;
+        asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(word) : "memory");
+        if (v >= target) return true;
+        __nanosleep(200);
+    }
+    return false;
+}
+
 // 2D tiled TMA load of box {box_x, box_y} at element coordinates (x, y) into
 // shared memory, completing on `bar` (byte count set by the caller).  The
 // tensor map lives in global memory, written by the host before launch.

@@ -132,6 +132,37 @@ def test_dropin_entry_matches_oracle_entry(torch_cuda, orc, name, form):
         assert e["ph_rms"] < SPLIT_PH_RMS_MRAD, e
 
 
+def test_dropin_pinned_upload_in_blocks(torch_cuda):
+    """With the range lines in pinned host memory the drop-in starts the
+    backprojection while the lines are still uploading (block by block, each
+    chunk waiting for its rows); the .geo it writes is bit-identical to the
+    one from pageable lines (uploaded in full before the launch), call after
+    call."""
+    torch = torch_cuda
+    b = scene.config0_point_targets()
+    pinned = torch.from_numpy(np.ascontiguousarray(b.burst, np.complex64)).pin_memory()
+    outs = []
+    with tempfile.TemporaryDirectory() as td:
+        dem_path = os.path.join(td, "e.dem")
+        np.ascontiguousarray(b.dem, np.int16).tofile(dem_path)
+        fd_dem = os.open(dem_path, os.O_RDWR)
+        try:
+            for i, host in enumerate([b.burst, pinned.numpy(), pinned.numpy(), b.burst]):
+                geo_path = os.path.join(td, f"s{i}.geo")
+                np.zeros((b.demlength, b.demwidth), np.complex64).tofile(geo_path)
+                fd = os.open(geo_path, os.O_RDWR)
+                try:
+                    api.azimuth_compress_files(b, fd, fd_dem, burst=host)
+                finally:
+                    os.close(fd)
+                outs.append(np.fromfile(geo_path, np.complex64))
+        finally:
+            os.close(fd_dem)
+    assert np.count_nonzero(outs[0]) > 0
+    for o in outs[1:]:
+        assert np.array_equal(o.view(np.uint32), outs[0].view(np.uint32))
+
+
 def test_status_entry_reports_errors(torch_cuda):
     b = mini_case("flat")
     with tempfile.TemporaryDirectory() as td:
