@@ -173,7 +173,10 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 // WB: staged bins per pulse (the launch passes the same value as its last
 // argument, shared with the first-generation kernels); MINB: blocks per SM
 // the register allocation is sized for.
-template <int FORM, int TX, int TY, int NC, int CK, int NS, int WB, int MINB>
+// GATE: the range lines may still be uploading (BurstDev::ready); the
+// producer waits for each chunk's rows.  A separate instantiation, because
+// the wait's code alone costs the ungated kernel ~4 % (measured).
+template <int FORM, int TX, int TY, int NC, int CK, int NS, int WB, int MINB, bool GATE = false>
 __global__ void __launch_bounds__((NC + 1) * 32, MINB)
 bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
       const CUtensorMap *__restrict__ tmaps, int *__restrict__ work_counter,
@@ -430,6 +433,10 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
             const double dev_scale = (double)__int_as_float(ctl.dmax_bits) * B.inv_dmrg;
             const double *satl = B.satloc;
             const int Pm1 = B.P - 1;
+            // upload gate (GATE only), held in registers with the last value seen
+            const int *const ready = GATE ? B.ready : nullptr;
+            const int ready_base = GATE ? B.ready_base : 0, ready_rows = GATE ? B.ready_rows : 1;
+            int ready_seen = INT_MIN;
             // satellite position of this lane's pulse, one chunk ahead
             double nsx, nsy, nsz;
             {
@@ -567,13 +574,15 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                 }
                 // Range lines still in transfer: wait (bounded) until the rows
                 // of this chunk are in device memory.
-                if (B.ready) {
-                    const int rows_needed = min(k0 + CK, B.P);
-                    const int blocks = (rows_needed + B.ready_rows - 1) / B.ready_rows;
-                    if (!wait_word_at_least(B.ready, B.ready_base + blocks)) {
-                        if (lane == 0) atomicOr(err, ERR_UPLOAD_TIMEOUT);
-                        ctl.abort = 1;
-                        break;
+                if (GATE && ready) {
+                    const int target = ready_base + (min(k0 + CK, Pm1 + 1) + ready_rows - 1) / ready_rows;
+                    if (ready_seen < target) {
+                        if (!wait_word_at_least(ready, target)) {
+                            if (lane == 0) atomicOr(err, ERR_UPLOAD_TIMEOUT);
+                            ctl.abort = 1;
+                            break;
+                        }
+                        ready_seen = target;
                     }
                 }
                 // The copy first: the stage's header and pulse parameters are

@@ -274,16 +274,17 @@ struct UploadGate {
 // Azimuth centres (for descriptors without them) and one backprojection
 // launch over `descs` on `st`; with `before_sum` the launch also waits for
 // that event (the azimuth centres need no range lines, so they may overlap
-// the upload the event marks).  With `gate` (one burst), a warp-specialised
-// kernel starts at once and its producer waits for each chunk's rows instead;
-// the first-generation kernels still wait for `before_sum`.  `band`
-// (optional): see launch_tile_list.
+// the upload the event marks).  With `gate` (one burst) and a shape that has
+// a gated twin (kGatedKernels), the twin starts at once and its producer waits
+// for each chunk's rows instead; other shapes still wait for `before_sum`.
+// `band` (optional): see launch_tile_list.
 int run_bursts(DevCtx &c, const srg_burst_desc *descs, int n, const srg_bp_options &o,
                cudaStream_t st, cudaEvent_t before_sum = nullptr,
                const UploadGate *gate = nullptr, int *band = nullptr) {
     const KernelEntry *ke = pick_kernel(o.form, o.tile_cfg);
     if (!ke) return fail(SRG_E_ARG, "no kernel for form %d shape %d", o.form, o.tile_cfg);
-    const bool gated = gate && n == 1 && std::strncmp(ke->name, "bp_ws", 5) == 0;
+    const KernelEntry *twin = gate && n == 1 ? gated_twin(*ke) : nullptr;
+    const bool gated = twin != nullptr;
     const int TX = ke->shape.tx, TY = ke->shape.ty;
     // coefficient scratch
     size_t coef_total = 0;
@@ -341,16 +342,22 @@ int run_bursts(DevCtx &c, const srg_burst_desc *descs, int n, const srg_bp_optio
     CK(cudaMemsetAsync(c.flags.p, 0, sizeof(int), st));  // work counter only
     const int idx = kernel_index(ke);
     ensure_attrs(c, idx);
-    const int smem = shared_bytes(*ke);
+    if (gated && !c.gated_attrs_done[twin - kGatedKernels]) {
+        CK(cudaFuncSetAttribute(twin->fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                shared_bytes(*twin)));
+        c.gated_attrs_done[twin - kGatedKernels] = true;
+    }
+    const KernelEntry &run = gated ? *twin : *ke;
+    const int smem = shared_bytes(run);
     int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ke->fn, ke->shape.threads, smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, run.fn, run.shape.threads, smem));
     if (per_sm < 1) return fail(SRG_E_UNSUPPORTED, "kernel shape %d does not fit an SM", idx);
     const int grid = std::min(total, per_sm * c.sms);
     int *flags = static_cast<int *>(c.flags.p);
     if (before_sum && !gated) CK(cudaStreamWaitEvent(st, before_sum, 0));
     const BurstDev *d_bursts = static_cast<const BurstDev *>(c.bursts.p);
     CK(launch_tile_list(d_bursts, n, max_burst_tiles, total, TX, TY, c.tiles.p, st, band));
-    CK(launch_tiles(*ke, grid, smem, st, d_bursts, n, total,
+    CK(launch_tiles(run, grid, smem, st, d_bursts, n, total,
                     static_cast<const CUtensorMap *>(c.tmaps.p), flags, flags + 1,
                     static_cast<const int *>(c.tiles.p)));
     // host vectors hb/hm were copied from pageable memory: the copies are

@@ -70,6 +70,7 @@ struct DevCtx {
     cudaEvent_t ev_burst = nullptr, ev_flags = nullptr, ev_blk[kOutBlocks] = {};
     int *host_flags = nullptr;
     bool attrs_done[64] = {};
+    bool gated_attrs_done[8] = {};
 };
 
 // Per-device context (sets the device current).

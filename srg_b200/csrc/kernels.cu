@@ -1,5 +1,7 @@
 // kernels.cu -- auxiliary device kernels and the compiled shapes of the
 // tiled backprojection.
+#include <cstring>
+
 #include "bp_kernel.cuh"
 #include "bp_ws.cuh"
 #include "kernels.h"
@@ -405,6 +407,28 @@ cudaError_t launch_fma_peak(int fp64, int blocks, int iters, void *sink, cudaStr
 const KernelEntry kKernels[] = {SRG_WS_SHAPES(SRG_WS_ENTRY) SRG_SHAPES(SRG_ENTRY)
                                     SRG_WS_FP64_SHAPES(SRG_WS_ENTRY)};
 const int kNumKernels = sizeof(kKernels) / sizeof(kKernels[0]);
+
+// Gated twins (range lines still uploading; the drop-in entry) of the
+// default warp-specialised shapes.  Not listed among the tunable shapes.
+#define SRG_WS_GATED_ENTRY(F, TXv, TYv, NCv, CKv, NSv, WBv, MBv)                                \
+    {F, {TXv, TYv, (NCv + 1) * 32, CKv, WBv}, ws_smem_bytes<F, CKv, NSv>(WBv),                  \
+     (const void *)bp_ws<F, TXv, TYv, NCv, CKv, NSv, WBv, MBv, true>,                           \
+     "bp_ws<" #F "," #TXv "x" #TYv ",consumer warps " #NCv ",chunk " #CKv ",stages " #NSv       \
+     ",window " #WBv ",min blocks " #MBv ",gated>"},
+const KernelEntry kGatedKernels[] = {SRG_WS_GATED_ENTRY(FORM_SPLIT, 32, 8, 4, 31, 2, 128, 3)};
+const int kNumGatedKernels = sizeof(kGatedKernels) / sizeof(kGatedKernels[0]);
+
+const KernelEntry *gated_twin(const KernelEntry &e) {
+    for (int i = 0; i < kNumGatedKernels; ++i) {
+        const KernelEntry &g = kGatedKernels[i];
+        // same template arguments: the names agree up to the closing '>'
+        const size_t n = std::strlen(e.name);
+        if (g.form == e.form && n > 1 && std::strncmp(g.name, e.name, n - 1) == 0 &&
+            g.name[n - 1] == ',')
+            return &g;
+    }
+    return nullptr;
+}
 
 cudaError_t launch_tiles(const KernelEntry &e, int grid, size_t smem, cudaStream_t st,
                          const BurstDev *bursts, int nb, int total, const CUtensorMap *tmaps,

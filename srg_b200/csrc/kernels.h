@@ -31,6 +31,10 @@ struct KernelEntry {
 
 extern const KernelEntry kKernels[];
 extern const int kNumKernels;
+extern const KernelEntry kGatedKernels[];
+extern const int kNumGatedKernels;
+// The twin of `e` that waits for range lines still uploading, or nullptr.
+const KernelEntry *gated_twin(const KernelEntry &e);
 
 // tile_list: the kept tiles from launch_tile_list (list[0] = count, list[1..]
 // = tile indices); nullptr = every tile in [0, total).
