@@ -93,16 +93,27 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
     return false;
 }
 
-// Bounded wait until the device word `word` reaches `target` (a value a copy
-// engine raises; read with acquire semantics); false when the limit ran out.
+// Bounded wait of a whole warp until the device word `word` reaches `target`
+// (a value a copy engine raises).  Lane 0 alone polls, with acquire semantics
+// and a 1 us pause between polls (hundreds of CTAs poll one word while the
+// copy engine writes the lines); the warp barrier orders the other lanes'
+// later accesses after its load.  false when the limit ran out.
 __device__ __forceinline__ bool wait_word_at_least(const int *word, int target) {
-    for (uint32_t i = 0; i < kSpinLimit; ++i) {
-        int v;
-        asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(word) : "memory");
-        if (v >= target) return true;
-        __nanosleep(200);
+    int ok = 0;
+    if ((threadIdx.x & 31) == 0) {
+        for (uint32_t i = 0; i < kSpinLimit / 4; ++i) {
+            int v;
+            asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(word) : "memory");
+            if (v >= target) {
+                ok = 1;
+                break;
+            }
+            __nanosleep(1000);
+        }
     }
-    return false;
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    __syncwarp();
+    return ok != 0;
 }
 
 // 2D tiled TMA load of box {box_x, box_y} at element coordinates (x, y) into
