@@ -221,6 +221,16 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
     __syncthreads();
     // work items index the list of tiles with a formed pixel when there is one
     const int nitems = tile_list ? tile_list[0] : total_tiles;
+    // Range lines arriving in pulse order (GATE, one burst): take the tiles in
+    // the order their pulses arrive.  Grid lines run against the pulses when
+    // the azimuth centre of the last formed line precedes the first's.
+    bool reverse = false;
+    if constexpr (GATE) {
+        if (nbursts == 1 && bursts[0].nlines >= 3) {
+            const double *cf = bursts[0].coef;
+            reverse = cf[3 * (bursts[0].nlines - 2) + 2] < cf[2];
+        }
+    }
     uint32_t gchunk = 0;  // chunks issued/consumed by this CTA so far (uniform)
     uint32_t issued = 0, issued_par = 0;  // producer lane 0: stages with a TMA issued this tile
     int b = 0;  // burst of the current tile (tiles grow, so the search resumes here)
@@ -238,7 +248,8 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
         __syncthreads();
         const int item = ctl.item;
         if (item >= nitems) break;
-        const int tile = tile_list ? tile_list[1 + item] : item;
+        const int order = reverse ? nitems - 1 - item : item;
+        const int tile = tile_list ? tile_list[1 + order] : order;
         while (b + 1 < nbursts && bursts[b + 1].tile_base <= tile) ++b;
         const BurstDev &B = bursts[b];
         const int ti = tile - B.tile_base;

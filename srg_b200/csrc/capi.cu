@@ -644,22 +644,33 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     c->upload_seq = c->upload_seq >= (1 << 26) ? 1 : c->upload_seq + 1;
     const int ready_base = c->upload_seq * 16;
     const size_t row_bytes = (size_t)samplesPerBurst * 8;
-    for (int k = 0; k < nup; ++k) {
-        const int r0 = k * up_rows, r1 = std::min(rawdatalines, r0 + up_rows);
-        if (r0 >= r1) {
-            c->host_flags[DevCtx::kReadyHost + k] = ready_base + nup;
-        } else {
-            CK(cudaMemcpyAsync(static_cast<char *>(c->in_burst.p) + r0 * row_bytes,
-                               reinterpret_cast<const char *>(burstdata) + r0 * row_bytes,
-                               (r1 - r0) * row_bytes, cudaMemcpyHostToDevice, c->s_copy));
-            c->host_flags[DevCtx::kReadyHost + k] = ready_base + k + 1;
+    auto upload = [&](int kb, int ke) -> int {
+        for (int k = kb; k < ke; ++k) {
+            const int r0 = k * up_rows, r1 = std::min(rawdatalines, r0 + up_rows);
+            if (r0 >= r1) {
+                c->host_flags[DevCtx::kReadyHost + k] = ready_base + nup;
+            } else {
+                CK(cudaMemcpyAsync(static_cast<char *>(c->in_burst.p) + r0 * row_bytes,
+                                   reinterpret_cast<const char *>(burstdata) + r0 * row_bytes,
+                                   (r1 - r0) * row_bytes, cudaMemcpyHostToDevice, c->s_copy));
+                c->host_flags[DevCtx::kReadyHost + k] = ready_base + k + 1;
+            }
+            CK(cudaMemcpyAsync(ready_word, c->host_flags + DevCtx::kReadyHost + k, sizeof(int),
+                               cudaMemcpyHostToDevice, c->s_copy));
         }
-        CK(cudaMemcpyAsync(ready_word, c->host_flags + DevCtx::kReadyHost + k, sizeof(int),
-                           cudaMemcpyHostToDevice, c->s_copy));
-    }
-    CK(cudaEventRecord(c->ev_burst, c->s_copy));
+        return SRG_OK;
+    };
     const UploadGate gate{ready_word, ready_base, up_rows};
+    // Host-to-device copies leave the copy engine in the order they are
+    // issued, whatever their stream: with a gated kernel the small inputs go
+    // first, then the first block, then (while it travels) the DEM box and the
+    // launch, and the other blocks last; without one, every block before the
+    // launch, which waits for them all.
+    const KernelEntry *ke0 = pick_kernel(o.form, o.tile_cfg);
+    const bool pipelined = ke0 && gated_twin(*ke0) != nullptr;
     CK(cudaMemcpyAsync(c->in_sat.p, satloc, 24 * (size_t)rawdatalines, cudaMemcpyHostToDevice, st));
+    if ((rc = upload(0, pipelined ? 1 : nup))) return rc;
+    if (!pipelined) CK(cudaEventRecord(c->ev_burst, c->s_copy));
     // DEM box of rows [fl, fl + nl) (azimuth_compress.cu:399-408), read by the
     // pool's threads; bytes past the end of the file read as 0
     int16_t *slab = static_cast<int16_t *>(c->host_stage);
@@ -728,7 +739,13 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     int *band = static_cast<int *>(c->flags.p) + DevCtx::kBandWord;
     CK(cudaMemsetAsync(band, 0x7f, sizeof(int), st));      // INT_MAX-like
     CK(cudaMemsetAsync(band + 1, 0xff, sizeof(int), st));  // -1
-    rc = run_bursts(*c, &d, 1, o, st, c->ev_burst, &gate, band);
+    rc = run_bursts(*c, &d, 1, o, st, pipelined ? nullptr : c->ev_burst, pipelined ? &gate : nullptr,
+                    band);
+    if (!rc && pipelined) {
+        rc = upload(1, nup);
+        if (!rc && cudaEventRecord(c->ev_burst, c->s_copy) != cudaSuccess)
+            rc = fail(SRG_E_CUDA, "event record failed");
+    }
     if (rc) {
         cudaStreamSynchronize(c->s_copy);
         cudaStreamSynchronize(st);
