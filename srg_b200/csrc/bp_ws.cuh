@@ -63,8 +63,9 @@ struct StageHdr {
     float dmx, dmy, dmz;  // u_{k+1} - u_k at the chunk's middle pulse
     float inv2R, c2;      // 1/(2 R_c) and 1/(2 R_c^2) at the chunk's middle pulse
     // closed forms over the chunk in the centred pulse index f = j - (nk-1)/2:
-    float r0, r1, r2;     // window-relative bin of R_c = r0 + f r1 + f^2 r2
-    float p0, p1, p2;     // reference phase (rad) = p0 + f p1 + f^2 p2, p0 in [-pi, pi]
+    // R_c at the chunk's first pulse and its first and second forward differences:
+    float r0, r1, r2;     // as window-relative bins
+    float p0, p1, p2;     // as phase (rad), p0 in [-pi, pi]
     float u0x, u0y, u0z;  // u_{j+1} - u_j = u0 + j us (j = pulse index within the chunk)
     float usx, usy, usz;
 };
@@ -563,14 +564,19 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                         // w error accumulated over the chunk: nk * step error * max |d|
                         err = fmaf(fabsf(pq[c] - fmaf((float)lane, us[c], u0[c])), dmaxc, err);
                     }
-                    const double cR = Ra + (double)c0;
+                    // the fitted R_c at the first pulse (f = -jc), its first and
+                    // second forward differences
+                    const double djc = (double)jc;
+                    const double cR = Ra + (((double)c2 * djc - (double)c1) * djc + (double)c0);
+                    const double cD1 = (double)c1 + (double)c2 * (1.0 - 2.0 * djc);
+                    const double cD2 = 2.0 * (double)c2;
                     const double q = cR * B.K;
                     hv.r0 = __double2float_rn((cR - B.rngstart) * B.inv_dmrg - (double)x0);
-                    hv.r1 = __double2float_rn((double)c1 * B.inv_dmrg);
-                    hv.r2 = __double2float_rn((double)c2 * B.inv_dmrg);
+                    hv.r1 = __double2float_rn(cD1 * B.inv_dmrg);
+                    hv.r2 = __double2float_rn(cD2 * B.inv_dmrg);
                     hv.p0 = __double2float_rn(kTwoPi * (q - rint(q)));
-                    hv.p1 = __double2float_rn(kTwoPi * B.K * (double)c1);
-                    hv.p2 = __double2float_rn(kTwoPi * B.K * (double)c2);
+                    hv.p1 = __double2float_rn(kTwoPi * B.K * cD1);
+                    hv.p2 = __double2float_rn(kTwoPi * B.K * cD2);
                     hv.u0x = u0[0];
                     hv.u0y = u0[1];
                     hv.u0z = u0[2];
@@ -660,8 +666,10 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                     // Closed forms.  Within the chunk the pixel's range offset from
                     // R_c advances by dw_j = d.(u0 + j us) + g (g: slope of the folded
                     // second-order term), so uacc_j = dwa + dr2_0 + sum_{i<j} dw_i is
-                    // a quadratic in j; with R_c's quadratic the bin and the phase are
-                    // quadratics in f = j - jc, advanced per term by forward differences.
+                    // a quadratic in j: uacc_0 = dwa + dr2_0, first difference
+                    // d.u0 + g, second difference d.us.  With R_c's quadratic (from the
+                    // producer, in the same form) the bin and the phase are advanced per
+                    // term by forward differences from the chunk's first pulse.
                     const float jc = 0.5f * (float)(nk - 1);
                     const float jmid = (float)(nk >> 1);
                     float T0[M], T1[M], T2[M], P0[M], P1[M], P2[M];
@@ -675,24 +683,21 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                         const float bq = fmaf(d[m][0], h.usx, fmaf(d[m][1], h.usy, d[m][2] * h.usz));
                         const float g = fmaf(-2.f * w0, q0, -n0 * h.c2) * fmaf(bq, jmid, a1);
                         const float A = a1 + g;
-                        const float U2 = 0.5f * bq;
-                        const float U1 = fmaf(bq, jc - 0.5f, A);
-                        const float V0 = fmaf(U2, jc * jc - jc, fmaf(A, jc, dr0));
-                        T0[m] = fmaf(whi[m] + (dwa[m] + V0), invd, h.r0);
-                        T1[m] = fmaf(U1, invd, h.r1);
-                        T2[m] = fmaf(U2, invd, h.r2);
-                        float p0 = fmaf(Kr, V0, cph[m] + h.p0);
+                        T0[m] = fmaf(whi[m] + (dwa[m] + dr0), invd, h.r0);
+                        T1[m] = fmaf(A, invd, h.r1);
+                        T2[m] = fmaf(bq, invd, h.r2);
+                        const float p0 = fmaf(Kr, dr0, cph[m] + h.p0);
                         const float nr = rintf(p0 * kInvTwoPi);
                         P0[m] = fmaf(-nr, kTwoPiLo, fmaf(-nr, kTwoPiHi, p0));
-                        P1[m] = fmaf(Kr, U1, h.p1);
-                        P2[m] = fmaf(Kr, U2, h.p2);
+                        P1[m] = fmaf(Kr, A, h.p1);
+                        P2[m] = fmaf(Kr, bq, h.p2);
                         // state at the next chunk: sum of d.(u0 + j us) over the chunk
                         const float S = (float)nk * fmaf(bq, jc, a1);
                         dwa[m] += S;
                         cph[m] = fmaf(Kr, S, cph[m]);
                     }
                     // edge chunks add the exact azimuth-window test of every term;
-                    // the quadratics and the floor run on pixel pairs (f32x2)
+                    // the differences and the floor run on pixel pairs (f32x2)
                     static_assert(M % 2 == 0, "pixel pairs");
                     auto terms = [&](auto masked) {
                         constexpr bool MASKED = decltype(masked)::value;
@@ -702,32 +707,19 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                             ja[m] = max(azs[m] - k0, 0);
                             nj[m] = max(min(aze[m] - k0, nk) - ja[m], 0);
                         }
-                        uint64_t t0[M / 2], t1[M / 2], t2[M / 2], q0[M / 2], q1[M / 2], q2[M / 2];
+                        // bin (tt) and phase (pv) at the current pulse, their first (dt,
+                        // dp) and second (ddt, ddp) differences, per pixel pair
+                        uint64_t tt[M / 2], dt[M / 2], ddt[M / 2], pv[M / 2], dp[M / 2], ddp[M / 2];
 #pragma unroll
                         for (int e = 0; e < M / 2; ++e) {
-                            t0[e] = f2_pack(T0[2 * e], T0[2 * e + 1]);
-                            t1[e] = f2_pack(T1[2 * e], T1[2 * e + 1]);
-                            t2[e] = f2_pack(T2[2 * e], T2[2 * e + 1]);
-                            q0[e] = f2_pack(P0[2 * e], P0[2 * e + 1]);
-                            q1[e] = f2_pack(P1[2 * e], P1[2 * e + 1]);
-                            q2[e] = f2_pack(P2[2 * e], P2[2 * e + 1]);
+                            tt[e] = f2_pack(T0[2 * e], T0[2 * e + 1]);
+                            dt[e] = f2_pack(T1[2 * e], T1[2 * e + 1]);
+                            ddt[e] = f2_pack(T2[2 * e], T2[2 * e + 1]);
+                            pv[e] = f2_pack(P0[2 * e], P0[2 * e + 1]);
+                            dp[e] = f2_pack(P1[2 * e], P1[2 * e + 1]);
+                            ddp[e] = f2_pack(P2[2 * e], P2[2 * e + 1]);
                         }
                         const uint64_t mag = f2_pack(kFloorMagic, kFloorMagic);
-                        // forward differences of the quadratics from f = -jc
-                        uint64_t tt[M / 2], dt[M / 2], ddt[M / 2], pv[M / 2], dp[M / 2], ddp[M / 2];
-                        {
-                            const uint64_t f0 = f2_pack(-jc, -jc), f1 = f2_pack(1.f - 2.f * jc, 1.f - 2.f * jc);
-                            const uint64_t two = f2_pack(2.f, 2.f);
-#pragma unroll
-                            for (int e = 0; e < M / 2; ++e) {
-                                tt[e] = f2_fma(f2_fma(t2[e], f0, t1[e]), f0, t0[e]);
-                                dt[e] = f2_fma(t2[e], f1, t1[e]);
-                                ddt[e] = f2_mul(t2[e], two);
-                                pv[e] = f2_fma(f2_fma(q2[e], f0, q1[e]), f0, q0[e]);
-                                dp[e] = f2_fma(q2[e], f1, q1[e]);
-                                ddp[e] = f2_mul(q2[e], two);
-                            }
-                        }
                         // pair accumulators: sum vr cs, sum vi sn, sum (vr sn + vi cs)
                         uint64_t aR[M / 2], aM[M / 2], aI[M / 2];
 #pragma unroll
