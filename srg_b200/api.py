@@ -41,6 +41,13 @@ def limits(b: Burst):
 
 def azimuth_compress_files(b: Burst, fdout: int, fddem: int, burst: Optional[np.ndarray] = None):
     """Call the drop-in ``azimuth_compress_`` (33 by-reference arguments)."""
+    prepare_azimuth_compress(b, fdout, fddem, burst)()
+
+
+def prepare_azimuth_compress(b: Burst, fdout: int, fddem: int, burst: Optional[np.ndarray] = None):
+    """The 33 by-reference arguments of one ``azimuth_compress_`` call, built
+    once; returns a callable that makes the call (as a Fortran caller does, with
+    its arrays and scalars already in place)."""
     L = lib()
     burst = np.ascontiguousarray(b.burst if burst is None else burst, np.complex64)
     keep = {k: _d(getattr(b, k)) for k in
@@ -53,13 +60,20 @@ def azimuth_compress_files(b: Burst, fdout: int, fddem: int, burst: Optional[np.
           "tmid", "dtaz", "dmrg", "wvl", "angc0", "angc1", "prf")}
     r = C.byref
     p = lambda a: a.ctypes.data_as(_dp)  # noqa: E731
-    L.azimuth_compress_(
+    args = (
         burst.ctypes.data_as(_fp), p(keep["satloc"]), r(i["P"]), r(i["S"]), r(i["W"]), r(i["L"]),
         r(i["fo"]), r(i["fd"]), r(d["deltalat"]), r(d["deltalon"]), r(d["firstlat"]),
         r(d["firstlon"]), p(keep["latlons"]), p(keep["timeorbit"]), p(keep["xx"]), p(keep["vv"]),
         r(i["n"]), r(d["rngstart"]), r(d["rngend"]), r(d["tstart"]), r(d["tend"]), r(d["tmid"]),
         p(keep["xyz_mid"]), p(keep["vel_mid"]), p(keep["pulse_time"]), r(d["dtaz"]), r(d["dmrg"]),
         r(d["wvl"]), r(i["ap"]), r(i["iap"]), r(d["angc0"]), r(d["angc1"]), r(d["prf"]))
+    fn = L.azimuth_compress_
+    held = (burst, keep, i, d)  # the buffers the pointers refer to stay alive with the call
+
+    def call():
+        fn(*args)
+        return held is not None
+    return call
 
 
 def azimuth_compress_status(b: Burst, fdout: int, fddem: int, form: int = FORM_SPLIT,

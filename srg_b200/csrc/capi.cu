@@ -669,7 +669,11 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     const KernelEntry *ke0 = pick_kernel(o.form, o.tile_cfg);
     const bool pipelined = ke0 && gated_twin(*ke0) != nullptr;
     CK(cudaMemcpyAsync(c->in_sat.p, satloc, 24 * (size_t)rawdatalines, cudaMemcpyHostToDevice, st));
-    if ((rc = upload(0, pipelined ? 1 : nup))) return rc;
+    if ((rc = upload(0, pipelined ? 1 : nup))) {
+        cudaStreamSynchronize(c->s_copy);  // the caller's buffer stays in use until then
+        cudaStreamSynchronize(st);
+        return rc;
+    }
     if (!pipelined) CK(cudaEventRecord(c->ev_burst, c->s_copy));
     // DEM box of rows [fl, fl + nl) (azimuth_compress.cu:399-408), read by the
     // pool's threads; bytes past the end of the file read as 0
