@@ -121,39 +121,59 @@ __global__ void merge_kernel(float2 *dst, long long dst_ld, const float2 *src, l
 // Ordered merge of every burst of a scene into the scene raster: for each
 // scene pixel the last burst (in order) whose output there has
 // |Re| > 1e-18 wins, which is what merging the bursts one after the other
-// with the reference's rule gives.  Each CTA covers a 32 x 8 patch and first
-// collects (ballot) the bursts whose output window meets it.
-__global__ void merge_scene_kernel(const BurstDev *__restrict__ bursts, int n, float2 *dst,
-                                   long long dst_ld, int lines, int cols) {
-    const int c0 = blockIdx.x * 32, l0 = blockIdx.y * 8;
+// with the reference's rule gives.  Each CTA covers a 32 x 32 patch (four
+// rows per thread) and first collects (ballot) the bursts whose output window
+// meets it.  With the work-list mask of the backprojection that wrote the
+// outputs (tiles of 2^tx_log2 x 2^ty_log2 pixels), a burst whose tile at the
+// pixel has no formed pixel is passed over without reading its output (that
+// output is zero, which the rule never takes).
+__global__ void __launch_bounds__(256) merge_scene_kernel(const BurstDev *__restrict__ bursts, int n,
+                                                          float2 *dst, long long dst_ld, int lines,
+                                                          int cols,
+                                                          const unsigned char *__restrict__ tmask,
+                                                          int tx_log2, int ty_log2) {
+    const int c0 = blockIdx.x * 32, l0 = blockIdx.y * 32;
     __shared__ unsigned mask[8];  // up to 256 bursts
-    const int tid = threadIdx.y * 32 + threadIdx.x;
-    for (int w = 0; w < 8; ++w) {
-        const int b = w * 32 + (tid & 31);
-        bool hit = false;
-        if (tid < 32 && b < n) {
-            const BurstDev &B = bursts[b];
-            const int gl0 = B.firstline, gl1 = B.firstline + B.nlines - 1;
-            hit = !(gl1 < l0 || gl0 > l0 + 7 || B.lastpix_eff < c0 || B.firstpix > c0 + 31);
+    const int nw = (n + 31) / 32;
+    if (threadIdx.y == 0) {
+        for (int w = 0; w < nw; ++w) {
+            const int b = w * 32 + threadIdx.x;
+            bool hit = false;
+            if (b < n) {
+                const BurstDev &B = bursts[b];
+                const int gl0 = B.firstline, gl1 = B.firstline + B.nlines - 1;
+                hit = !(gl1 < l0 || gl0 > l0 + 31 || B.lastpix_eff < c0 || B.firstpix > c0 + 31);
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, hit);
+            if (threadIdx.x == 0) mask[w] = m;
         }
-        const unsigned m = __ballot_sync(0xffffffffu, hit);
-        if (tid == 0) mask[w] = m;
     }
     __syncthreads();
-    const int l = l0 + threadIdx.y, c = c0 + threadIdx.x;
-    if (l >= lines || c >= cols) return;
-    for (int w = (n - 1) / 32; w >= 0; --w) {
-        unsigned m = mask[w];
-        while (m) {
-            const int bit = 31 - __clz(m);
-            m &= ~(1u << bit);
-            const BurstDev &B = bursts[w * 32 + bit];
-            const int ll = l - B.firstline;
-            if (ll < 0 || ll >= B.nlines || c < B.firstpix || c > B.lastpix_eff) continue;
-            const float2 v = B.out[(long long)ll * B.out_ld + (c - B.out_pix0)];
-            if (fabs((double)v.x) > 1.e-18) {
-                dst[(long long)l * dst_ld + c] = v;
-                return;
+    const int c = c0 + threadIdx.x;
+    if (c >= cols) return;
+#pragma unroll 1
+    for (int rr = 0; rr < 4; ++rr) {
+        const int l = l0 + threadIdx.y + 8 * rr;
+        if (l >= lines) break;
+        bool done = false;
+        for (int w = nw - 1; w >= 0 && !done; --w) {
+            unsigned m = mask[w];
+            while (m) {
+                const int bit = 31 - __clz(m);
+                m &= ~(1u << bit);
+                const BurstDev &B = bursts[w * 32 + bit];
+                const int ll = l - B.firstline;
+                if (ll < 0 || ll >= B.nlines || c < B.firstpix || c > B.lastpix_eff) continue;
+                if (tmask) {
+                    const int ti = (ll >> ty_log2) * B.tiles_x + ((c - B.firstpix) >> tx_log2);
+                    if (!tmask[B.tile_base + ti]) continue;
+                }
+                const float2 v = B.out[(long long)ll * B.out_ld + (c - B.out_pix0)];
+                if (fabs((double)v.x) > 1.e-18) {
+                    dst[(long long)l * dst_ld + c] = v;
+                    done = true;
+                    break;
+                }
             }
         }
     }
@@ -491,11 +511,17 @@ cudaError_t launch_tile_list(const BurstDev *bursts, int nbursts, int max_burst_
 }
 
 cudaError_t launch_merge_scene(const BurstDev *bursts, int n, float2 *dst, long long dst_ld,
-                               int lines, int cols, cudaStream_t st) {
+                               int lines, int cols, cudaStream_t st, const unsigned char *tile_mask,
+                               int tx, int ty) {
     if (lines <= 0 || cols <= 0 || n <= 0) return cudaSuccess;
     if (n > 256) return cudaErrorInvalidValue;
-    dim3 grid((cols + 31) / 32, (lines + 7) / 8);
-    merge_scene_kernel<<<grid, dim3(32, 8), 0, st>>>(bursts, n, dst, dst_ld, lines, cols);
+    int txl = 0, tyl = 0;
+    while ((1 << txl) < tx) ++txl;
+    while ((1 << tyl) < ty) ++tyl;
+    if (tile_mask && ((1 << txl) != tx || (1 << tyl) != ty)) tile_mask = nullptr;  // powers of two only
+    dim3 grid((cols + 31) / 32, (lines + 31) / 32);
+    merge_scene_kernel<<<grid, dim3(32, 8), 0, st>>>(bursts, n, dst, dst_ld, lines, cols, tile_mask,
+                                                     txl, tyl);
     return cudaGetLastError();
 }
 

@@ -66,8 +66,11 @@ cudaError_t launch_line_centres(const BurstDev &B, const Orbit &o, const CentreP
                                 double *coef, cudaStream_t st);
 cudaError_t launch_line_centres_batch(const BurstDev *bursts, const CentreJob *jobs, int n,
                                       int total, cudaStream_t st);
+// tile_mask (optional): the work-list mask of the backprojection that wrote the
+// outputs, for tiles of tx x ty pixels (see merge_scene_kernel).
 cudaError_t launch_merge_scene(const BurstDev *bursts, int n, float2 *dst, long long dst_ld,
-                               int lines, int cols, cudaStream_t st);
+                               int lines, int cols, cudaStream_t st,
+                               const unsigned char *tile_mask = nullptr, int tx = 0, int ty = 0);
 cudaError_t launch_count_terms(const BurstDev &B, unsigned long long *terms, int sms,
                                cudaStream_t st);
 cudaError_t launch_merge(float2 *dst, long long dst_ld, const float2 *src, long long src_ld,

@@ -42,6 +42,7 @@ struct srg_scene {
     void *d_tiles = nullptr;         // work list of the backprojection (tile_list_bytes)
     size_t tiles_cap = 0;
     int max_burst_tiles = 0;
+    bool mask_valid = false;         // d_tiles holds the mask of the outputs' last backprojection
     cudaGraphExec_t graph = nullptr;
     cudaStream_t graph_stream = nullptr;
 };
@@ -106,6 +107,7 @@ int set_kernel(srg_scene *s, int idx) {
     }
     s->total_tiles = total;
     s->max_burst_tiles = max_burst_tiles;
+    s->mask_valid = false;
     s->kernel = idx;
     drop_graph(s);
     return SRG_OK;
@@ -129,10 +131,21 @@ int enqueue_backprojection(srg_scene *s, cudaStream_t st) {
     SCK(cudaMemsetAsync(s->d_flags, 0, sizeof(int), st));
     SCK(launch_tile_list(s->d_bursts, s->n, s->max_burst_tiles, s->total_tiles, ke.shape.tx,
                          ke.shape.ty, s->d_tiles, st));
+    s->mask_valid = true;
     SCK(launch_tiles(ke, std::min(s->total_tiles, per_sm * c->sms), ke.smem, st, s->d_bursts, s->n,
                      s->total_tiles, s->d_tmaps, s->d_flags, s->d_flags + 1,
                      static_cast<const int *>(s->d_tiles)));
     return SRG_OK;
+}
+
+// the ordered merge into the scene raster, skipping the tiles the last
+// backprojection found without a formed pixel
+cudaError_t merge(srg_scene *s, cudaStream_t st) {
+    const KernelEntry &ke = kKernels[s->kernel];
+    const unsigned char *tm =
+        s->mask_valid && s->total_tiles > 0 ? tile_list_mask(s->d_tiles, s->total_tiles) : nullptr;
+    return launch_merge_scene(s->d_bursts, s->n, s->scene, s->scene_ld, s->scene_lines,
+                              s->scene_cols, st, tm, ke.shape.tx, ke.shape.ty);
 }
 
 int enqueue_pass(srg_scene *s, cudaStream_t st) {
@@ -140,9 +153,7 @@ int enqueue_pass(srg_scene *s, cudaStream_t st) {
     if (rc) return rc;
     rc = enqueue_backprojection(s, st);
     if (rc) return rc;
-    if (s->scene)
-        SCK(launch_merge_scene(s->d_bursts, s->n, s->scene, s->scene_ld, s->scene_lines,
-                               s->scene_cols, st));
+    if (s->scene) SCK(merge(s, st));
     return SRG_OK;
 }
 
@@ -279,9 +290,7 @@ int srg_scene_run_stages(srg_scene *s, int stages, void *stream) {
     int rc = SRG_OK;
     if (stages & 1) rc = enqueue_centres(s, st);
     if (!rc && (stages & 2)) rc = enqueue_backprojection(s, st);
-    if (!rc && (stages & 4) && s->scene)
-        SCK(launch_merge_scene(s->d_bursts, s->n, s->scene, s->scene_ld, s->scene_lines,
-                               s->scene_cols, st));
+    if (!rc && (stages & 4) && s->scene) SCK(merge(s, st));
     return rc;
 }
 
