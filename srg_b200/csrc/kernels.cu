@@ -9,71 +9,81 @@
 namespace srg {
 
 // ---------------------------------------------------------------------------
-// Per-line azimuth-centre parabola (sentinel/azimuth_compress.cu:438-481),
-// one thread per grid line.  The reference runs this loop serially on the
-// host; the arithmetic here is the same operation for operation.  Lines
-// firstline .. lastline-1 get a parabola; the last line keeps zeros (the
-// reference leaves it unset), so it is never formed.
-__device__ void line_coef(const BurstDev &B, const Orbit &o, const CentreParams &cp, int line,
-                          double *cl) {
+// Per-line azimuth-centre parabola (sentinel/azimuth_compress.cu:438-481).
+// The reference runs this loop serially on the host; the arithmetic here is
+// the same operation for operation.  Lines firstline .. lastline-1 get a
+// parabola; the last line keeps zeros (the reference leaves it unset), so it
+// is never formed.  The three samples of a line (first, middle and last pixel:
+// a Newton zero-Doppler solve each) run on three lanes of a warp, ten lines
+// per warp, and lane 3i writes line i's coefficients.
+__device__ int centre_sample(const BurstDev &B, const Orbit &o, const CentreParams &cp, int line,
+                             int s) {
     const int half = (B.lastpix - B.firstpix) / 2 - 1;
-    int y[3];
-    for (int s = 0; s < 3; ++s) {
-        const int pix = B.firstpix + s * half;
-        double g[3] = {0.0, 0.0, 0.0};
-        if (pix >= B.firstpix && pix <= B.lastpix && pix >= 0 && pix < B.W) {
-            const double h = (double)B.dem[(long long)line * B.dem_ld + pix];
-            pixel_ecef(B, line, pix, h, g[0], g[1], g[2]);
-        }
-        const double rngpix = zero_doppler_range(o, g, cp.tmid, cp.xm, cp.vm);
-        double u0 = dsub(g[0], cp.xm[0]), u1 = dsub(g[1], cp.xm[1]), u2 = dsub(g[2], cp.xm[2]);
-        const double umag = __dsqrt_rn(dadd(dadd(dmul(u0, u0), dmul(u1, u1)), dmul(u2, u2)));
-        u0 = ddiv(u0, umag);
-        u1 = ddiv(u1, umag);
-        u2 = ddiv(u2, umag);
-        const double udotv = dadd(dadd(dmul(cp.vm[0], u0), dmul(cp.vm[1], u1)), dmul(cp.vm[2], u2));
-        const double fd = dmul(ddiv(2.0, cp.wvl), udotv);
-        const double veff = __dsqrt_rn(
-            dadd(dadd(dmul(cp.vm[0], cp.vm[0]), dmul(cp.vm[1], cp.vm[1])), dmul(cp.vm[2], cp.vm[2])));
-        const double num = dsub(dmul(ddiv(ddiv(ddiv(dmul(rngpix, cp.wvl), 2.0), veff), veff), fd),
-                                ddiv(ddiv(dmul(dmul(rngpix, cp.angc0), cp.pi), 180.0), veff));
-        const double den = dadd(1.0, ddiv(ddiv(dmul(dmul(rngpix, cp.angc1), cp.pi), 180.0), veff));
-        const double td = ddiv(num, den);
-        y[s] = (int)dadd(dmul(td, cp.prf), (double)(B.P / 2));
+    const int pix = B.firstpix + s * half;
+    double g[3] = {0.0, 0.0, 0.0};
+    if (pix >= B.firstpix && pix <= B.lastpix && pix >= 0 && pix < B.W) {
+        const double h = (double)B.dem[(long long)line * B.dem_ld + pix];
+        pixel_ecef(B, line, pix, h, g[0], g[1], g[2]);
     }
-    cl[0] = dmul(0.5, dsub((double)(y[0] + y[2]), dmul(2.0, (double)y[1])));
-    cl[1] = dmul(0.5, (double)(y[2] - y[0]));
-    cl[2] = (double)y[1];
+    const double rngpix = zero_doppler_range(o, g, cp.tmid, cp.xm, cp.vm);
+    double u0 = dsub(g[0], cp.xm[0]), u1 = dsub(g[1], cp.xm[1]), u2 = dsub(g[2], cp.xm[2]);
+    const double umag = __dsqrt_rn(dadd(dadd(dmul(u0, u0), dmul(u1, u1)), dmul(u2, u2)));
+    u0 = ddiv(u0, umag);
+    u1 = ddiv(u1, umag);
+    u2 = ddiv(u2, umag);
+    const double udotv = dadd(dadd(dmul(cp.vm[0], u0), dmul(cp.vm[1], u1)), dmul(cp.vm[2], u2));
+    const double fd = dmul(ddiv(2.0, cp.wvl), udotv);
+    const double veff = __dsqrt_rn(
+        dadd(dadd(dmul(cp.vm[0], cp.vm[0]), dmul(cp.vm[1], cp.vm[1])), dmul(cp.vm[2], cp.vm[2])));
+    const double num = dsub(dmul(ddiv(ddiv(ddiv(dmul(rngpix, cp.wvl), 2.0), veff), veff), fd),
+                            ddiv(ddiv(dmul(dmul(rngpix, cp.angc0), cp.pi), 180.0), veff));
+    const double den = dadd(1.0, ddiv(ddiv(dmul(dmul(rngpix, cp.angc1), cp.pi), 180.0), veff));
+    const double td = ddiv(num, den);
+    return (int)dadd(dmul(td, cp.prf), (double)(B.P / 2));
+}
+
+// Lanes 3i, 3i+1, 3i+2 hold samples 0, 1, 2 of one line; lane 3i stores.
+__device__ __forceinline__ void store_coef(int lane, int y, bool last, double *cl) {
+    const int y1 = __shfl_down_sync(0xffffffffu, y, 1);
+    const int y2 = __shfl_down_sync(0xffffffffu, y, 2);
+    if (cl && lane % 3 == 0) {
+        if (last) {
+            cl[0] = cl[1] = cl[2] = 0.0;
+        } else {
+            cl[0] = dmul(0.5, dsub((double)(y + y2), dmul(2.0, (double)y1)));
+            cl[1] = dmul(0.5, (double)(y2 - y));
+            cl[2] = (double)y1;
+        }
+    }
 }
 
 __global__ void line_centres_kernel(BurstDev B, Orbit o, CentreParams cp, double *coef) {
-    const int line = blockIdx.x * blockDim.x + threadIdx.x;
-    if (line >= B.nlines) return;
-    double *cl = coef + 3 * line;
-    if (line == B.nlines - 1) {
-        cl[0] = cl[1] = cl[2] = 0.0;
-        return;
-    }
-    line_coef(B, o, cp, line, cl);
+    const int lane = threadIdx.x & 31;
+    const int line = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 10 + lane / 3;
+    const bool mine = lane < 30 && line < B.nlines;
+    const bool last = line == B.nlines - 1;
+    int y = 0;
+    if (mine && !last) y = centre_sample(B, o, cp, line, lane % 3);
+    store_coef(lane, y, last, mine ? coef + 3 * line : nullptr);
 }
 
-// Batched per-line azimuth centres: one thread per (burst, line) over all
-// bursts of a scene (the same arithmetic as line_centres_kernel).
+// Batched per-line azimuth centres over all bursts of a scene (the same
+// arithmetic as line_centres_kernel; lines numbered across the bursts).
 __global__ void line_centres_batch_kernel(const BurstDev *__restrict__ bursts,
                                           const CentreJob *__restrict__ jobs, int n, int total) {
-    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (gid >= total) return;
+    const int lane = threadIdx.x & 31;
+    const int gid = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 10 + lane / 3;
+    const bool mine = lane < 30 && gid < total;
     int b = 0;
-    while (b + 1 < n && jobs[b + 1].line_base <= gid) ++b;
+    if (mine)
+        while (b + 1 < n && jobs[b + 1].line_base <= gid) ++b;
     const CentreJob &J = jobs[b];
     const BurstDev &B = bursts[b];
     const int line = gid - J.line_base;
-    double *cl = J.coef + 3 * line;
-    if (line == B.nlines - 1) {
-        cl[0] = cl[1] = cl[2] = 0.0;
-        return;
-    }
-    line_coef(B, J.orbit, J.cp, line, cl);
+    const bool last = line == B.nlines - 1;
+    int y = 0;
+    if (mine && !last) y = centre_sample(B, J.orbit, J.cp, line, lane % 3);
+    store_coef(lane, y, last, mine ? J.coef + 3 * line : nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -461,8 +471,8 @@ cudaError_t launch_tiles(const KernelEntry &e, int grid, size_t smem, cudaStream
 
 cudaError_t launch_line_centres(const BurstDev &B, const Orbit &o, const CentreParams &cp,
                                 double *coef, cudaStream_t st) {
-    const int nt = 128;
-    line_centres_kernel<<<(B.nlines + nt - 1) / nt, nt, 0, st>>>(B, o, cp, coef);
+    const int warps = (B.nlines + 9) / 10;  // ten lines per warp
+    line_centres_kernel<<<(warps + 3) / 4, 128, 0, st>>>(B, o, cp, coef);
     return cudaGetLastError();
 }
 
@@ -490,7 +500,8 @@ cudaError_t launch_merge(float2 *dst, long long dst_ld, const float2 *src, long 
 cudaError_t launch_line_centres_batch(const BurstDev *bursts, const CentreJob *jobs, int n,
                                       int total, cudaStream_t st) {
     if (total <= 0) return cudaSuccess;
-    line_centres_batch_kernel<<<(total + 127) / 128, 128, 0, st>>>(bursts, jobs, n, total);
+    const int warps = (total + 9) / 10;  // ten lines per warp
+    line_centres_batch_kernel<<<(warps + 3) / 4, 128, 0, st>>>(bursts, jobs, n, total);
     return cudaGetLastError();
 }
 
