@@ -724,7 +724,8 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                         uint64_t aR[M / 2], aM[M / 2], aI[M / 2];
 #pragma unroll
                         for (int e = 0; e < M / 2; ++e) aR[e] = aM[e] = aI[e] = 0ull;
-#pragma unroll 4
+// unroll 5 measured best of 2..8 (31 = 6 x 5 + 1)
+#pragma unroll 5
                         for (int j = 0; j < nk; ++j) {
                             const float2 *row = win + j * WB;
 #pragma unroll
