@@ -19,6 +19,7 @@
 #include <unistd.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -246,6 +247,7 @@ int ensure_dropin(DevCtx &c) {
     CK(cudaStreamCreateWithFlags(&c.s_copy, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&c.ev_burst, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&c.ev_flags, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c.ev_band, cudaEventDisableTiming));
     for (int i = 0; i < DevCtx::kOutBlocks; ++i)
         CK(cudaEventCreateWithFlags(&c.ev_blk[i], cudaEventDisableTiming));
     if (cudaMallocHost(&c.host_flags, 64) != cudaSuccess) {
@@ -277,10 +279,13 @@ struct UploadGate {
 // the upload the event marks).  With `gate` (one burst) and a shape that has
 // a gated twin (kGatedKernels), the twin starts at once and its producer waits
 // for each chunk's rows instead; other shapes still wait for `before_sum`.
-// `band` (optional): see launch_tile_list.
+// `band` (optional): see launch_tile_list; with `band_host` the two words are
+// also copied there right after the work list and `band_ready` is recorded,
+// ahead of the backprojection.
 int run_bursts(DevCtx &c, const srg_burst_desc *descs, int n, const srg_bp_options &o,
                cudaStream_t st, cudaEvent_t before_sum = nullptr,
-               const UploadGate *gate = nullptr, int *band = nullptr) {
+               const UploadGate *gate = nullptr, int *band = nullptr, int *band_host = nullptr,
+               cudaEvent_t band_ready = nullptr) {
     const KernelEntry *ke = pick_kernel(o.form, o.tile_cfg);
     if (!ke) return fail(SRG_E_ARG, "no kernel for form %d shape %d", o.form, o.tile_cfg);
     const KernelEntry *twin = gate && n == 1 ? gated_twin(*ke) : nullptr;
@@ -357,6 +362,10 @@ int run_bursts(DevCtx &c, const srg_burst_desc *descs, int n, const srg_bp_optio
     if (before_sum && !gated) CK(cudaStreamWaitEvent(st, before_sum, 0));
     const BurstDev *d_bursts = static_cast<const BurstDev *>(c.bursts.p);
     CK(launch_tile_list(d_bursts, n, max_burst_tiles, total, TX, TY, c.tiles.p, st, band));
+    if (band && band_host) {
+        CK(cudaMemcpyAsync(band_host, band, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaEventRecord(band_ready, st));
+    }
     CK(launch_tiles(run, grid, smem, st, d_bursts, n, total,
                     static_cast<const CUtensorMap *>(c.tmaps.p), flags, flags + 1,
                     static_cast<const int *>(c.tiles.p)));
@@ -743,8 +752,11 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     int *band = static_cast<int *>(c->flags.p) + DevCtx::kBandWord;
     CK(cudaMemsetAsync(band, 0x7f, sizeof(int), st));      // INT_MAX-like
     CK(cudaMemsetAsync(band + 1, 0xff, sizeof(int), st));  // -1
+    c->host_flags[DevCtx::kBandWord] = INT_MAX;  // an empty band unless the list reports one
+    c->host_flags[DevCtx::kBandWord + 1] = -1;
+    CK(cudaEventRecord(c->ev_band, st));
     rc = run_bursts(*c, &d, 1, o, st, pipelined ? nullptr : c->ev_burst, pipelined ? &gate : nullptr,
-                    band);
+                    band, c->host_flags + DevCtx::kBandWord, c->ev_band);
     if (!rc && pipelined) {
         rc = upload(1, nup);
         if (!rc && cudaEventRecord(c->ev_burst, c->s_copy) != cudaSuccess)
@@ -755,20 +767,13 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
         cudaStreamSynchronize(st);
         return rc;
     }
-    // the error word and the band, then the band's rows in blocks: the merge of
-    // a block starts as soon as that block is back
-    CK(cudaMemcpyAsync(c->host_flags, c->flags.p, (DevCtx::kBandWord + 2) * sizeof(int),
-                       cudaMemcpyDeviceToHost, st));
+    // The band is known once the work list is built, ahead of the backprojection:
+    // its rows' copies back are queued behind the sum at once, after the error
+    // word; the merge of a block starts as soon as that block is back (and the
+    // error word is clear).
+    CK(cudaEventSynchronize(c->ev_band));
+    CK(cudaMemcpyAsync(c->host_flags, c->flags.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaEventRecord(c->ev_flags, st));
-    CK(cudaEventSynchronize(c->ev_flags));
-    if (c->host_flags[1]) {
-        const int word = c->host_flags[1];
-        cudaStreamSynchronize(c->s_copy);
-        cudaStreamSynchronize(st);
-        cudaMemsetAsync(static_cast<int *>(c->flags.p) + 1, 0, sizeof(int), st);
-        cudaStreamSynchronize(st);
-        return fail(SRG_E_TIMEOUT, "device error word 0x%x (a bounded device wait gave up)", word);
-    }
     const int band_lo = std::max(0, c->host_flags[DevCtx::kBandWord]);
     const int band_hi = std::min(nl - 1, c->host_flags[DevCtx::kBandWord + 1]);
     const int nband = band_hi >= band_lo ? band_hi - band_lo + 1 : 0;
@@ -789,7 +794,8 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     const int per_blk = std::max(1, ntask / std::max(nblk, 1));
     if (nblk > 0) pool.run(nblk * per_blk, [&](int t) {
         const int k = t / per_blk, part = t % per_blk;
-        if (cudaEventSynchronize(c->ev_blk[k]) != cudaSuccess) {
+        if (cudaEventSynchronize(c->ev_flags) != cudaSuccess || c->host_flags[1] ||
+            cudaEventSynchronize(c->ev_blk[k]) != cudaSuccess) {
             cuda_err = 1;
             return;
         }
@@ -833,6 +839,12 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     // buffer stays in use until then
     CK(cudaStreamSynchronize(c->s_copy));
     CK(cudaGetLastError());
+    if (c->host_flags[1]) {  // nothing was merged
+        const int word = c->host_flags[1];
+        cudaMemsetAsync(static_cast<int *>(c->flags.p) + 1, 0, sizeof(int), st);
+        cudaStreamSynchronize(st);
+        return fail(SRG_E_TIMEOUT, "device error word 0x%x (a bounded device wait gave up)", word);
+    }
     if (cuda_err) return fail(SRG_E_CUDA, "copy of the output box failed");
     if (io_err == 1) return fail(SRG_E_IO, "output read failed (fd %d)", fdout);
     if (io_err == 2) return fail(SRG_E_IO, "output write failed (fd %d)", fdout);

@@ -67,7 +67,7 @@ struct DevCtx {
     int upload_seq = 0;
     bool dropin_ready = false;
     cudaStream_t s_main = nullptr, s_copy = nullptr;
-    cudaEvent_t ev_burst = nullptr, ev_flags = nullptr, ev_blk[kOutBlocks] = {};
+    cudaEvent_t ev_burst = nullptr, ev_flags = nullptr, ev_band = nullptr, ev_blk[kOutBlocks] = {};
     int *host_flags = nullptr;
     bool attrs_done[64] = {};
     bool gated_attrs_done[8] = {};
