@@ -225,15 +225,25 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
     // work items index the list of tiles with a formed pixel when there is one
     const int nitems = tile_list ? tile_list[0] : total_tiles;
     // Range lines arriving in pulse order (GATE, one burst): take the tiles in
-    // the order their pulses arrive.  Grid lines run against the pulses when
-    // the azimuth centre of the last formed line precedes the first's.
+    // the order their pulses arrive.
     bool reverse = false;
     if constexpr (GATE) {
-        if (nbursts == 1 && bursts[0].nlines >= 3) {
-            const double *cf = bursts[0].coef;
-            reverse = cf[3 * (bursts[0].nlines - 2) + 2] < cf[2];
-        }
+        if (nbursts == 1) reverse = lines_against_pulses(bursts[0]);
     }
+    // GATE with row blocks: a tile's stores are counted once the CTA has
+    // passed the barrier after them; the count that completes a row block
+    // raises the block's word, releasing its copy back to the host.
+    auto tile_stored = [&](const BurstDev &B, int ly0) {
+        if constexpr (GATE) {
+            if (tid == 0 && B.rb_done) {
+                const int k = (ly0 / TY) / B.rb_tile_rows;
+                if (atomicAdd(B.rb_count + k, 1) == B.rb_expect[k] - 1) {
+                    __threadfence_system();
+                    atomicExch(B.rb_done + k, B.rb_seq);
+                }
+            }
+        }
+    };
     uint32_t gchunk = 0;  // chunks issued/consumed by this CTA so far (uniform)
     uint32_t issued = 0, issued_par = 0;  // producer lane 0: stages with a TMA issued this tile
     int b = 0;  // burst of the current tile (tiles grow, so the search resumes here)
@@ -336,7 +346,9 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
             } else if (lane == 0) {
                 ctl.item = atomicAdd(work_counter, 1);
             }
+            if (GATE && B.rb_done) __threadfence();
             __syncthreads();
+            tile_stored(B, ly0);
             continue;
         }
         // Phase B: consumers place their formed pixels; the producer's lane 0
@@ -939,6 +951,7 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                         B.out[(long long)line * B.out_ld + (px - B.out_pix0)] = o;
                     }
                 }
+                if (GATE && B.rb_done) __threadfence();
             }
         }
         gchunk += nchunks;
@@ -952,6 +965,7 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
             }
             return;
         }
+        tile_stored(B, ly0);
     }
 }
 

@@ -96,6 +96,29 @@ PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
     return fn;
 }
 
+// Stream memory operations of the driver API (a stream waits for, or writes,
+// a 32-bit device word), or nulls where the driver offers none.
+StreamValueOps stream_value_ops() {
+    static StreamValueOps ops;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaDriverEntryPointQueryResult q1, q2;
+        void *w = nullptr, *r = nullptr;
+        if (cudaGetDriverEntryPoint("cuStreamWaitValue32", &w, cudaEnableDefault, &q1) ==
+                cudaSuccess &&
+            q1 == cudaDriverEntryPointSuccess &&
+            cudaGetDriverEntryPoint("cuStreamWriteValue32", &r, cudaEnableDefault, &q2) ==
+                cudaSuccess &&
+            q2 == cudaDriverEntryPointSuccess) {
+            ops.wait = reinterpret_cast<StreamValueFn>(w);
+            ops.write = reinterpret_cast<StreamValueFn>(r);
+        } else {
+            cudaGetLastError();
+        }
+    });
+    return ops;
+}
+
 // Kernel entry for a form and shape index (-1: the default of that form).
 const KernelEntry *pick_kernel(int form, int cfg) {
     if (cfg >= 0) {
@@ -254,6 +277,13 @@ int ensure_dropin(DevCtx &c) {
         cudaGetLastError();
         return fail(SRG_E_NOMEM, "pinned error word allocation failed");
     }
+    CK(cudaStreamCreateWithFlags(&c.s_back, cudaStreamNonBlocking));
+    if (cudaMallocHost(&c.host_rb, 4 * DevCtx::kRowBlocks * sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(SRG_E_NOMEM, "pinned row-block words allocation failed");
+    }
+    int rc = c.rb.ensure(4 * DevCtx::kRowBlocks * sizeof(int));  // zeroed
+    if (rc) return rc;
     c.dropin_ready = true;
     return SRG_OK;
 }
@@ -270,6 +300,12 @@ namespace {
 struct UploadGate {
     const int *word;
     int base, rows;
+    // row blocks finished while the sum runs (null: none): the DevCtx::rb
+    // words, tile rows per block, the value of a finished block's word, and
+    // the pinned copy of the kept counts and the order word
+    int *rb = nullptr;
+    int rb_tile_rows = 0, rb_seq = 0;
+    int *rb_host = nullptr;
 };
 
 // Core: launch the tiled kernel over n prepared bursts.
@@ -336,6 +372,15 @@ int run_bursts(DevCtx &c, const srg_burst_desc *descs, int n, const srg_bp_optio
             B.ready = gate->word;
             B.ready_base = gate->base;
             B.ready_rows = gate->rows;
+            if (gate->rb) {
+                constexpr int K = DevCtx::kRowBlocks;
+                B.rb_count = gate->rb;
+                B.rb_expect = gate->rb + K;
+                B.rb_order = gate->rb + 2 * K;
+                B.rb_done = gate->rb + 3 * K;
+                B.rb_tile_rows = gate->rb_tile_rows;
+                B.rb_seq = gate->rb_seq;
+            }
         }
         hb[i] = B;
     }
@@ -364,6 +409,9 @@ int run_bursts(DevCtx &c, const srg_burst_desc *descs, int n, const srg_bp_optio
     CK(launch_tile_list(d_bursts, n, max_burst_tiles, total, TX, TY, c.tiles.p, st, band));
     if (band && band_host) {
         CK(cudaMemcpyAsync(band_host, band, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+        if (gated && gate->rb && gate->rb_host)
+            CK(cudaMemcpyAsync(gate->rb_host, gate->rb + DevCtx::kRowBlocks,
+                               (DevCtx::kRowBlocks + 1) * sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaEventRecord(band_ready, st));
     }
     CK(launch_tiles(run, grid, smem, st, d_bursts, n, total,
@@ -669,7 +717,7 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
         }
         return SRG_OK;
     };
-    const UploadGate gate{ready_word, ready_base, up_rows};
+    UploadGate gate{ready_word, ready_base, up_rows};
     // Host-to-device copies leave the copy engine in the order they are
     // issued, whatever their stream: with a gated kernel the small inputs go
     // first, then the first block, then (while it travels) the DEM box and the
@@ -677,6 +725,30 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     // launch, which waits for them all.
     const KernelEntry *ke0 = pick_kernel(o.form, o.tile_cfg);
     const bool pipelined = ke0 && gated_twin(*ke0) != nullptr;
+    // With the gated kernel the output also comes back while the sum runs: the
+    // grid lines are cut into row blocks of whole tile rows; the kernel counts
+    // the stored tiles of each block and raises the block's done word when the
+    // count reaches the block's kept tiles, and a stream of its own waits for
+    // that word before it copies the block back.  Every done word is also
+    // written on the main stream after the kernel, so each wait ends even when
+    // the kernel gives up early (the block then merges only if the error word
+    // is clear).
+    constexpr int K = DevCtx::kRowBlocks;
+    const StreamValueOps svo = stream_value_ops();
+    const int tile_ty = ke0 ? ke0->shape.ty : 1;
+    const int tiles_y = (nl + tile_ty - 1) / tile_ty;
+    const int rb_tiles = std::max(1, (tiles_y + K - 1) / K);
+    const int nrb = (tiles_y + rb_tiles - 1) / rb_tiles;
+    const bool rows_back = pipelined && svo.wait && svo.write;
+    int *rbw = static_cast<int *>(c->rb.p);
+    if (rows_back) {
+        gate.rb = rbw;
+        gate.rb_tile_rows = rb_tiles;
+        gate.rb_seq = c->upload_seq;
+        gate.rb_host = c->host_rb;
+        for (int k = 0; k <= K; ++k) c->host_rb[k] = 0;
+        CK(cudaMemsetAsync(rbw, 0, (2 * K + 1) * sizeof(int), st));
+    }
     CK(cudaMemcpyAsync(c->in_sat.p, satloc, 24 * (size_t)rawdatalines, cudaMemcpyHostToDevice, st));
     if ((rc = upload(0, pipelined ? 1 : nup))) {
         cudaStreamSynchronize(c->s_copy);  // the caller's buffer stays in use until then
@@ -767,10 +839,20 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
         cudaStreamSynchronize(st);
         return rc;
     }
-    // The band is known once the work list is built, ahead of the backprojection:
-    // its rows' copies back are queued behind the sum at once, after the error
-    // word; the merge of a block starts as soon as that block is back (and the
-    // error word is clear).
+    // The done words' writes after the kernel, issued after every upload copy
+    // (a stream's wait for the kernel must not hold copies the kernel needs,
+    // should two streams share a hardware queue).  Blocks [0, nfall) have one.
+    int nfall = 0;
+    if (rows_back) {
+        while (nfall < nrb &&
+               svo.write(st, reinterpret_cast<CUdeviceptr>(rbw + 3 * K + nfall),
+                         (cuuint32_t)c->upload_seq, 0) == CUDA_SUCCESS)
+            ++nfall;
+    }
+    // The band is known once the work list is built, ahead of the backprojection.
+    // Without row blocks its rows' copies back are queued behind the sum at
+    // once, after the error word, in up to kOutBlocks blocks; the merge of a
+    // block starts as soon as that block is back and the error word is clear.
     CK(cudaEventSynchronize(c->ev_band));
     CK(cudaMemcpyAsync(c->host_flags, c->flags.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaEventRecord(c->ev_flags, st));
@@ -778,14 +860,54 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     const int band_hi = std::min(nl - 1, c->host_flags[DevCtx::kBandWord + 1]);
     const int nband = band_hi >= band_lo ? band_hi - band_lo + 1 : 0;
     float *win = static_cast<float *>(c->host_stage);
-    const int nblk = std::min(nband, (int)DevCtx::kOutBlocks);
-    for (int k = 0; k < nblk; ++k) {
-        const int r0 = band_lo + (int)((long long)nband * k / nblk);
-        const int r1 = band_lo + (int)((long long)nband * (k + 1) / nblk);
+    struct OutBlock {
+        int r0, r1;  // rows [r0, r1) of the box
+        int rb;      // row block whose stored count came back with it, or -1
+    };
+    OutBlock blk[DevCtx::kOutBlocks];
+    int nblk = 0;
+    auto copy_back = [&](int r0, int r1, cudaStream_t s) {
         const size_t off = (size_t)r0 * ncols * 2, n = (size_t)(r1 - r0) * ncols * 8;
-        CK(cudaMemcpyAsync(win + off, static_cast<float *>(c->out.p) + off, n, cudaMemcpyDeviceToHost,
-                           st));
-        CK(cudaEventRecord(c->ev_blk[k], st));
+        return cudaMemcpyAsync(win + off, static_cast<float *>(c->out.p) + off, n,
+                               cudaMemcpyDeviceToHost, s);
+    };
+    if (rows_back) {
+        // in the order the kernel finishes them (it takes the tiles from the
+        // last line back when the lines run against the pulses)
+        const bool from_last = c->host_rb[K] != 0;
+        for (int i = 0; i < nrb; ++i) {
+            const int k = from_last ? nrb - 1 - i : i;
+            const int r0 = std::max(band_lo, k * rb_tiles * tile_ty);
+            const int r1 = std::min(band_hi + 1, std::min(nl, (k + 1) * rb_tiles * tile_ty));
+            if (r0 >= r1 || c->host_rb[k] == 0) continue;  // no kept tile: nothing formed
+            OutBlock &b = blk[nblk];
+            b.r0 = r0;
+            b.r1 = r1;
+            b.rb = -1;
+            if (k < nfall &&
+                svo.wait(c->s_back, reinterpret_cast<CUdeviceptr>(rbw + 3 * K + k),
+                         (cuuint32_t)c->upload_seq, CU_STREAM_WAIT_VALUE_EQ) == CUDA_SUCCESS) {
+                CK(copy_back(r0, r1, c->s_back));
+                CK(cudaMemcpyAsync(c->host_rb + 2 * K + k, rbw + k, sizeof(int),
+                                   cudaMemcpyDeviceToHost, c->s_back));
+                CK(cudaEventRecord(c->ev_blk[nblk], c->s_back));
+                b.rb = k;
+            } else {
+                CK(copy_back(r0, r1, st));
+                CK(cudaEventRecord(c->ev_blk[nblk], st));
+            }
+            ++nblk;
+        }
+    } else {
+        const int n = std::min(nband, (int)DevCtx::kOutBlocks);
+        for (int k = 0; k < n; ++k) {
+            OutBlock &b = blk[nblk++];
+            b.r0 = band_lo + (int)((long long)nband * k / n);
+            b.r1 = band_lo + (int)((long long)nband * (k + 1) / n);
+            b.rb = -1;
+            CK(copy_back(b.r0, b.r1, st));
+            CK(cudaEventRecord(c->ev_blk[k], st));
+        }
     }
 
     // merge into the .geo rows (azimuth_compress.cu:510-537); pixels outside
@@ -794,13 +916,18 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     const int per_blk = std::max(1, ntask / std::max(nblk, 1));
     if (nblk > 0) pool.run(nblk * per_blk, [&](int t) {
         const int k = t / per_blk, part = t % per_blk;
-        if (cudaEventSynchronize(c->ev_flags) != cudaSuccess || c->host_flags[1] ||
-            cudaEventSynchronize(c->ev_blk[k]) != cudaSuccess) {
+        if (cudaEventSynchronize(c->ev_blk[k]) != cudaSuccess) {
             cuda_err = 1;
             return;
         }
-        const int b0 = band_lo + (int)((long long)nband * k / nblk);
-        const int b1 = band_lo + (int)((long long)nband * (k + 1) / nblk);
+        // a row block came back with every kept tile stored; any other block
+        // waits for the kernel's end and merges only with the error word clear
+        const bool whole = blk[k].rb >= 0 && c->host_rb[2 * K + blk[k].rb] == c->host_rb[blk[k].rb];
+        if (!whole && (cudaEventSynchronize(c->ev_flags) != cudaSuccess || c->host_flags[1])) {
+            cuda_err = 1;
+            return;
+        }
+        const int b0 = blk[k].r0, b1 = blk[k].r1;
         const int r0 = b0 + (int)((long long)(b1 - b0) * part / per_blk);
         const int r1 = b0 + (int)((long long)(b1 - b0) * (part + 1) / per_blk);
         std::vector<float> cur(2 * (size_t)ncols);
@@ -838,8 +965,9 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     // the upload may end after the last chunk that needed it: the caller's
     // buffer stays in use until then
     CK(cudaStreamSynchronize(c->s_copy));
+    CK(cudaStreamSynchronize(c->s_back));
     CK(cudaGetLastError());
-    if (c->host_flags[1]) {  // nothing was merged
+    if (c->host_flags[1]) {  // only row blocks whose every tile was stored were merged
         const int word = c->host_flags[1];
         cudaMemsetAsync(static_cast<int *>(c->flags.p) + 1, 0, sizeof(int), st);
         cudaStreamSynchronize(st);

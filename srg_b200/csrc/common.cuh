@@ -41,7 +41,21 @@ struct BurstDev {
     // n * ready_rows pulse rows are in device memory.
     const int *ready;
     int ready_base, ready_rows;
+    // Rows finished while the sum still runs (the drop-in entry): null, or per
+    // row block of rb_tile_rows tile rows a count of stored tiles, the count of
+    // kept tiles (the work list adds it up), and a word set to rb_seq once
+    // the two agree; the work list also sets *rb_order to
+    // lines_against_pulses (the order the blocks finish in).
+    int *rb_count, *rb_expect, *rb_done, *rb_order;
+    int rb_tile_rows, rb_seq;
 };
+
+// Grid lines run against the pulses (the azimuth centre of the last formed
+// line precedes the first's): a burst's tiles are then taken from the last
+// line back when its range lines arrive in pulse order.
+__device__ __forceinline__ bool lines_against_pulses(const BurstDev &B) {
+    return B.nlines >= 3 && B.coef[3 * (B.nlines - 2) + 2] < B.coef[2];
+}
 
 // Kernel shape of the tiled backprojection.
 struct TileShape {

@@ -64,9 +64,18 @@ struct DevCtx {
     // tiles, [kReadyWord] rows-uploaded word; host_flags[kReadyHost + k] holds
     // the value the copy stream writes after upload block k
     static constexpr int kBandWord = 4, kReadyWord = 6, kReadyHost = 8, kUploadBlocks = 8;
+    // row blocks copied back while the sum still runs (gated kernel): device
+    // words rb[k] stored-tile counts, rb[kRowBlocks + k] kept-tile counts,
+    // rb[2 kRowBlocks] the order word, rb[3 kRowBlocks + k] done words;
+    // host_rb[0 .. kRowBlocks] the kept counts and the order word, copied back
+    // with the band, host_rb[2 kRowBlocks + k] the stored count read with
+    // block k
+    static constexpr int kRowBlocks = kOutBlocks;
+    DevBuf rb;
+    int *host_rb = nullptr;
     int upload_seq = 0;
     bool dropin_ready = false;
-    cudaStream_t s_main = nullptr, s_copy = nullptr;
+    cudaStream_t s_main = nullptr, s_copy = nullptr, s_back = nullptr;
     cudaEvent_t ev_burst = nullptr, ev_flags = nullptr, ev_band = nullptr, ev_blk[kOutBlocks] = {};
     int *host_flags = nullptr;
     bool attrs_done[64] = {};
@@ -75,6 +84,11 @@ struct DevCtx {
 
 // Per-device context (sets the device current).
 int get_ctx(int device, DevCtx **out);
+using StreamValueFn = CUresult (*)(CUstream, CUdeviceptr, cuuint32_t, unsigned int);
+struct StreamValueOps {
+    StreamValueFn wait = nullptr, write = nullptr;
+};
+StreamValueOps stream_value_ops();
 // Streams, events and pinned error word of the drop-in entry (made once).
 int ensure_dropin(DevCtx &c);
 // Kernel entry for a form and shape index (-1: the default of that form).

@@ -309,6 +309,7 @@ __global__ void __launch_bounds__(256) tile_mask_kernel(const BurstDev *__restri
         keep = !finite || !(hi < (double)B.ap2 - 1e-3 || lo > (double)(B.P - B.ap2) + 1e-3);
     }
     keep = __any_sync(0xffffffffu, keep);
+    if (B.rb_order && ti == 0 && lane == 0) *B.rb_order = lines_against_pulses(B) ? 1 : 0;
     if (!keep && lane < tx && px0 + lane <= px1) {
         for (int y = 0; y < nl; ++y)
             B.out[(long long)(ly0 + y) * B.out_ld + (px0 + lane - B.out_pix0)] = make_float2(0.f, 0.f);
@@ -322,6 +323,7 @@ __global__ void __launch_bounds__(256) tile_mask_kernel(const BurstDev *__restri
                 atomicMin(band, ly0);
                 atomicMax(band + 1, ly0 + nl - 1);
             }
+            if (B.rb_expect) atomicAdd(B.rb_expect + (ti / B.tiles_x) / B.rb_tile_rows, 1);
         }
     }
 }
