@@ -295,8 +295,8 @@ using namespace srg::detail;
 
 namespace {
 
-// Range lines that are still being copied in blocks of `rows` pulse rows:
-// the copy stream raises `*word` to base + n after the first n blocks.
+// Range lines that are still being copied in granules of `rows` pulse rows:
+// the copy stream raises `*word` to base + n once the first n granules are in.
 struct UploadGate {
     const int *word;
     int base, rows;
@@ -692,26 +692,29 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     // each block the copy stream raises a device word, and the backprojection,
     // launched without waiting for the whole upload, takes a chunk of pulses as
     // soon as its rows are in.  The orbit, the DEM box and the azimuth centres
-    // (which need no range lines) proceed meanwhile.  The word only grows
-    // (call number x 16 + blocks), so a value left by an earlier call never
-    // satisfies a later one.
+    // (which need no range lines) proceed meanwhile.  The word counts granules
+    // of P/32 pulse rows; the blocks shrink toward the end (6, 6, 5, 5, 4, 3,
+    // 2, 1 granules), so that little of the sum waits for the last one.  The
+    // word only grows (call number x 64 + granules), so a value left by an
+    // earlier call never satisfies a later one.
     int *ready_word = static_cast<int *>(c->flags.p) + DevCtx::kReadyWord;
-    const int nup = std::min(rawdatalines, (int)DevCtx::kUploadBlocks);
-    const int up_rows = (rawdatalines + nup - 1) / nup;
-    c->upload_seq = c->upload_seq >= (1 << 26) ? 1 : c->upload_seq + 1;
-    const int ready_base = c->upload_seq * 16;
+    constexpr int kGranules = 32;
+    static const int kBlockEnd[DevCtx::kUploadBlocks] = {6, 12, 17, 22, 26, 29, 31, 32};
+    const int nup = DevCtx::kUploadBlocks;
+    const int up_rows = (rawdatalines + kGranules - 1) / kGranules;  // rows per granule
+    const int ngran = (rawdatalines + up_rows - 1) / up_rows;
+    c->upload_seq = c->upload_seq >= (1 << 24) ? 1 : c->upload_seq + 1;
+    const int ready_base = c->upload_seq * 64;
     const size_t row_bytes = (size_t)samplesPerBurst * 8;
     auto upload = [&](int kb, int ke) -> int {
         for (int k = kb; k < ke; ++k) {
-            const int r0 = k * up_rows, r1 = std::min(rawdatalines, r0 + up_rows);
-            if (r0 >= r1) {
-                c->host_flags[DevCtx::kReadyHost + k] = ready_base + nup;
-            } else {
+            const int g0 = k ? std::min(kBlockEnd[k - 1], ngran) : 0, g1 = std::min(kBlockEnd[k], ngran);
+            const int r0 = std::min(rawdatalines, g0 * up_rows), r1 = std::min(rawdatalines, g1 * up_rows);
+            if (r0 < r1)
                 CK(cudaMemcpyAsync(static_cast<char *>(c->in_burst.p) + r0 * row_bytes,
                                    reinterpret_cast<const char *>(burstdata) + r0 * row_bytes,
                                    (r1 - r0) * row_bytes, cudaMemcpyHostToDevice, c->s_copy));
-                c->host_flags[DevCtx::kReadyHost + k] = ready_base + k + 1;
-            }
+            c->host_flags[DevCtx::kReadyHost + k] = ready_base + g1;
             CK(cudaMemcpyAsync(ready_word, c->host_flags + DevCtx::kReadyHost + k, sizeof(int),
                                cudaMemcpyHostToDevice, c->s_copy));
         }
