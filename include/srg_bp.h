@@ -80,7 +80,9 @@ void azimuth_compress_(
     double *dmrg, double *wvl, int *aperture, int *iaperture,
     double *angc0, double *angc1, double *prf);
 
-/* Same call with a status and explicit options (opts may be NULL). */
+/* Same call with a status and explicit options (opts may be NULL).  On
+ * SRG_E_TIMEOUT only rows whose every formed pixel was computed have been
+ * merged into *fdout; the other rows are left as they were. */
 int srg_azimuth_compress(
     const float *burstdata, const double *satloc, int rawdatalines,
     int samplesPerBurst, int demwidth, int demlength, int fdout, int fddem,
