@@ -15,7 +15,8 @@ lines are larger than L2, so no flush is needed between steps.
 
 --impl reference times the reference's own CPU backprojection
 (sentinel/azimuth_compress_cpu.c compiled from source into oracle/_ref,
-OpenMP over all host cores) on a bounded slab of the same burst.
+OpenMP over all host cores) on whole bursts of the same workload, one burst
+per step, built on the host (neither the GPU nor the CUDA library is used).
 """
 from __future__ import annotations
 
@@ -332,49 +333,139 @@ def combine_ranks(torch, dist, device, maxes, sums):
     return t.tolist(), u.tolist()
 
 
-def reference_cpu_sample(wl, budget_s: float = 15.0):
-    """Time the reference CPU backprojection (oracle/_ref, compiled from the
-    reference sources, unmodified) end to end on a slab of grid lines of the
-    workload's first burst, restricted through latlons as the reference's
-    driver would.  Returns (terms/s, cores, description)."""
-    import copy
+WORKLOADS = {
+    "c1": ("IW1 burst 1500x21000 complex64 -> 2400x1200 grid at 1e-4 deg, volcano DEM "
+           "(0-2500 m cone + fBm, Hurst 0.8, 30 m RMS)", 1),
+    "c2": ("IW1 burst 1500x21000 complex64 on 2x-oversampled range lines (8-tap windowed sinc) "
+           "-> 2400x1200 grid at 1e-4 deg, volcano DEM", 1),
+    "c3": ("IW scene: 3 subswaths x 9 bursts (P 1380-1620, S 18000/21500/25600 complex64), "
+           "sub-grids 2000-2600 x 1000-1300 at 1e-4 deg on a shared 16504x6646 volcano DEM, "
+           "merged in burst order", 27),
+    "c4": ("repeat-pass stack: 32 passes of 1500x21000 complex64 onto a common 2400x1200 grid "
+           "at 1e-4 deg, perpendicular baselines U[+-150 m], along-track U[+-5 m], Mogi source "
+           "3 km deep, 10 cm max LOS; then crossmul of 31 sequential pairs", 32),
+}
+STEPS = {
+    "c3": "one pass over the scene: azimuth centres of every line, work list of the tiles with "
+          "a formed pixel, one persistent backprojection launch for all bursts, ordered merge "
+          "into the scene raster",
+    "c4": "one pass over the stack: azimuth centres of every pass, work list, one persistent "
+          "backprojection launch for all passes onto the common grid",
+    "c1": "one pass over the burst: azimuth centres of every line, work list, one "
+          "backprojection launch",
+    "c2": "one pass over the burst: azimuth centres of every line, work list, one "
+          "backprojection launch (lines oversampled once, beforehand)",
+}
 
+
+def workload_config(workload: str, world: int) -> dict:
+    """The `config` of the JSON line, identical in both arms."""
+    desc, nb = WORKLOADS[workload]
+    if world == 1:
+        par = "1 GPU"
+    elif workload == "c3":
+        par = (f"scene partition over {world} GPUs: bursts dealt by estimated terms (LPT), "
+               "ordered merge of the ranks' rasters in burst order")
+    else:
+        par = f"replicas x{world} (one workload per GPU)"
+    return {"workload": desc, "bursts": nb, "step": STEPS[workload],
+            "l2": "range lines of every burst > 126 MB L2; no flush between steps",
+            "parallelism": par}
+
+
+def host_bursts(workload: str):
+    """The workload's bursts on the host for the CPU runs, built without the
+    GPU or the CUDA library: the same geometry as the device workload (orbit,
+    grid, volcano DEM synthesised with numpy), range lines drawn per burst by
+    ``scene.host_clutter_samples`` when a burst is used.  Returns a list of
+    (burst, sample seed, line length)."""
+    from srg_b200 import scene
+    if workload == "c3":
+        _, bursts = scene.iw_scene(seed=1003)   # acquisition order, host DEM
+        return [(b, 1003 * 100 + i, b.samples) for i, b in enumerate(bursts)]
+    seed = {"c1": 1001, "c2": 1001, "c4": 1004}[workload]
+    b = scene.config1_geometry(seed=seed)
+    if workload == "c2":   # the 2x-oversampled line: 2S - 1 samples at dmrg / 2
+        b.dmrg = b.dmrg / 2.0
+        return [(b, seed, 2 * b.samples - 1)]
+    return [(b, seed, b.samples)]
+
+
+def reference_cpu(workload: str, steps: int, warmup: int):
+    """Time the reference CPU backprojection (sentinel/azimuth_compress_cpu.c
+    compiled from source, unmodified, in oracle/_ref; OpenMP over every host
+    core) end to end through its 33-argument entry, one whole burst per step
+    (the workload's bursts in acquisition order, cycling), with DEM and .geo
+    files on tmpfs.  Terms per burst come from the oracle's exact count
+    (liboracle.so, the reference's window and range test), outside the timed
+    call.  Neither the GPU nor the CUDA library is touched.  Returns
+    (terms/s over the timed steps, cores, sample description)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     cores = os.cpu_count() or 1
     os.environ["OMP_NUM_THREADS"] = str(cores)
     import oracle as O
-    from srg_b200 import api
-    ref = O.RefCPU()
-    db = wl.bursts[0]
-    b = copy.copy(db.b)
-    b.burst = db.burst.cpu().numpy()
-    formed = (db.out.abs() > 0).any(dim=1).cpu().numpy()
-    rows = np.nonzero(formed)[0]
-    mid = int(rows[len(rows) // 2]) + db.firstline if len(rows) else db.firstline + db.nlines // 2
-
-    def slab(n):
-        s = copy.copy(b)
-        s.latlons = np.array(b.latlons, np.float64)
-        lo, hi = mid - n // 2, mid - n // 2 + n   # lines [lo, hi] (hi excluded from sums)
-        s.latlons[1] = b.firstlat + (lo + 0.25) * b.deltalat
-        s.latlons[0] = b.firstlat + (hi + 0.25) * b.deltalat
-        return s
-
-    n = 4
-    while True:
-        s = slab(n)
+    from srg_b200 import scene
+    ref, orc = O.RefCPU(), O.Oracle()
+    bursts = host_bursts(workload)
+    tmp = "/dev/shm" if os.path.isdir("/dev/shm") else None
+    terms_tot, secs_tot, used = 0, 0.0, []
+    for step in range(warmup + steps):
+        k = step % len(bursts)
+        b, seed, S = bursts[k]
+        scene.host_clutter_samples(b, seed, samples=S)
         with quiet_stdout():
             timing = {}
-            ref.azimuth_compress_cpu(s, timing=timing)
-            dt = timing["call_s"]
-        if dt > budget_s / 8 or n >= db.nlines:
-            break
-        n = min(db.nlines, max(n * 2, int(n * budget_s / 4 / max(dt, 1e-3))))
-    # exact term count of the slab: the reference's FP64 predicate, on the GPU
-    sdb = api.to_device(s, device=db.out.device, burst_tensor=db.burst)
-    terms = api.count_terms([sdb])
-    return terms / dt, cores, (f"reference azimuth_compress_cpu_ (OpenMP, {cores} threads) end to "
-                               f"end on {sdb.nlines} grid lines of burst 0 ({terms} terms, {dt:.2f} s)")
+            O.run_33_files(ref.lib.azimuth_compress_cpu_, b, timing=timing, tmpdir=tmp,
+                               read_back=False)
+        if step >= warmup:
+            terms_tot += orc.count_terms(b, nthreads=cores)
+            secs_tot += timing["call_s"]
+            used.append(k)
+        b.burst = np.zeros((0, S), np.complex64)   # free the lines
+    desc = (f"reference azimuth_compress_cpu_ (OpenMP, {cores} threads) end to end on whole "
+            f"bursts {used} of the workload, one per step ({terms_tot} terms, {secs_tot:.1f} s)")
+    return terms_tot / secs_tot, cores, desc
+
+
+# ---------------------------------------------------------------------------
+# profiling driver
+
+
+def profile_shapes(torch, workload: str, shapes, samples: str = "random", seed=None):
+    """A fixed workload and a list of kernel shapes: one warm-up launch, then
+    one measured launch per shape, nothing else on the GPU (the command line
+    of the committed ncu summaries).  c1: one IW1-sized burst (random or
+    forward-projected samples); c3: the 27-burst IW scene, azimuth centres
+    and backprojection stages of its scene plan.  Under ncu, select the
+    backprojection kernels by name (regex:bp_) and skip the warm-up launches
+    with -s <number of shapes>."""
+    from srg_b200 import _lib, api, scene, workloads
+    cfgs = _lib.tile_configs()
+    if workload == "c3":
+        wl = workloads.config3(seed=1003 if seed is None else seed)
+        plan = wl.plan
+        for rep in range(2):  # warm-up, then measured
+            for s in shapes:
+                plan.set_form(cfgs[s][1], s)
+                plan.run_stages(1 | 2, 0)
+        plan.sync(0)
+        return
+    seed = 1001 if seed is None else seed
+    if samples == "forward":
+        wl = workloads.config1(seed=seed)
+        db, coef = wl.bursts[0], wl.coefs[0]
+    else:
+        b = scene.config1_geometry(seed=seed)
+        g = torch.Generator(device="cuda")
+        g.manual_seed(seed)
+        bt = torch.complex(torch.randn(b.rawdatalines, b.samples, device="cuda", generator=g),
+                           torch.randn(b.rawdatalines, b.samples, device="cuda", generator=g))
+        db = api.to_device(b, burst_tensor=bt)
+        coef = api.line_centres(db)
+    for rep in range(2):  # warm-up, then measured
+        for s in shapes:
+            api.backproject([db], form=cfgs[s][1], tile_cfg=s, coefs=[coef])
+    torch.cuda.synchronize()
 
 
 # ---------------------------------------------------------------------------
@@ -392,35 +483,31 @@ def main():
     ap.add_argument("--shapes", default=None,
                     help="SPLIT,FP64 kernel shape indices (srg_tile_config; -1: the form's "
                          "default shape); default: tuned")
+    ap.add_argument("--profile-shapes", default=None,
+                    help="comma-separated kernel shape indices: run the profiling driver on "
+                         "--workload c1 or c3 instead of the benchmark")
+    ap.add_argument("--samples", default="random", choices=["random", "forward"],
+                    help="profiling driver, c1: random or forward-projected range lines")
     args = ap.parse_args()
+    if args.profile_shapes is not None:
+        import torch
+        profile_shapes(torch, args.workload, [int(x) for x in args.profile_shapes.split(",")],
+                       args.samples)
+        print("ok", args.profile_shapes)
+        return
     pinned = [int(x) for x in args.shapes.split(",")] if args.shapes else None
     rank, world, local = dist_env()
-    if args.impl == "reference" and rank != 0:
-        return  # the reference arm runs on rank 0 only
-
-    import torch
-    import torch.distributed as dist
-    if world > 1 and args.impl == "ours":
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
-    torch.cuda.set_device(local)
-    from srg_b200 import _lib, workloads
-
-    build = {"c1": workloads.config1, "c2": workloads.config1, "c3": workloads.config3,
-             "c4": workloads.config4}[args.workload]
+    config = workload_config(args.workload, world)
     if args.impl == "reference":
-        wl = build(device=f"cuda:{local}")
-        from srg_b200 import api
-        for db in wl.bursts[:1]:  # marks the formed rows of the sampled burst
-            api.backproject([db], form=_lib.FORM_FP64)
-        vals = []
-        for _ in range(max(1, args.steps)):
-            v, cores, sample = reference_cpu_sample(wl, budget_s=8.0)
-            vals.append(v)
-        value = float(np.median(vals)) / 1e9
+        if rank != 0:
+            return  # the reference arm runs on rank 0 only
+        # host only: neither torch.cuda nor the CUDA library is loaded here
+        value, cores, sample = reference_cpu(args.workload, max(1, args.steps), args.warmup)
+        value /= 1e9
         line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
                 "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic", "config": {"workload": wl.description},
+                "data": "synthetic", "config": config,
                 "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
                                  "sample": sample},
                 "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
@@ -428,6 +515,15 @@ def main():
         print(json.dumps(line))
         return
 
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    from srg_b200 import _lib, workloads
+
+    build = {"c1": workloads.config1, "c2": workloads.config1, "c3": workloads.config3,
+             "c4": workloads.config4}[args.workload]
     wl = build(device=f"cuda:{local}",
                seed={"c1": 1001, "c2": 1001, "c3": 1003, "c4": 1004}[args.workload] + rank)
 
@@ -493,9 +589,10 @@ def main():
     achieved = FLOPS_PER_TERM * wl.terms / (s_kern * 1e-3) / 1e12
     traffic = load_traffic("bp_split", wl.name)
     cpu = None
-    if rank == 0 and not args.no_cpu_baseline and os.path.exists(
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(
             os.path.join(ROOT, "oracle", "_ref", "libref_cpu.so")):
-        v, cores, sample = reference_cpu_sample(wl)
+        # a bounded sample: one whole burst per subswath (c3) or the burst
+        v, cores, sample = reference_cpu(args.workload, 3 if args.workload == "c3" else 1, 0)
         cpu = {"value": v / 1e9, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample}
     if rank != 0:
         if world > 1:
@@ -510,20 +607,10 @@ def main():
                        "deformation, repeat-pass baselines",
                  "c1": "synthetic, seeded: forward-projected scatterers",
                  "c2": "synthetic, seeded: forward-projected scatterers"}[args.workload],
-        "config": {"workload": wl.description, "bursts": len(wl.bursts),
-                   "terms_per_step_per_gpu": wl.terms,
-                   "l2": "range lines of every burst > 126 MB L2; no flush between steps",
-                   "parallelism": f"replicas x{world} (one workload per GPU)",
-                   "kernel_shapes": {k: _lib.tile_config_name(v[0]) for k, v in tuned.items()},
-                   "step": {"c3": "one graph replay: azimuth centres of every line, work list of the "
-                                  "tiles with a formed pixel, one persistent backprojection launch for "
-                                  "all bursts, ordered merge into the scene raster",
-                            "c4": "one graph replay: azimuth centres of every pass, work list, one "
-                                  "persistent backprojection launch for all passes onto the common grid",
-                            "c1": "one graph replay: azimuth centres of every line, work list, one "
-                                  "backprojection launch",
-                            "c2": "one graph replay: azimuth centres of every line, work list, one "
-                                  "backprojection launch (lines oversampled once, beforehand)"}[args.workload]},
+        "config": config,
+        "workload_detail": wl.description,
+        "terms_per_step": terms_all,
+        "kernel_shapes": {k: _lib.tile_config_name(v[0]) for k, v in tuned.items()},
         "fp64_form": {"value": fp64_value, "ms_per_step": d_ms, "kernel_ms": d_kern,
                       "split_over_fp64": value / fp64_value},
         "phase_error_vs_fp64": perr,

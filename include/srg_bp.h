@@ -42,10 +42,18 @@ typedef struct srg_bp_options {
     int centres_on_host; /* 1: per-line azimuth centres solved on the host CPU,
                             0: on the GPU (default) */
     int verbose;       /* 1: print the reference's "Burst line limits" line */
+    int spin_limit;    /* polls of a bounded device-side wait (for range lines
+                          still uploading, or for a staged tile) before the
+                          kernel gives up and the call returns SRG_E_TIMEOUT;
+                          0: the default, 4,194,304 (about 1-2 s) */
+    long long scratch_limit; /* bytes of device scratch one drop-in call may
+                          hold (range lines, orbit, DEM box, output box, work
+                          list); a call needing more returns SRG_E_NOMEM before
+                          any GPU work; 0: no limit */
 } srg_bp_options;
 
 /* Fill *o with the defaults (split form, tuned tile, current device,
- * centres on the GPU, quiet). */
+ * centres on the GPU, quiet, default wait limit, no scratch limit). */
 void srg_bp_default_options(srg_bp_options *o);
 
 /* Message of the last failing call on this thread ("" if none). */
@@ -97,6 +105,39 @@ int srg_azimuth_compress(
 void srg_set_default_options(const srg_bp_options *o);
 
 /* ------------------------------------------------------------------------
+ * Per-burst scalars of the azimuth_compress_ call, derived as
+ * sentinel/backprojectgpusub.f90 derives them before each call: burstparams
+ * (:406-429) from the first line's header, the steering-angle fit fdopcoefs
+ * (:262-309, linfit :381-403; all but 20 lines at each end), the aperture
+ * (:190-209, from the velocity of pulse P/2 in 1-based numbering) and the
+ * azimuth and range limits (:213-227).  Replaces that Fortran, which the
+ * caller runs on the host; the arithmetic keeps its single- and
+ * double-precision steps, so the values are the reference's bit for bit.
+ * ------------------------------------------------------------------------ */
+typedef struct srg_burst_params_t {
+    double starttime;  /* s of day, line 0's header bytes 68-75 */
+    double prf;        /* Hz */
+    double samplefreq; /* Hz */
+    double pri;        /* s */
+    double range0;     /* m, near range incl. the reference's 60 m calibration */
+    double wvl;        /* m (the reference's single-precision literal) */
+    double angc0, angc1; /* steering fit: angle (deg) = angc0 + angc1 t */
+    double tstart, tend, tmid, dtaz; /* s */
+    double rngstart, rngend, dmrg;   /* m */
+    int aperture;      /* pulses */
+    int pad;
+} srg_burst_params_t;
+
+/* lines: [P][ld] complex64 decoded range lines of one burst whose first 10
+ * samples (80 bytes) still hold each line's header (the reference zeroes
+ * them only after this step, backprojectgpusub.f90:191); S: samples per line
+ * including those 10; satvel: [P][3] per-pulse velocity (m/s).  Host
+ * pointers.  SRG_E_ARG for fewer than 41 lines, a zero PRI code or an
+ * unknown range decimation code. */
+int srg_burst_params(const float *lines, long long ld, int P, int S, const double *satvel,
+                     srg_burst_params_t *out);
+
+/* ------------------------------------------------------------------------
  * Device-resident bursts (no file I/O; all pointers are device pointers
  * unless noted).  The unit of the batched scene launch.
  * ------------------------------------------------------------------------ */
@@ -130,6 +171,22 @@ typedef struct srg_burst_desc {
  * enqueueing; srg_sync_check() reports device-side errors. */
 int srg_bp_bursts_device(const srg_burst_desc *bursts, int n,
                          const srg_bp_options *opts, void *stream);
+
+/* One burst whose range lines are still being copied to the device, in
+ * blocks of pulse rows, by the caller (a pipelined upload; the drop-in entry
+ * does the same with its own copies).  The caller raises the device word
+ * *ready_word to ready_base + n once the first n * ready_rows pulse rows are
+ * in device memory (e.g. a 4-byte copy on its copy stream after each block;
+ * the word must only grow, and start below ready_base + 1).  The kernel starts
+ * at once and takes each chunk of pulses when its rows are in, waiting at
+ * most opts->spin_limit polls; if a wait gives up, the tiles not yet stored
+ * keep their old output and srg_sync_check() returns SRG_E_TIMEOUT.  Only the
+ * default split shape has such a twin (SRG_E_UNSUPPORTED otherwise).
+ * Asynchronous, as srg_bp_bursts_device.  No reference counterpart (the
+ * reference copies the whole burst before it launches, azimuth_compress.cu:
+ * 367-368). */
+int srg_bp_burst_device_gated(const srg_burst_desc *b, const int *ready_word, int ready_base,
+                              int ready_rows, const srg_bp_options *opts, void *stream);
 
 /* ------------------------------------------------------------------------
  * Scene plans: a reusable, graph-captured pass over a fixed set of
@@ -218,14 +275,21 @@ int srg_sync_check(void *stream);
  * (cudaGetSymbolAddress): make that first call before any stream capture.
  * Every call shares the array and clears only the counter and the error word;
  * calls whose GPU work overlaps (other streams, other host threads) race.
- * Blocking: returns once the work on `stream` has finished, with
- * SRG_E_TIMEOUT if a device-side wait gave up.
+ * opts->centres_on_host with b->coef NULL is SRG_E_UNSUPPORTED, as in
+ * srg_bp_bursts_device.  Blocking: the call copies its descriptors from host
+ * memory, waits for `stream` (cudaStreamSynchronize) and reads the error word
+ * back before it returns, with SRG_E_TIMEOUT if a device-side wait gave up.
  * ------------------------------------------------------------------------ */
 #define SRG_NOALLOC_MAX_LINES    8192
 #define SRG_NOALLOC_MAX_STATEVEC 64
 #define SRG_NOALLOC_SCRATCH_BYTES (2048 + 7 * 8 * SRG_NOALLOC_MAX_STATEVEC + 3 * 8 * SRG_NOALLOC_MAX_LINES)
 int srg_bp_burst_device_noalloc(const srg_burst_desc *b, const srg_bp_options *opts,
                                 void *stream);
+
+/* Testing hook: set the drop-in entry's call number on `device` (-1:
+ * current), 0 .. 2^24.  The number restarts at 1 after 2^24 calls; a test
+ * sets it near there to run calls across the restart. */
+int srg_test_set_dropin_sequence(int device, int seq);
 
 /* Calibration: measured FMA issue-rate peak of the current device in
  * TFLOP/s (2 flops per FMA), FP32 (fp64 = 0) or FP64 (fp64 = 1), from a

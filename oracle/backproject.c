@@ -242,6 +242,37 @@ int64_t srg_oracle_pixelint(const float *burst, const double *satloc,
     return terms;
 }
 
+/* Executed-term count of pixelint without the sum: the same aperture window
+ * (azimuth_compress_cpu.c:50-57) and range test (:63-64) per pixel and pulse. */
+int64_t srg_oracle_count_terms(const double *satloc, const double *xyz, const double *azoff,
+                               int demwidth, int aperture, int rawdatalines, double rngstart,
+                               double rngend, double dmrg, int nlines, int nthreads)
+{
+    const double rmax = rngend - dmrg;
+    const long total = (long)nlines * demwidth;
+    int64_t terms = 0;
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : terms)
+    for (long idx = 0; idx < total; ++idx) {
+        if (!(azoff[idx] > 0.)) continue;
+        int a0 = (int)round(azoff[idx] - aperture / 2);
+        int a1 = (int)round(azoff[idx] + aperture / 2);
+        if (a0 < 0) a0 = 0;
+        if (a1 > rawdatalines - 1) a1 = rawdatalines - 1;
+        const double *p = xyz + 3 * idx;
+        for (int az = a0; az < a1; ++az) {
+            const double vx = p[0] - satloc[3 * az + 0];
+            const double vy = p[1] - satloc[3 * az + 1];
+            const double vz = p[2] - satloc[3 * az + 2];
+            const double range = sqrt(vx * vx + vy * vy + vz * vz);
+            if (range >= rngstart && range <= rmax) ++terms;
+        }
+    }
+    return terms;
+}
+
 /* Merge rules. */
 static int merge_gpu(float re) { return fabs((double)re) > 1.e-18; }
 static int merge_cpu(float re)

@@ -56,6 +56,7 @@ class Oracle:
         L = self.lib
         L.srg_oracle_pixelint.restype = C.c_int64
         L.srg_oracle_burst.restype = C.c_int64
+        L.srg_oracle_count_terms.restype = C.c_int64
 
     # -- building blocks ------------------------------------------------
     def limits(self, b):
@@ -119,6 +120,33 @@ class Oracle:
             acc.ctypes.data_as(_dp) if acc is not None else None, C.byref(o))
         return out, acc, int(terms)
 
+    def pulse_orbit(self, times, b):
+        """Per-pulse positions and velocities ([P][3] each) by the window rule
+        of sentinel/sentineltimingsub.f90:55-63 (unclamped); raises if a pulse
+        time falls where the reference would read outside the vectors."""
+        t = _d(times)
+        P = t.shape[0]
+        pos, vel = np.zeros((P, 3)), np.zeros((P, 3))
+        to, xx, vv = _d(b.timeorbit), _d(b.xx), _d(b.vv)
+        bad = self.lib.srg_oracle_pulse_orbit(_ptr(t, _dp), C.c_int(P), _ptr(to, _dp),
+                                              _ptr(xx, _dp), _ptr(vv, _dp), C.c_int(len(to)),
+                                              _ptr(pos, _dp), _ptr(vel, _dp))
+        if bad:
+            raise ValueError(f"{bad} pulse times outside the state-vector window")
+        return pos, vel
+
+    def count_terms(self, b, nthreads=0):
+        """Executed-term count of one burst (limits, ECEF, azimuth centres,
+        azoff, then pixelint's window and range test without the sum)."""
+        fl, ll, fp, lp = self.limits(b)
+        nl = ll - fl + 1
+        xyz, fit = self.setxyz(b, fl, nl, fp, lp)
+        az = self.setazoff(b, self.line_coefs(b, fit), fp, lp)
+        return int(self.lib.srg_oracle_count_terms(
+            _ptr(_d(b.satloc), _dp), _ptr(xyz, _dp), _ptr(az, _dp), C.c_int(b.demwidth),
+            C.c_int(b.aperture), C.c_int(b.rawdatalines), C.c_double(b.rngstart),
+            C.c_double(b.rngend), C.c_double(b.dmrg), C.c_int(nl), C.c_int(nthreads)))
+
     # -- one burst --------------------------------------------------------
     def stages(self, b, gpu_lerp=1, gpu_scale=1, nthreads=0, want_acc=False):
         """Every intermediate of one burst: dict(firstline, nlines, firstpix,
@@ -181,17 +209,20 @@ def call_33(fn, b, fdout: int, fddem: int, burst=None):
        r(dbl["angc0"]), r(dbl["angc1"]), r(dbl["prf"]))
 
 
-def run_33_files(fn, b, geo_init=None, timing=None):
+def run_33_files(fn, b, geo_init=None, timing=None, tmpdir=None, read_back=True):
     """Run a 33-arg entry with a temporary DEM file and .geo file; return the
-    resulting [L][W] complex64 raster.  timing (dict, optional) receives the
-    wall time of the entry call alone as timing["call_s"]."""
-    with tempfile.TemporaryDirectory() as td:
+    resulting [L][W] complex64 raster (None without read_back).  timing
+    (dict, optional) receives the wall time of the entry call alone as
+    timing["call_s"]; tmpdir: where the files go (default: the temp dir)."""
+    with tempfile.TemporaryDirectory(dir=tmpdir) as td:
         dem_path = os.path.join(td, "elevation.dem")
         geo_path = os.path.join(td, "scene.geo")
         np.ascontiguousarray(b.dem, np.int16).tofile(dem_path)
-        g = (np.zeros((b.demlength, b.demwidth), np.complex64) if geo_init is None
-             else np.ascontiguousarray(geo_init, np.complex64))
-        g.tofile(geo_path)
+        if geo_init is None:
+            with open(geo_path, "wb") as f:   # a zero-filled raster
+                f.truncate(b.demlength * b.demwidth * 8)
+        else:
+            np.ascontiguousarray(geo_init, np.complex64).tofile(geo_path)
         fddem = os.open(dem_path, os.O_RDWR)
         fdout = os.open(geo_path, os.O_RDWR)
         try:
@@ -206,6 +237,8 @@ def run_33_files(fn, b, geo_init=None, timing=None):
         finally:
             os.close(fddem)
             os.close(fdout)
+        if not read_back:
+            return None
         return np.fromfile(geo_path, np.complex64).reshape(b.demlength, b.demwidth)
 
 

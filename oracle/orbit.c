@@ -137,3 +137,29 @@ void orbitrangetime_(const double *xyz, const double *timeorbit, const double *x
     *tline = t;
     *range = sqrt(dot3(dr, dr));
 }
+
+/* Per-pulse satellite position and velocity, sentinel/sentineltimingsub.f90:
+ * timedelta = timeorbit(2) - timeorbit(1) (:41); for each line time,
+ * ilocation = (time - timeorbit(1)) / timedelta assigned to an integer
+ * (truncation toward zero, :61), then orbithermite over the four vectors that
+ * start at 1-based ilocation - 1 (:62), with no clamp.  pos, vel: [P][3].
+ * Where the window would leave the vector array (the reference reads outside
+ * it there) the pulse is left unset; returns how many such pulses there were. */
+int srg_oracle_pulse_orbit(const double *times, int P, const double *timeorbit,
+                           const double *xx, const double *vv, int numstatevec,
+                           double *pos, double *vel)
+{
+    const double timedelta = timeorbit[1] - timeorbit[0];
+    int outside = 0;
+    for (int k = 0; k < P; ++k) {
+        const double time = times[k];
+        const int ilocation = (int)((time - timeorbit[0]) / timedelta);
+        const int s = ilocation - 2; /* 0-based index of 1-based ilocation - 1 */
+        if (s < 0 || s + 3 > numstatevec - 1) {
+            ++outside;
+            continue;
+        }
+        orbithermite_(xx + 3 * s, vv + 3 * s, timeorbit + s, &time, pos + 3 * k, vel + 3 * k);
+    }
+    return outside;
+}

@@ -26,6 +26,13 @@ void orbitrangetime_(const double *xyz, const double *timeorbit, const double *x
                      const double *satx0, const double *satv0, double *tline,
                      double *range);
 
+/* Per-pulse orbit of sentinel/sentineltimingsub.f90:41,55-63 (unclamped
+ * Hermite window).  Returns the number of pulses left unset because their
+ * window would leave the state-vector array. */
+int srg_oracle_pulse_orbit(const double *times, int P, const double *timeorbit,
+                           const double *xx, const double *vv, int numstatevec,
+                           double *pos, double *vel);
+
 /* ---- backprojection (oracle/backproject.c) ---- */
 
 /* Arithmetic variant of the per-pixel sum.
@@ -81,6 +88,12 @@ int64_t srg_oracle_pixelint(const float *burst, const double *satloc,
                             int samples, double rngstart, double rngend,
                             double dmrg, double wvl, int nlines, float *out,
                             double *acc, const srg_oracle_opts *opts);
+
+/* Executed-term count of srg_oracle_pixelint on the same inputs (its window
+ * and range test, no sum). */
+int64_t srg_oracle_count_terms(const double *satloc, const double *xyz, const double *azoff,
+                               int demwidth, int aperture, int rawdatalines, double rngstart,
+                               double rngend, double dmrg, int nlines, int nthreads);
 
 /* One whole burst in memory.  dem: the full [demlength][W] int16 DEM;
  * geo: the full [demlength][W] complex64 raster, merged in place with the

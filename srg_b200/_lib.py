@@ -31,7 +31,8 @@ _ip = C.POINTER(C.c_int)
 
 class Options(C.Structure):
     _fields_ = [("form", C.c_int), ("tile_cfg", C.c_int), ("device", C.c_int),
-                ("centres_on_host", C.c_int), ("verbose", C.c_int)]
+                ("centres_on_host", C.c_int), ("verbose", C.c_int), ("spin_limit", C.c_int),
+                ("scratch_limit", C.c_longlong)]
 
 
 class BurstDesc(C.Structure):
@@ -50,6 +51,13 @@ class BurstDesc(C.Structure):
         ("tmid", C.c_double), ("xyz_mid", C.c_double * 3), ("vel_mid", C.c_double * 3),
         ("angc0", C.c_double), ("angc1", C.c_double), ("prf", C.c_double),
     ]
+
+
+class BurstParams(C.Structure):
+    _fields_ = [(k, C.c_double) for k in (
+        "starttime", "prf", "samplefreq", "pri", "range0", "wvl", "angc0", "angc1", "tstart",
+        "tend", "tmid", "dtaz", "rngstart", "rngend", "dmrg")] + [("aperture", C.c_int),
+                                                                 ("pad", C.c_int)]
 
 
 class SrgError(RuntimeError):
@@ -72,6 +80,11 @@ _SIGS = {
     "srg_pulse_orbit_device": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp, C.c_int, C.c_void_p,
                                          C.c_void_p, C.c_void_p]),
     "srg_sync_check": (C.c_int, [C.c_void_p]),
+    "srg_bp_burst_device_gated": (C.c_int, [C.POINTER(BurstDesc), C.c_void_p, C.c_int, C.c_int,
+                                            C.POINTER(Options), C.c_void_p]),
+    "srg_test_set_dropin_sequence": (C.c_int, [C.c_int, C.c_int]),
+    "srg_burst_params": (C.c_int, [C.c_void_p, C.c_longlong, C.c_int, C.c_int, _dp,
+                                   C.POINTER(BurstParams)]),
     "srg_measure_fma_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
     "srg_bp_burst_device_noalloc": (C.c_int, [C.POINTER(BurstDesc), C.POINTER(Options), C.c_void_p]),
     "srg_scene_create": (C.c_int, [C.POINTER(BurstDesc), C.c_int, C.c_void_p, C.c_int64, C.c_int,

@@ -77,14 +77,18 @@ def prepare_azimuth_compress(b: Burst, fdout: int, fddem: int, burst: Optional[n
 
 
 def azimuth_compress_status(b: Burst, fdout: int, fddem: int, form: int = FORM_SPLIT,
-                            tile_cfg: int = -1, burst: Optional[np.ndarray] = None) -> int:
-    """The status-returning twin of the drop-in entry (raises on error)."""
+                            tile_cfg: int = -1, burst: Optional[np.ndarray] = None,
+                            **options) -> int:
+    """The status-returning twin of the drop-in entry (raises on error);
+    `options`: further srg_bp_options fields (spin_limit, scratch_limit, ...)."""
     L = lib()
     burst = np.ascontiguousarray(b.burst if burst is None else burst, np.complex64)
     keep = {k: _d(getattr(b, k)) for k in
             ("satloc", "latlons", "timeorbit", "xx", "vv", "xyz_mid", "vel_mid")}
     p = lambda a: a.ctypes.data_as(_dp)  # noqa: E731
     o = default_options(form, tile_cfg)
+    for k, v in options.items():
+        setattr(o, k, v)
     rc = L.srg_azimuth_compress(
         burst.ctypes.data_as(_fp), p(keep["satloc"]), b.rawdatalines, b.samples, b.demwidth,
         b.demlength, fdout, fddem, b.deltalat, b.deltalon, b.firstlat, b.firstlon,
@@ -93,6 +97,20 @@ def azimuth_compress_status(b: Burst, fdout: int, fddem: int, form: int = FORM_S
         b.aperture, b.angc0, b.angc1, b.prf, C.byref(o))
     check(rc)
     return rc
+
+
+def burst_params(lines: np.ndarray, satvel: np.ndarray) -> dict:
+    """Per-burst scalars of the azimuth_compress_ call (srg_burst_params:
+    burstparams, fdopcoefs, aperture and limits of
+    sentinel/backprojectgpusub.f90) from decoded lines whose first 10 samples
+    still hold the line headers ([P][S] complex64, host) and the per-pulse
+    velocities ([P][3])."""
+    lines = np.ascontiguousarray(lines, np.complex64)
+    sv = _d(satvel)
+    r = _lib.BurstParams()
+    check(lib().srg_burst_params(C.c_void_p(lines.ctypes.data), lines.shape[1], lines.shape[0],
+                                 lines.shape[1], sv.ctypes.data_as(_dp), C.byref(r)))
+    return {k: getattr(r, k) for k, _ in r._fields_ if k != "pad"}
 
 
 def set_default_form(form: int, tile_cfg: int = -1) -> None:

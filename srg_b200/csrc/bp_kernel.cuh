@@ -378,7 +378,7 @@ bp_tiles(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                 }
                 __syncthreads();
             } else {
-                const bool ok = mbar_wait_bounded(&ctl.bar, phase);
+                const bool ok = mbar_wait_bounded(&ctl.bar, phase, B.spin);
                 if (__syncthreads_or(!ok)) {
                     // give up on this launch: record, let the copy drain, leave
                     if (tid == 0) atomicOr(err, ERR_TMA_TIMEOUT);

@@ -74,6 +74,7 @@ struct CtlWS {
     uint64_t full[4], empty[4];
     int item, kmin, kmax, azs_max, aze_min, bmin, bmax, abort;
     int dmax_bits;        // max |d| over formed pixels (non-negative float bits)
+    unsigned spin;        // poll limit of the bounded waits
     double xc[3];
     double rc0, rc1;
     double ua[3], ub[3];  // unit look vectors at kmin and kmax-1
@@ -216,6 +217,7 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
         }
         fence_barrier_init();
         ctl.abort = 0;
+        ctl.spin = bursts[0].spin;
         // Later items are claimed by the producer once it has issued a tile's
         // last chunk, so the atomic's latency hides behind the consumers' last
         // chunks (claiming a whole tile ahead would unbalance the tail).
@@ -599,7 +601,7 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                         __int_as_float(__reduce_max_sync(0xffffffffu, __float_as_int(act ? err : 0.f)));
                     hv.poly = (nk >= 3 && (double)resmax * kTwoPi * B.K < kPolyTolRad) ? 1 : 0;
                 }
-                if (!mbar_wait_bounded(&ctl.empty[s], (r & 1) ^ 1)) {
+                if (!mbar_wait_bounded(&ctl.empty[s], (r & 1) ^ 1, ctl.spin)) {
                     ctl.abort = 1;
                     break;
                 }
@@ -608,11 +610,14 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                 if (GATE && ready) {
                     const int target = ready_base + (min(k0 + CK, Pm1 + 1) + ready_rows - 1) / ready_rows;
                     if (ready_seen < target) {
-                        if (!wait_word_at_least(ready, target)) {
+                        if (!wait_word_at_least(ready, target, ctl.spin)) {
                             if (lane == 0) atomicOr(err, ERR_UPLOAD_TIMEOUT);
                             ctl.abort = 1;
                             break;
                         }
+                        // the rows were seen through a generic-proxy acquire;
+                        // order the TMA (async-proxy) reads of them after it
+                        if (lane == 0) fence_proxy_async_global();
                         ready_seen = target;
                     }
                 }
@@ -662,7 +667,7 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                 const uint32_t g = gchunk + c;
                 const int s = g % NS;
                 const uint32_t r = g / NS;
-                if (!mbar_wait_bounded(&ctl.full[s], r & 1)) {
+                if (!mbar_wait_bounded(&ctl.full[s], r & 1, ctl.spin)) {
                     ctl.abort = 1;
                     break;
                 }
@@ -958,7 +963,8 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
         __syncthreads();
         if (ctl.abort) {
             if (tid == 0) atomicOr(err, ERR_TMA_TIMEOUT);
-            // let the copies this CTA issued drain before it leaves (bounded)
+            // let the copies this CTA issued drain before it leaves (bounded by
+            // the default limit whatever the launch's: a copy in flight ends in us)
             if (producer && lane == 0) {
                 for (int s = 0; s < NS; ++s)
                     if (issued & (1u << s)) mbar_wait_bounded(&ctl.full[s], (issued_par >> s) & 1u);

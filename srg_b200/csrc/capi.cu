@@ -59,7 +59,7 @@ int fail(int code, const char *fmt, ...) {
             return fail(SRG_E_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));   \
     } while (0)
 
-srg_bp_options g_default_opts = {SRG_FORM_SPLIT, -1, -1, 0, 0};
+srg_bp_options g_default_opts = {SRG_FORM_SPLIT, -1, -1, 0, 0, 0, 0};
 std::mutex g_opts_mu;
 
 DevCtx g_ctx[64];
@@ -151,6 +151,12 @@ void ref_limits(const double *latlons, double firstlat, double deltalat, double 
 
 double ref_pi() { return 4.0 * atan2(1.0, 1.0); }
 
+bool all_finite(const double *v, size_t n) {
+    for (size_t i = 0; i < n; ++i)
+        if (!std::isfinite(v[i])) return false;
+    return true;
+}
+
 int validate_desc(const srg_burst_desc &d) {
     if (!d.burst || !d.satloc || !d.dem || !d.out)
         return fail(SRG_E_ARG, "null device pointer in burst descriptor");
@@ -191,6 +197,7 @@ BurstDev make_burst_dev(const srg_burst_desc &d, const double *coef) {
     B.aperture = d.aperture;
     B.ap2 = d.aperture / 2;
     B.tmap = -1;
+    B.spin = kSpinLimit;
     const double pi = ref_pi();
     B.firstlat = d.firstlat;
     B.deltalat = d.deltalat;
@@ -256,10 +263,21 @@ int centres_device(DevCtx &c, const srg_burst_desc &d, const BurstDev &B, double
 }
 
 void ensure_attrs(DevCtx &c, int idx) {
+    std::lock_guard<std::mutex> g(c.attrs_mu);
     if (c.attrs_done[idx]) return;
     const KernelEntry &e = kKernels[idx];
     cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, shared_bytes(e));
     c.attrs_done[idx] = true;
+}
+
+int ensure_gated_attrs(DevCtx &c, const KernelEntry &twin) {
+    std::lock_guard<std::mutex> g(c.attrs_mu);
+    const int i = (int)(&twin - kGatedKernels);
+    if (c.gated_attrs_done[i]) return SRG_OK;
+    CK(cudaFuncSetAttribute(twin.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            shared_bytes(twin)));
+    c.gated_attrs_done[i] = true;
+    return SRG_OK;
 }
 
 int kernel_index(const KernelEntry *e) { return (int)(e - kKernels); }
@@ -361,6 +379,7 @@ int run_bursts(DevCtx &c, const srg_burst_desc *descs, int n, const srg_bp_optio
             coef = dst;
         }
         BurstDev B = make_burst_dev(d, coef);
+        if (o.spin_limit > 0) B.spin = (unsigned)o.spin_limit;
         const int nx = B.lastpix_eff - B.firstpix + 1;
         B.tiles_x = nx > 0 ? (nx + TX - 1) / TX : 0;
         B.tiles_y = (B.nlines + TY - 1) / TY;
@@ -392,11 +411,7 @@ int run_bursts(DevCtx &c, const srg_burst_desc *descs, int n, const srg_bp_optio
     CK(cudaMemsetAsync(c.flags.p, 0, sizeof(int), st));  // work counter only
     const int idx = kernel_index(ke);
     ensure_attrs(c, idx);
-    if (gated && !c.gated_attrs_done[twin - kGatedKernels]) {
-        CK(cudaFuncSetAttribute(twin->fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                shared_bytes(*twin)));
-        c.gated_attrs_done[twin - kGatedKernels] = true;
-    }
+    if (gated && (rc = ensure_gated_attrs(c, *twin))) return rc;
     const KernelEntry &run = gated ? *twin : *ke;
     const int smem = shared_bytes(run);
     int per_sm = 0;
@@ -444,6 +459,8 @@ void srg_bp_default_options(srg_bp_options *o) {
     o->device = -1;
     o->centres_on_host = 0;
     o->verbose = 0;
+    o->spin_limit = 0;
+    o->scratch_limit = 0;
 }
 
 const char *srg_last_error(void) { return g_err.c_str(); }
@@ -483,6 +500,40 @@ int srg_bp_bursts_device(const srg_burst_desc *bursts, int n, const srg_bp_optio
     if (rc) return rc;
     std::lock_guard<std::mutex> g(c->mu);
     return run_bursts(*c, bursts, n, o, static_cast<cudaStream_t>(stream));
+}
+
+int srg_bp_burst_device_gated(const srg_burst_desc *b, const int *ready_word, int ready_base,
+                              int ready_rows, const srg_bp_options *opts, void *stream) {
+    if (!b || !ready_word || ready_rows < 1 || ready_base < 0)
+        return fail(SRG_E_ARG, "bad arguments (ready_word %p, base %d, rows %d)",
+                    (const void *)ready_word, ready_base, ready_rows);
+    if ((long long)ready_base + (b->P + ready_rows - 1) / ready_rows > INT_MAX)
+        return fail(SRG_E_ARG, "ready_base %d leaves no room for the granule count", ready_base);
+    srg_bp_options o;
+    srg_bp_default_options(&o);
+    if (opts) o = *opts;
+    const KernelEntry *ke = pick_kernel(o.form, o.tile_cfg);
+    if (!ke) return fail(SRG_E_ARG, "no kernel for form %d shape %d", o.form, o.tile_cfg);
+    if (!gated_twin(*ke))
+        return fail(SRG_E_UNSUPPORTED, "kernel shape %s has no twin that waits for arriving lines",
+                    ke->name);
+    DevCtx *c = nullptr;
+    int rc = get_ctx(o.device, &c);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> g(c->mu);
+    UploadGate gate{ready_word, ready_base, ready_rows};
+    return run_bursts(*c, b, 1, o, static_cast<cudaStream_t>(stream), nullptr, &gate);
+}
+
+int srg_test_set_dropin_sequence(int device, int seq) {
+    if (seq < 0 || seq > DevCtx::kSeqLimit)
+        return fail(SRG_E_ARG, "sequence %d outside [0, %d]", seq, DevCtx::kSeqLimit);
+    DevCtx *c = nullptr;
+    int rc = get_ctx(device, &c);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> g(c->mu);
+    c->upload_seq = seq;
+    return SRG_OK;
 }
 
 int srg_sync_check(void *stream) {
@@ -644,6 +695,21 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
         numstatevec < 4 || !(dmrg > 0) || !(wvl > 0) || aperture < 0)
         return fail(SRG_E_ARG, "bad sizes or scalars (P=%d S=%d W=%d L=%d n=%d)", rawdatalines,
                     samplesPerBurst, demwidth, demlength, numstatevec);
+    // Non-finite geometry would leave every pixel unformed without a word
+    // (NaN fails every range and window test): refuse it before any work.
+    {
+        const double sc[] = {deltalat, deltalon, firstlat, firstlon, rngstart, rngend, tmid,
+                             dmrg, wvl, angc0, angc1, prf};
+        const char *bad = !all_finite(sc, sizeof sc / sizeof sc[0]) ? "a scalar argument"
+                          : !all_finite(latlons, 4)                 ? "latlons"
+                          : !all_finite(xyz_mid, 3) || !all_finite(vel_mid, 3) ? "xyz_mid / vel_mid"
+                          : !all_finite(timeorbit, numstatevec)     ? "timeorbit"
+                          : !all_finite(xx, 3 * (size_t)numstatevec) ? "xx"
+                          : !all_finite(vv, 3 * (size_t)numstatevec) ? "vv"
+                          : !all_finite(satloc, 3 * (size_t)rawdatalines) ? "satloc"
+                                                                    : nullptr;
+        if (bad) return fail(SRG_E_ARG, "non-finite value in %s", bad);
+    }
     srg_bp_options o;
     if (opts) o = *opts;
     else {
@@ -655,15 +721,11 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
                &lp_);
     const int nl = ll - fl + 1;
     if (o.verbose) printf("Burst line limits, size (first,last,nlines) %d %d %d\n", fl, ll, nl);
+    if (nl < 1)
+        return fail(SRG_E_ARG, "latlons select no grid line (first line %d, last line %d)", fl, ll);
     const int W = demwidth;
     const int fp = fp_, lp = lp_;
 
-    DevCtx *c = nullptr;
-    int rc = get_ctx(o.device, &c);
-    if (rc) return rc;
-    std::lock_guard<std::mutex> g(c->mu);
-    if ((rc = ensure_dropin(*c))) return rc;
-    cudaStream_t st = c->s_main;
     const int fp_eff = std::max(fp, 0);
     const int lp_eff = std::min(lp, W - 1);
     const int ncols = lp_eff >= fp_eff ? lp_eff - fp_eff + 1 : 0;
@@ -671,6 +733,27 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     // pinned staging: the DEM box in, the output box back
     const size_t dem_bytes = (size_t)nl * ncols * 2;
     const size_t win_bytes = (size_t)nl * ncols * 8;
+    if (o.scratch_limit > 0) {
+        // device scratch of this call: range lines, orbit, DEM box, output box,
+        // parabolas, work list (for the smallest tiles of any shape) and descriptors
+        const KernelEntry *kc = pick_kernel(o.form, o.tile_cfg);
+        const int tx = kc ? kc->shape.tx : 32, ty = kc ? kc->shape.ty : 4;
+        const long long tiles = (long long)((ncols + tx - 1) / tx) * ((nl + ty - 1) / ty);
+        const long long need = (long long)rawdatalines * samplesPerBurst * 8 +
+                               24LL * rawdatalines + (long long)dem_bytes + (long long)win_bytes +
+                               24LL * nl + 56LL * numstatevec +
+                               (long long)tile_list_bytes((int)std::min<long long>(tiles, INT_MAX)) +
+                               4096;
+        if (need > o.scratch_limit)
+            return fail(SRG_E_NOMEM, "the call needs %lld bytes of device scratch, the limit is %lld",
+                        need, (long long)o.scratch_limit);
+    }
+    DevCtx *c = nullptr;
+    int rc = get_ctx(o.device, &c);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> g(c->mu);
+    if ((rc = ensure_dropin(*c))) return rc;
+    cudaStream_t st = c->s_main;
     const size_t stage_bytes = std::max(dem_bytes, win_bytes) + 64;
     if (stage_bytes > c->host_cap) {
         if (c->host_stage) cudaFreeHost(c->host_stage);
@@ -688,6 +771,21 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
         (rc = c->flags.ensure(64)))
         return rc;
     HostPool &pool = HostPool::get();
+    // Once the first copy is queued, a failure waits for the three streams
+    // before it returns: queued copies may still read the caller's buffers.
+    auto drain = [&] {
+        cudaStreamSynchronize(c->s_copy);
+        cudaStreamSynchronize(c->s_back);
+        cudaStreamSynchronize(st);
+    };
+#define CKD(call)                                                                      \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess) {                                                       \
+            drain();                                                                   \
+            return fail(SRG_E_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));   \
+        }                                                                              \
+    } while (0)
     // The range lines upload on their own stream in blocks of pulse rows; after
     // each block the copy stream raises a device word, and the backprojection,
     // launched without waiting for the whole upload, takes a chunk of pulses as
@@ -695,15 +793,25 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     // (which need no range lines) proceed meanwhile.  The word counts granules
     // of P/32 pulse rows; the blocks shrink toward the end (6, 6, 5, 5, 4, 3,
     // 2, 1 granules), so that little of the sum waits for the last one.  The
-    // word only grows (call number x 64 + granules), so a value left by an
-    // earlier call never satisfies a later one.
+    // word grows from call to call (call number x 64 + granules), so a value
+    // left by an earlier call never satisfies a later one; the row blocks'
+    // done words hold the call number.  When the call number restarts, both
+    // are cleared first (every earlier call has finished its GPU work: each
+    // call waits for its three streams before it returns).
     int *ready_word = static_cast<int *>(c->flags.p) + DevCtx::kReadyWord;
     constexpr int kGranules = 32;
     static const int kBlockEnd[DevCtx::kUploadBlocks] = {6, 12, 17, 22, 26, 29, 31, 32};
     const int nup = DevCtx::kUploadBlocks;
     const int up_rows = (rawdatalines + kGranules - 1) / kGranules;  // rows per granule
     const int ngran = (rawdatalines + up_rows - 1) / up_rows;
-    c->upload_seq = c->upload_seq >= (1 << 24) ? 1 : c->upload_seq + 1;
+    if (c->upload_seq >= DevCtx::kSeqLimit) {
+        CK(cudaMemsetAsync(ready_word, 0, sizeof(int), st));
+        CK(cudaMemsetAsync(static_cast<int *>(c->rb.p) + 3 * DevCtx::kRowBlocks, 0,
+                           DevCtx::kRowBlocks * sizeof(int), st));
+        CK(cudaStreamSynchronize(st));
+        c->upload_seq = 0;
+    }
+    ++c->upload_seq;
     const int ready_base = c->upload_seq * 64;
     const size_t row_bytes = (size_t)samplesPerBurst * 8;
     auto upload = [&](int kb, int ke) -> int {
@@ -754,13 +862,13 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     }
     CK(cudaMemcpyAsync(c->in_sat.p, satloc, 24 * (size_t)rawdatalines, cudaMemcpyHostToDevice, st));
     if ((rc = upload(0, pipelined ? 1 : nup))) {
-        cudaStreamSynchronize(c->s_copy);  // the caller's buffer stays in use until then
-        cudaStreamSynchronize(st);
+        drain();  // the caller's buffer stays in use until then
         return rc;
     }
-    if (!pipelined) CK(cudaEventRecord(c->ev_burst, c->s_copy));
+    if (!pipelined) CKD(cudaEventRecord(c->ev_burst, c->s_copy));
     // DEM box of rows [fl, fl + nl) (azimuth_compress.cu:399-408), read by the
-    // pool's threads; bytes past the end of the file read as 0
+    // pool's threads; a file that ends before the box does is an error (the
+    // reference would use whatever its buffer held)
     int16_t *slab = static_cast<int16_t *>(c->host_stage);
     std::atomic<int> io_err{0};
     const int ntask = std::max(1, std::min(nl, 4 * HostPool::threads()));
@@ -768,20 +876,25 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
         const size_t want = (size_t)ncols * 2;
         for (int r = (int)((long long)nl * t / ntask); r < (int)((long long)nl * (t + 1) / ntask); ++r) {
             char *dst = reinterpret_cast<char *>(slab + (size_t)r * ncols);
-            const ssize_t got = pread(fddem, dst, want, ((off_t)(fl + r) * W + fp_eff) * 2);
-            if (got < 0) {
-                io_err = 1;
-                return;
+            size_t done = 0;
+            while (done < want) {   // pread may return fewer bytes than asked
+                const ssize_t got = pread(fddem, dst + done, want - done,
+                                          ((off_t)(fl + r) * W + fp_eff) * 2 + (off_t)done);
+                if (got <= 0) {
+                    io_err = got < 0 ? 1 : 2;
+                    return;
+                }
+                done += (size_t)got;
             }
-            if ((size_t)got < want) std::memset(dst + got, 0, want - (size_t)got);
         }
     });
     if (io_err) {
-        cudaStreamSynchronize(c->s_copy);
-        cudaStreamSynchronize(st);
-        return fail(SRG_E_IO, "DEM read failed (fd %d)", fddem);
+        drain();
+        return fail(SRG_E_IO, io_err == 1 ? "DEM read failed (fd %d)"
+                                          : "DEM file (fd %d) ends before the burst's rows do",
+                    fddem);
     }
-    CK(cudaMemcpyAsync(c->in_dem.p, slab, dem_bytes, cudaMemcpyHostToDevice, st));
+    CKD(cudaMemcpyAsync(c->in_dem.p, slab, dem_bytes, cudaMemcpyHostToDevice, st));
 
     srg_burst_desc d{};
     d.burst = static_cast<const float *>(c->in_burst.p);
@@ -825,11 +938,11 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     d.prf = prf;
     // rows of the kept tiles (the band): rows outside it have no formed pixel
     int *band = static_cast<int *>(c->flags.p) + DevCtx::kBandWord;
-    CK(cudaMemsetAsync(band, 0x7f, sizeof(int), st));      // INT_MAX-like
-    CK(cudaMemsetAsync(band + 1, 0xff, sizeof(int), st));  // -1
+    CKD(cudaMemsetAsync(band, 0x7f, sizeof(int), st));      // INT_MAX-like
+    CKD(cudaMemsetAsync(band + 1, 0xff, sizeof(int), st));  // -1
     c->host_flags[DevCtx::kBandWord] = INT_MAX;  // an empty band unless the list reports one
     c->host_flags[DevCtx::kBandWord + 1] = -1;
-    CK(cudaEventRecord(c->ev_band, st));
+    CKD(cudaEventRecord(c->ev_band, st));
     rc = run_bursts(*c, &d, 1, o, st, pipelined ? nullptr : c->ev_burst, pipelined ? &gate : nullptr,
                     band, c->host_flags + DevCtx::kBandWord, c->ev_band);
     if (!rc && pipelined) {
@@ -838,8 +951,7 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
             rc = fail(SRG_E_CUDA, "event record failed");
     }
     if (rc) {
-        cudaStreamSynchronize(c->s_copy);
-        cudaStreamSynchronize(st);
+        drain();
         return rc;
     }
     // The done words' writes after the kernel, issued after every upload copy
@@ -856,9 +968,9 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     // Without row blocks its rows' copies back are queued behind the sum at
     // once, after the error word, in up to kOutBlocks blocks; the merge of a
     // block starts as soon as that block is back and the error word is clear.
-    CK(cudaEventSynchronize(c->ev_band));
-    CK(cudaMemcpyAsync(c->host_flags, c->flags.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
-    CK(cudaEventRecord(c->ev_flags, st));
+    CKD(cudaEventSynchronize(c->ev_band));
+    CKD(cudaMemcpyAsync(c->host_flags, c->flags.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CKD(cudaEventRecord(c->ev_flags, st));
     const int band_lo = std::max(0, c->host_flags[DevCtx::kBandWord]);
     const int band_hi = std::min(nl - 1, c->host_flags[DevCtx::kBandWord + 1]);
     const int nband = band_hi >= band_lo ? band_hi - band_lo + 1 : 0;
@@ -890,14 +1002,14 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
             if (k < nfall &&
                 svo.wait(c->s_back, reinterpret_cast<CUdeviceptr>(rbw + 3 * K + k),
                          (cuuint32_t)c->upload_seq, CU_STREAM_WAIT_VALUE_EQ) == CUDA_SUCCESS) {
-                CK(copy_back(r0, r1, c->s_back));
-                CK(cudaMemcpyAsync(c->host_rb + 2 * K + k, rbw + k, sizeof(int),
+                CKD(copy_back(r0, r1, c->s_back));
+                CKD(cudaMemcpyAsync(c->host_rb + 2 * K + k, rbw + k, sizeof(int),
                                    cudaMemcpyDeviceToHost, c->s_back));
-                CK(cudaEventRecord(c->ev_blk[nblk], c->s_back));
+                CKD(cudaEventRecord(c->ev_blk[nblk], c->s_back));
                 b.rb = k;
             } else {
-                CK(copy_back(r0, r1, st));
-                CK(cudaEventRecord(c->ev_blk[nblk], st));
+                CKD(copy_back(r0, r1, st));
+                CKD(cudaEventRecord(c->ev_blk[nblk], st));
             }
             ++nblk;
         }
@@ -908,8 +1020,8 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
             b.r0 = band_lo + (int)((long long)nband * k / n);
             b.r1 = band_lo + (int)((long long)nband * (k + 1) / n);
             b.rb = -1;
-            CK(copy_back(b.r0, b.r1, st));
-            CK(cudaEventRecord(c->ev_blk[k], st));
+            CKD(copy_back(b.r0, b.r1, st));
+            CKD(cudaEventRecord(c->ev_blk[k], st));
         }
     }
 
@@ -964,12 +1076,12 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
             }
         }
     });
-    CK(cudaStreamSynchronize(st));
+    CKD(cudaStreamSynchronize(st));
     // the upload may end after the last chunk that needed it: the caller's
     // buffer stays in use until then
-    CK(cudaStreamSynchronize(c->s_copy));
-    CK(cudaStreamSynchronize(c->s_back));
-    CK(cudaGetLastError());
+    CKD(cudaStreamSynchronize(c->s_copy));
+    CKD(cudaStreamSynchronize(c->s_back));
+    CKD(cudaGetLastError());
     if (c->host_flags[1]) {  // only row blocks whose every tile was stored were merged
         const int word = c->host_flags[1];
         cudaMemsetAsync(static_cast<int *>(c->flags.p) + 1, 0, sizeof(int), st);
@@ -980,6 +1092,7 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     if (io_err == 1) return fail(SRG_E_IO, "output read failed (fd %d)", fdout);
     if (io_err == 2) return fail(SRG_E_IO, "output write failed (fd %d)", fdout);
     return SRG_OK;
+#undef CKD
 }
 
 void azimuth_compress_(float *burstdata, double *satloc, int *rawdatalines, int *samplesPerBurst,

@@ -5,6 +5,10 @@
 
 namespace srg {
 
+// Default poll limit of the kernels' bounded waits (try_wait polls, each
+// suspending up to ~1 us; a launch may set another through BurstDev::spin).
+constexpr unsigned kSpinLimit = 1u << 22;
+
 // Error bits raised by kernels into the device error word.
 enum : int {
     ERR_TMA_TIMEOUT = 1,   // a bounded mbarrier wait for a TMA tile gave up
@@ -28,7 +32,7 @@ struct BurstDev {
     int aperture, ap2;        // ap2 = aperture / 2 (integer division, as the reference)
     int tiles_x, tiles_y, tile_base;
     int tmap;                 // index of this burst's TMA descriptor, -1 = none
-    int pad0;
+    unsigned spin;            // polls of a bounded device-side wait (the launch's first burst's)
     double firstlat, deltalat, firstlon, deltalon, deg2rad;
     double rngstart, rmax;    // rmax = rngend - dmrg (the reference's upper range test)
     double dmrg, k4pi;        // k4pi = 4*pi/wvl, grouped as the reference

@@ -73,11 +73,15 @@ struct DevCtx {
     static constexpr int kRowBlocks = kOutBlocks;
     DevBuf rb;
     int *host_rb = nullptr;
+    // drop-in call number on this device, 1 .. kSeqLimit (then it restarts)
+    static constexpr int kSeqLimit = 1 << 24;
     int upload_seq = 0;
     bool dropin_ready = false;
     cudaStream_t s_main = nullptr, s_copy = nullptr, s_back = nullptr;
     cudaEvent_t ev_burst = nullptr, ev_flags = nullptr, ev_band = nullptr, ev_blk[kOutBlocks] = {};
     int *host_flags = nullptr;
+    // kernel attributes set once per device (any entry, any host thread)
+    std::mutex attrs_mu;
     bool attrs_done[64] = {};
     bool gated_attrs_done[8] = {};
 };
@@ -100,6 +104,8 @@ BurstDev make_burst_dev(const srg_burst_desc &d, const double *coef);
 // 0 and *out filled when a TMA descriptor can describe the burst, else -1.
 int make_tmap(const BurstDev &B, int box_x, int box_y, CUtensorMap *out);
 double ref_pi();
+// Every one of the n values is finite.
+bool all_finite(const double *v, size_t n);
 
 }  // namespace detail
 }  // namespace srg

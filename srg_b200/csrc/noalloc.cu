@@ -76,6 +76,8 @@ extern "C" int srg_bp_burst_device_noalloc(const srg_burst_desc *b, const srg_bp
     srg_bp_options o;
     srg_bp_default_options(&o);
     if (opts) o = *opts;
+    if (o.centres_on_host && !b->coef)  // as srg_bp_bursts_device
+        return fail(SRG_E_UNSUPPORTED, "host centres need host DEM (use the file entry)");
     const KernelEntry *ke = pick_kernel(o.form, o.tile_cfg);
     if (!ke) return fail(SRG_E_ARG, "no kernel for form %d shape %d", o.form, o.tile_cfg);
     DevCtx *c = nullptr;
@@ -125,6 +127,7 @@ extern "C" int srg_bp_burst_device_noalloc(const srg_burst_desc *b, const srg_bp
         coef = d_coef;
     }
     BurstDev B = make_burst_dev(*b, coef);
+    if (o.spin_limit > 0) B.spin = (unsigned)o.spin_limit;
     const int nx = B.lastpix_eff - B.firstpix + 1;
     B.tiles_x = nx > 0 ? (nx + ke->shape.tx - 1) / ke->shape.tx : 0;
     B.tiles_y = (B.nlines + ke->shape.ty - 1) / ke->shape.ty;

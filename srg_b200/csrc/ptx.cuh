@@ -1,16 +1,16 @@
 // ptx.cuh -- mbarrier and TMA (cp.async.bulk.tensor) wrappers for sm_100a.
 //
-// Every wait is bounded: after kSpinLimit polls the caller gets `false`,
-// raises an error bit in device memory and abandons the work item instead of
-// spinning forever.  No cluster multicast is used anywhere: each CTA loads
+// Every wait is bounded: after a limit of polls (kSpinLimit unless the launch
+// sets another) the caller gets `false`, raises an error bit in device memory
+// and abandons the work item instead of spinning forever.  No cluster multicast is used anywhere: each CTA loads
 // its own tiles, and only from this GPU's memory.
 #pragma once
 #include <cstdint>
 #include <cuda.h>
+#include "common.cuh"
 
 namespace srg {
 
-constexpr uint32_t kSpinLimit = 1u << 22;  // try_wait polls (each suspends up to ~us)
 
 // Packed FP32 pairs (sm_100 f32x2 arithmetic): one instruction works on two
 // independent lanes held in a 64-bit register pair.
@@ -67,6 +67,12 @@ __device__ __forceinline__ void fence_proxy_async_shared() {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
+// Order this thread's earlier generic-proxy accesses of global memory (an
+// acquire that saw data arrive) before its later async-proxy (TMA) reads.
+__device__ __forceinline__ void fence_proxy_async_global() {
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
 // Raise the transaction count of the barrier's current phase by `bytes`
 // without an arrival (the caller's copy completes them).
 __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
@@ -91,9 +97,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait for phase `parity` of `bar`; false if the limit was reached.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
-    for (uint32_t i = 0; i < kSpinLimit; ++i)
+// Bounded wait for phase `parity` of `bar` (at most `limit` polls); false if
+// the limit was reached.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity,
+                                                  uint32_t limit = kSpinLimit) {
+    for (uint32_t i = 0; i < limit; ++i)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
@@ -102,11 +110,12 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
 // (a value a copy engine raises).  Lane 0 alone polls, with acquire semantics
 // and a 1 us pause between polls (hundreds of CTAs poll one word while the
 // copy engine writes the lines); the warp barrier orders the other lanes'
-// later accesses after its load.  false when the limit ran out.
-__device__ __forceinline__ bool wait_word_at_least(const int *word, int target) {
+// later accesses after its load.  false when `limit` / 4 polls ran out.
+__device__ __forceinline__ bool wait_word_at_least(const int *word, int target,
+                                                   uint32_t limit = kSpinLimit) {
     int ok = 0;
     if ((threadIdx.x & 31) == 0) {
-        for (uint32_t i = 0; i < kSpinLimit / 4; ++i) {
+        for (uint32_t i = 0; i < limit / 4 + 1; ++i) {
             int v;
             asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(word) : "memory");
             if (v >= target) {

@@ -232,6 +232,7 @@ int srg_scene_create(const srg_burst_desc *bursts, int n, float *scene, int64_t 
         J.coef = s->d_coef + 3 * lo;
         J.line_base = (int)lo;
         s->hb[i] = make_burst_dev(d, J.coef);
+        if (o.spin_limit > 0) s->hb[i].spin = (unsigned)o.spin_limit;
         lo += (size_t)d.nlines;
         oo += 7 * (size_t)k;
     }

@@ -631,6 +631,70 @@ def mini_fixture(seed: int, pulses: int = 320, samples: int = 384, width: int = 
     return b
 
 
+def host_clutter_samples(b: Burst, seed: int, ntargets: int = 200, target_db: float = 30.0,
+                         samples: Optional[int] = None) -> None:
+    """Fill b.burst on the host with circular complex Gaussian clutter (unit
+    power per sample) plus `ntargets` point targets at +`target_db` on random
+    grid pixels of the burst's pixel window (``add_point_targets``): the
+    statistics of the device workloads' range lines, drawn with numpy so that
+    CPU-only runs need neither a GPU nor the CUDA library.  `samples`
+    (default b.samples) sets the line length."""
+    rng = np.random.default_rng([seed, 7])
+    P = b.rawdatalines
+    S = b.samples if samples is None else samples
+    z = rng.standard_normal((P, S, 2), dtype=np.float32) * np.float32(math.sqrt(0.5))
+    b.burst = (z[..., 0] + 1j * z[..., 1]).astype(np.complex64)
+    del z
+    ll = int((b.latlons[0] - b.firstlat) / b.deltalat)
+    fl = int((b.latlons[1] - b.firstlat) / b.deltalat)
+    fl, ll = min(max(fl, 0), b.demlength - 1), min(max(ll, 0), b.demlength - 1)
+    fp = max(int((b.latlons[2] - b.firstlon) / b.deltalon), 0)
+    lp = min(int((b.latlons[3] - b.firstlon) / b.deltalon), b.demwidth - 1)
+    lines = rng.integers(fl, ll + 1, ntargets)
+    pix = rng.integers(fp, lp + 1, ntargets)
+    h = b.dem[lines, pix].astype(np.float64) if b.dem is not None else np.zeros(ntargets)
+    add_point_targets(b, grid_ecef(b, lines, pix, h), np.full(ntargets, 10.0 ** (target_db / 20.0)))
+
+
+# Sentinel-1 header fields the burst-parameter derivation reads (byte
+# offsets in a line's 80-byte header, sentinel/backprojectgpusub.f90:266-299,
+# 406-429): range decimation code (40), rank (49, low 5 bits), PRI code (50,
+# 24-bit big endian, in units of 1/fref us), SWST code (53, idem), azimuth
+# beam word (60, 16-bit big endian, address in the low 10 bits), line time
+# (68, native double).
+FREF_MHZ = 37.53472224
+
+
+def encode_line_headers(times, pri_code: int, rank: int, swst_code: int, decimation: int,
+                        beam_address) -> np.ndarray:
+    """[P][10] complex64 holding each line's 80-byte header with the given
+    fields (the other bytes zero): the first 10 samples of a decoded line."""
+    times = np.asarray(times, np.float64)
+    P = times.shape[0]
+    beam = np.broadcast_to(np.asarray(beam_address, np.int64), (P,))
+    h = np.zeros((P, 80), np.uint8)
+    h[:, 40] = decimation & 255
+    h[:, 49] = rank & 31
+    for off, v in ((50, pri_code), (53, swst_code)):
+        h[:, off] = (v >> 16) & 255
+        h[:, off + 1] = (v >> 8) & 255
+        h[:, off + 2] = v & 255
+    h[:, 60] = (beam >> 8) & 3
+    h[:, 61] = beam & 255
+    h[:, 68:76] = times.astype("<f8").view(np.uint8).reshape(P, 8)
+    return h.view(np.complex64).reshape(P, 10)
+
+
+def header_codes(prf: float, rngstart: float, rank: int = 9):
+    """PRI and SWST codes whose decoded PRF and near range come closest to
+    the given ones (the inverse of burstparams, up to the codes' rounding)."""
+    pri_us = 1e6 / prf
+    pri_code = int(round(pri_us * FREF_MHZ))
+    pri = pri_code / FREF_MHZ * 1e-6
+    swst = 2.0 * (rngstart - 60.0) / C_LIGHT - rank * pri
+    return pri_code, int(round(swst * 1e6 * FREF_MHZ))
+
+
 # Fields of a Burst that a fixture stores verbatim.
 ARRAY_FIELDS = ("satloc", "satvel", "pulse_time", "latlons", "timeorbit", "xx", "vv", "xyz_mid",
                 "vel_mid", "dem")

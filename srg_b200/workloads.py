@@ -150,6 +150,39 @@ def config3(device="cuda", seed: int = 1003, ntargets: int = 200, target_db: flo
     return wl
 
 
+def iw_bursts(indices=(0, 1, 2), device="cuda", seed: int = 1003, ntargets: int = 200,
+              target_db: float = 30.0):
+    """Selected bursts of the IW scene (configuration 3) on their own, for
+    checks at full size: the scene's geometry and shared volcano DEM, each
+    burst's range lines circular complex Gaussian clutter plus `ntargets`
+    forward-projected point targets at +30 dB (the scene's statistics; the
+    samples are drawn per burst, so they are not the ones config3 draws).
+    Indices 0, 1, 2 are the first burst of subswaths 1, 2, 3.  Returns
+    (SceneGrid with a host DEM, [DeviceBurst]); each burst's `b.dem` is the
+    host DEM and `b.burst` is left empty (the samples live on the device)."""
+    import torch
+    grid, bursts = scene.iw_scene(seed=seed, device=device)
+    dem_dev = grid.dem
+    host_dem = dem_dev.cpu().numpy()
+    amp = 10.0 ** (target_db / 20.0)
+    dbs = []
+    for i in indices:
+        b = bursts[i]
+        b.dem = host_dem
+        gen = torch.Generator(device=device)
+        gen.manual_seed(seed * 100 + i)
+        P, S = b.rawdatalines, b.samples
+        bt = torch.complex(torch.randn((P, S), generator=gen, device=device),
+                           torch.randn((P, S), generator=gen, device=device)) * (1.0 / np.sqrt(2.0))
+        db = api.to_device(b, device=device, burst_tensor=bt, dem_tensor=dem_dev, narrow_out=True)
+        refl = torch.zeros((db.nlines, grid.width), dtype=torch.complex64, device=device)
+        _add_targets(db, refl, np.random.default_rng(seed * 100 + i), ntargets, amp)
+        dbs.append(db)
+    torch.cuda.synchronize(device)
+    grid.dem = host_dem
+    return grid, dbs
+
+
 def config4(device="cuda", seed: int = 1004, acquisitions: int = 32, bperp_max: float = 150.0,
             along_max: float = 5.0, los_max: float = 0.10, depth: float = 3000.0,
             ntargets: int = 200, target_db: float = 30.0, form=None) -> Workload:

@@ -187,12 +187,19 @@ def test_batched_launch_equals_single(torch_cuda):
         assert np.array_equal(db.out.cpu().numpy().view(np.uint32), s.view(np.uint32))
 
 
-def test_pulse_orbit_kernel(torch_cuda):
+def test_pulse_orbit_kernel(torch_cuda, orc):
+    """Per-pulse orbit on the GPU against the oracle's restatement of
+    sentinel/sentineltimingsub.f90:41,55-63 (window from the truncated index,
+    unclamped, orbithermite.f): bit for bit; and against the orbit the
+    state vectors were sampled from."""
     torch = torch_cuda
     b = scene.make_geometry(pulses=1500, samples=64, width=8, length=8, spacing=1e-4,
                             quantise=False)
     t = torch.from_numpy(b.pulse_time).cuda()
     pos, vel = api.pulse_orbit(t, b)
+    opos, ovel = orc.pulse_orbit(b.pulse_time, b)
+    assert np.array_equal(pos.cpu().numpy(), opos)
+    assert np.array_equal(vel.cpu().numpy(), ovel)
     np.testing.assert_allclose(pos.cpu().numpy(), b.satloc, rtol=0, atol=1e-6)
     np.testing.assert_allclose(vel.cpu().numpy(), b.satvel, rtol=0, atol=1e-9)
 
@@ -285,3 +292,43 @@ def test_dropin_sequential_bursts_merge_like_the_oracle(torch_cuda, orc):
     assert np.array_equal(got != init, ref != init)
     assert (ref != init).sum() > 0
     assert rel_err(got, ref) < FP64_REL
+
+
+@pytest.mark.parametrize("form", [_lib.FORM_FP64, _lib.FORM_SPLIT])
+def test_dropin_with_burst_params_from_line_headers(torch_cuda, orc, form):
+    """The caller's side of the call, as backprojectgpusub.f90:140-247 makes
+    it: the burst's scalars (PRF, near range, sampling rate, wavelength,
+    steering fit angc0/angc1, aperture, limits) derived from the line headers
+    and velocities by srg_burst_params, the 10 header samples then zeroed
+    (:191), and the call made through azimuth_compress_; the same arguments
+    through the oracle's entry give the same .geo."""
+    b = mini_case("slope")
+    P = b.burst.shape[0]
+    pri_code, swst_code = scene.header_codes(b.prf, b.rngstart)
+    rng = np.random.default_rng(17)
+    addr = np.rint((np.linspace(-0.3, 0.3, P) + 0.9) / 1.8 * 1024).astype(np.int64)
+    addr += rng.integers(-2, 3, P)
+    lines = b.burst.copy()
+    lines[:, :10] = scene.encode_line_headers(b.pulse_time, pri_code, 9, swst_code, 8, addr)
+    p = api.burst_params(lines, b.satvel)
+    lines[:, :10] = 0
+    for k in ("prf", "angc0", "angc1", "rngstart", "rngend", "dmrg", "wvl", "tstart", "tend",
+              "tmid", "dtaz", "aperture"):
+        setattr(b, k, p[k])
+    b.burst = lines
+    init = (rng.standard_normal((b.demlength, b.demwidth)) +
+            1j * rng.standard_normal((b.demlength, b.demwidth))).astype(np.complex64)
+    ref = O.run_33_files(orc.lib.srg_oracle_azimuth_compress_, b, geo_init=init)
+    api.set_default_form(form)
+    try:
+        got = O.run_33_files(_lib.lib().azimuth_compress_, b, geo_init=init)
+    finally:
+        api.set_default_form(_lib.FORM_SPLIT)
+    changed = ref != init
+    assert changed.sum() > 1000
+    assert np.array_equal(got != init, changed)
+    if form == _lib.FORM_FP64:
+        assert rel_err(got, ref) < FP64_REL
+    else:
+        e = phase_amp_errors(got[changed], ref[changed])
+        assert e["ph_rms"] < SPLIT_PH_RMS_MRAD, e

@@ -57,3 +57,62 @@ def test_errors_are_reported_without_gpu_work():
     rc = L.srg_bp_bursts_device(None, 0, None, None)
     assert rc == _lib.SRG_E_ARG
     assert "no bursts" in _lib.last_error()
+
+
+def _dropin_files(tmp_path, b):
+    dem = tmp_path / "d.dem"
+    geo = tmp_path / "s.geo"
+    np.ascontiguousarray(b.dem, np.int16).tofile(dem)
+    init = np.full((b.demlength, b.demwidth), 3 + 4j, np.complex64)
+    init.tofile(geo)
+    return str(dem), str(geo), init
+
+
+@pytest.mark.parametrize("field,where", [("xx", "xx"), ("satloc", "satloc"), ("vv", "vv"),
+                                         ("rngend", "a scalar argument"), ("latlons", "latlons")])
+def test_dropin_refuses_non_finite_geometry_before_any_work(tmp_path, field, where):
+    """A NaN or infinity in the orbit, the pulse positions, the box or a
+    scalar would leave every pixel unformed without a word (NaN fails every
+    window and range test): the status entry refuses it before touching the
+    GPU or the files."""
+    b = scene.mini_fixture(seed=11)
+    v = getattr(b, field)
+    if isinstance(v, np.ndarray):
+        v = v.copy()
+        v.flat[v.size // 2] = np.nan
+    else:
+        v = float("inf")
+    setattr(b, field, v)
+    dem, geo, init = _dropin_files(tmp_path, b)
+    fd_dem, fd_geo = os.open(dem, os.O_RDONLY), os.open(geo, os.O_RDWR)
+    try:
+        with pytest.raises(_lib.SrgError) as e:
+            api.azimuth_compress_status(b, fd_geo, fd_dem)
+    finally:
+        os.close(fd_dem)
+        os.close(fd_geo)
+    assert e.value.code == _lib.SRG_E_ARG
+    assert f"non-finite value in {where}" in str(e.value)
+    assert np.array_equal(np.fromfile(geo, np.complex64).reshape(init.shape), init)
+
+
+def test_dropin_refuses_an_empty_box_and_a_scratch_limit(tmp_path):
+    """latlons whose minimum latitude lies north of their maximum select no
+    grid line (SRG_E_ARG); a scratch limit below the call's device scratch is
+    SRG_E_NOMEM.  Both before any GPU work, the .geo untouched."""
+    b = scene.mini_fixture(seed=11)
+    dem, geo, init = _dropin_files(tmp_path, b)
+    fd_dem, fd_geo = os.open(dem, os.O_RDONLY), os.open(geo, os.O_RDWR)
+    try:
+        inv = scene.mini_fixture(seed=11)
+        inv.latlons = inv.latlons[[1, 0, 2, 3]].copy()
+        with pytest.raises(_lib.SrgError) as e:
+            api.azimuth_compress_status(inv, fd_geo, fd_dem)
+        assert e.value.code == _lib.SRG_E_ARG and "no grid line" in str(e.value)
+        with pytest.raises(_lib.SrgError) as e:
+            api.azimuth_compress_status(b, fd_geo, fd_dem, scratch_limit=1 << 16)
+        assert e.value.code == _lib.SRG_E_NOMEM and "limit" in str(e.value)
+    finally:
+        os.close(fd_dem)
+        os.close(fd_geo)
+    assert np.array_equal(np.fromfile(geo, np.complex64).reshape(init.shape), init)
