@@ -120,19 +120,23 @@ def load_traffic(kernel: str, workload: str):
 # our arm
 
 
-def e2e_dropin(torch, wl, steps, form, separate=False):
+def e2e_dropin(torch, wl, steps, form, separate=False, bursts=None):
     """End to end through azimuth_compress_ (the drop-in C ABI), one call per
     burst in acquisition order as the reference's driver makes them: burst
     lines in pinned host memory, the DEM and the .geo raster as files on tmpfs
     (when it has room, else the temp dir); `separate`: one .geo file per burst
-    (a stack of passes) instead of one scene raster.  Returns (s per step,
-    h2d, d2h bytes per step)."""
+    (a stack of passes) instead of one scene raster; `bursts`: the bursts to
+    run (default: all of the workload's).  Returns (s per step, h2d, d2h bytes
+    per step)."""
     from srg_b200 import api
     api.set_default_form(form)
-    b0 = wl.bursts[0].b
+    bursts = wl.bursts if bursts is None else bursts
+    if not bursts:
+        return 0.0, 0, 0
+    b0 = bursts[0].b
     geo_bytes = b0.demlength * b0.demwidth * 8
     dem_bytes = b0.demlength * b0.demwidth * 2
-    nfiles = len(wl.bursts) if separate else 1
+    nfiles = len(bursts) if separate else 1
     tmp = None
     if os.path.isdir("/dev/shm"):
         st = os.statvfs("/dev/shm")
@@ -152,20 +156,18 @@ def e2e_dropin(torch, wl, steps, form, separate=False):
         fd_of = (lambda i: fds[i]) if separate else (lambda i: fds[0])
         hosts = []
         try:
-            for db in wl.bursts:
+            for db in bursts:
                 host = torch.empty(tuple(db.burst.shape), dtype=torch.complex64, pin_memory=True)
                 host.copy_(db.burst)
                 hosts.append(host)
-                fl, ll, fp, lp = api.limits(db.b)
-                nl = ll - fl + 1
-                ncols = max(0, min(lp, db.b.demwidth - 1) - fp + 1)
-                h2d += host.numel() * 8 + db.b.rawdatalines * 24 + nl * ncols * 2
-                d2h += nl * ncols * 8
             # each call's arguments built once, as a Fortran caller holds them
             calls = [api.prepare_azimuth_compress(db.b, fd_of(i), fd_dem, burst=host.numpy())
-                     for i, (db, host) in enumerate(zip(wl.bursts, hosts))]
-            for call in calls:   # warm-up
+                     for i, (db, host) in enumerate(zip(bursts, hosts))]
+            for call in calls:   # warm-up; the bytes each call copies, as it reports them
                 call()
+                h, d = api.dropin_last_bytes()
+                h2d += h
+                d2h += d
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             for _ in range(steps):
@@ -524,11 +526,24 @@ def main():
 
     build = {"c1": workloads.config1, "c2": workloads.config1, "c3": workloads.config3,
              "c4": workloads.config4}[args.workload]
+    # N > 1, the IW scene: one scene partitioned over the ranks (every rank
+    # builds the same scene); other workloads: one replica per rank
+    partitioned = world > 1 and args.workload == "c3"
     wl = build(device=f"cuda:{local}",
-               seed={"c1": 1001, "c2": 1001, "c3": 1003, "c4": 1004}[args.workload] + rank)
+               seed={"c1": 1001, "c2": 1001, "c3": 1003, "c4": 1004}[args.workload] +
+               (0 if partitioned else rank))
+    if partitioned:
+        from srg_b200 import api, partition
+        weights = [api.count_terms([db]) for db in wl.bursts]
+        wl.plan.close()   # the one-rank plan gives way to this rank's share
+        wl.plan = partition.PartitionedScene(wl.bursts, wl.raster, rank, world, dist, weights,
+                                             _lib.FORM_SPLIT)
+        own_bursts, terms_rank = wl.plan.mine, int(wl.plan.own_weight())
 
     stream = torch.cuda.Stream()
     c2 = oversampled_lines(torch, wl, stream) if args.workload == "c2" else None
+    if not partitioned:
+        own_bursts, terms_rank = wl.bursts, wl.terms
     fp32_peak = _lib.measure_fma_peak(False)
     fp64_peak = _lib.measure_fma_peak(True)
     tuned = {}
@@ -562,7 +577,7 @@ def main():
     d_ms = time_plan(torch, plan, max(3, args.steps // 3), 1, stream)
     d_kern = d_ms
     if wl.raster is not None:
-        perr = raster_phase_error(torch, split_out, wl.raster)
+        perr = raster_phase_error(torch, split_out, wl.raster) if rank == 0 else None
     else:
         fp64_out = torch.stack([db.out for db in wl.bursts])
         perr = raster_phase_error(torch, split_out, fp64_out)
@@ -575,18 +590,20 @@ def main():
     # azimuth centres, work-list mask and compaction, backprojection (and the
     # ordered merge): one graph per pass
     launches = 5 if wl.raster is not None else 4
+    if partitioned:   # own plan (4) and, on rank 0, one merge per burst
+        launches = (4 if own_bursts else 0) + (len(wl.bursts) if rank == 0 else 0)
     if c2 is not None:
         c2["vs_config1_fp64"] = vs_plain_lines(torch, wl, c2.pop("plain_fp64"))
     e2e_s, h2d, d2h = e2e_dropin(torch, wl, args.e2e_steps, _lib.FORM_SPLIT,
-                                 separate=args.workload == "c4")
+                                 separate=args.workload == "c4", bursts=own_bursts)
     h2d_gbs = pinned_h2d_gbs(torch)
     # whole job: the slowest rank's times, every rank's terms and bytes
     (s_ms, d_ms, e2e_s), (terms_all, h2d, d2h) = combine_ranks(
-        torch, dist if world > 1 else None, "cuda", [s_ms, d_ms, e2e_s], [wl.terms, h2d, d2h])
+        torch, dist if world > 1 else None, "cuda", [s_ms, d_ms, e2e_s], [terms_rank, h2d, d2h])
     terms_all, h2d, d2h = int(terms_all), int(h2d), int(d2h)
     value = terms_all / (s_ms * 1e-3) / 1e9
     fp64_value = terms_all / (d_ms * 1e-3) / 1e9
-    achieved = FLOPS_PER_TERM * wl.terms / (s_kern * 1e-3) / 1e12
+    achieved = FLOPS_PER_TERM * terms_rank / (s_kern * 1e-3) / 1e12
     traffic = load_traffic("bp_split", wl.name)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(
@@ -600,7 +617,8 @@ def main():
         return
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": s_ms, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": s_ms, "higher_is_better": True,
+        "scaling": "strong" if partitioned else "weak",
         "vs_baseline": None, "dtype": "f32 (split; FP64 orbit/ECEF/reference range)",
         "data": {"c3": "synthetic, seeded: complex Gaussian clutter + forward-projected point targets",
                  "c4": "synthetic, seeded: forward-projected scatterers + point targets, Mogi "
@@ -621,7 +639,7 @@ def main():
                      "traffic": traffic, "flops_per_term": FLOPS_PER_TERM,
                      "peak_source": "measured in-run: FFMA-chain kernel (srg_measure_fma_peak)",
                      "fp64_peak": fp64_peak,
-                     "fp64_form_frac_of_fp64_peak": FLOPS_PER_TERM * wl.terms / (d_kern * 1e-3) / 1e12 / fp64_peak,
+                     "fp64_form_frac_of_fp64_peak": FLOPS_PER_TERM * terms_rank / (d_kern * 1e-3) / 1e12 / fp64_peak,
                      "kernel_ms": s_kern},
         "cpu_baseline": cpu,
         "e2e": {"value": terms_all / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d,

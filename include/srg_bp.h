@@ -46,6 +46,8 @@ typedef struct srg_bp_options {
                           still uploading, or for a staged tile) before the
                           kernel gives up and the call returns SRG_E_TIMEOUT;
                           0: the default, 4,194,304 (about 1-2 s) */
+    int full_lines;    /* drop-in: 1 uploads every line in full; 0 (default)
+                          only its range band (srg_dropin_last_bytes) */
     long long scratch_limit; /* bytes of device scratch one drop-in call may
                           hold (range lines, orbit, DEM box, output box, work
                           list); a call needing more returns SRG_E_NOMEM before
@@ -53,7 +55,8 @@ typedef struct srg_bp_options {
 } srg_bp_options;
 
 /* Fill *o with the defaults (split form, tuned tile, current device,
- * centres on the GPU, quiet, default wait limit, no scratch limit). */
+ * centres on the GPU, quiet, default wait limit, range band, no scratch
+ * limit). */
 void srg_bp_default_options(srg_bp_options *o);
 
 /* Message of the last failing call on this thread ("" if none). */
@@ -103,6 +106,14 @@ int srg_azimuth_compress(
 
 /* Options used by azimuth_compress_ (process-wide). */
 void srg_set_default_options(const srg_bp_options *o);
+
+/* Bytes the last drop-in call on `device` (-1: current) copied to the device
+ * (range lines of its range band, orbit, DEM box) and back (row blocks of the
+ * output box).  The drop-in uploads only the range bins a term of a formed
+ * pixel can read (with a margin of 8 bins), found on the device from the DEM
+ * box and the azimuth centres before the lines go up; the reference uploads
+ * every line in full (azimuth_compress.cu:367-368). */
+int srg_dropin_last_bytes(int device, long long *h2d, long long *d2h);
 
 /* ------------------------------------------------------------------------
  * Per-burst scalars of the azimuth_compress_ call, derived as
@@ -161,6 +172,10 @@ typedef struct srg_burst_desc {
     const double *timeorbit, *xx, *vv;
     int numstatevec;
     double tmid, xyz_mid[3], vel_mid[3], angc0, angc1, prf;
+    /* the range bins held in `burst`: bins [bin0, bin0 + nbins) of every
+     * line, column c of a row being bin bin0 + c (bin0 even); terms whose taps
+     * fall outside read zeros.  0 and 0: the whole line (nbins = S). */
+    int bin0, nbins;
 } srg_burst_desc;
 
 /* Backproject `n` bursts in one persistent launch on `stream` (a

@@ -99,6 +99,13 @@ def azimuth_compress_status(b: Burst, fdout: int, fddem: int, form: int = FORM_S
     return rc
 
 
+def dropin_last_bytes(device: int = -1):
+    """(host-to-device, device-to-host) bytes of the last drop-in call."""
+    h, d = C.c_longlong(), C.c_longlong()
+    check(lib().srg_dropin_last_bytes(device, C.byref(h), C.byref(d)))
+    return int(h.value), int(d.value)
+
+
 def burst_params(lines: np.ndarray, satvel: np.ndarray) -> dict:
     """Per-burst scalars of the azimuth_compress_ call (srg_burst_params:
     burstparams, fdopcoefs, aperture and limits of

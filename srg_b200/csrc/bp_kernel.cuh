@@ -127,7 +127,9 @@ __device__ __forceinline__ int warp_max(int v) {
 }
 
 __device__ __forceinline__ float2 ld_sample(const BurstDev &B, int k, int gi) {
-    if (gi >= 0 && gi < B.S && k < B.P) return __ldg(B.burst + (long long)k * B.ldb + gi);
+    const int p = gi - B.bin0;  // column of bin gi in the lines held
+    if (gi >= 0 && gi < B.S && (unsigned)p < (unsigned)B.nbins && k < B.P)
+        return __ldg(B.burst + (long long)k * B.ldb + p);
     return make_float2(0.f, 0.f);
 }
 
@@ -365,7 +367,7 @@ bp_tiles(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                         if (k0 == kmin) fence_tensormap_acquire(tmaps + B.tmap);
                         fence_proxy_async_shared();
                         mbar_arrive_expect_tx(&ctl.bar, (uint32_t)(WB * CK * 8));
-                        tma_load_2d(samp, tmaps + B.tmap, &ctl.bar, x0, k0);
+                        tma_load_2d(samp, tmaps + B.tmap, &ctl.bar, x0 - B.bin0, k0);
                     }
                 }
             }

@@ -629,7 +629,8 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                     if (c == 0) fence_tensormap_acquire(tmaps + B.tmap);
                     fence_proxy_async_shared();
                     mbar_expect_tx(&ctl.full[s], (uint32_t)(WB * CK * 8));
-                    tma_load_2d(samp0 + (size_t)s * CK * WB, tmaps + B.tmap, &ctl.full[s], x0, k0);
+                    tma_load_2d(samp0 + (size_t)s * CK * WB, tmaps + B.tmap, &ctl.full[s],
+                                x0 - B.bin0, k0);
                     issued |= 1u << s;
                     issued_par = (issued_par & ~(1u << s)) | ((r & 1u) << s);
                 }

@@ -59,7 +59,7 @@ int fail(int code, const char *fmt, ...) {
             return fail(SRG_E_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));   \
     } while (0)
 
-srg_bp_options g_default_opts = {SRG_FORM_SPLIT, -1, -1, 0, 0, 0, 0};
+srg_bp_options g_default_opts = {SRG_FORM_SPLIT, -1, -1, 0, 0, 0, 0, 0};
 std::mutex g_opts_mu;
 
 DevCtx g_ctx[64];
@@ -151,6 +151,38 @@ void ref_limits(const double *latlons, double firstlat, double deltalat, double 
 
 double ref_pi() { return 4.0 * atan2(1.0, 1.0); }
 
+// R_k^2 = |x - s_k|^2 has the second difference
+//   |ds_k|^2 + |ds_{k-1}|^2 - 2 (x - s_k) . d2s_k
+// (ds_k = s_{k+1} - s_k, d2s_k = s_{k+1} - 2 s_k + s_{k-1}), positive at every
+// pulse for every point x within rbound of it when
+// |ds_k|^2 + |ds_{k-1}|^2 > 2 rbound |d2s_k|.  A pixel with a term in range
+// lies within rngend of that term's pulse, so within rngend + the track's
+// length of every pulse of its window; the test takes twice that bound.  On
+// an orbit the left side is ~40 m^2 and the right ~10 m^2.
+bool pulses_convex(const double *s, int P, double rngend) {
+    if (P < 3) return true;
+    double track = 0.0;
+    for (int k = 0; k + 1 < P; ++k) {
+        const double a = s[3 * k + 3] - s[3 * k], b = s[3 * k + 4] - s[3 * k + 1],
+                     c = s[3 * k + 5] - s[3 * k + 2];
+        track += std::sqrt(a * a + b * b + c * c);
+    }
+    const double rbound = std::fabs(rngend) + track;
+    for (int k = 1; k + 1 < P; ++k) {
+        double n1 = 0.0, n0 = 0.0, n2 = 0.0;
+        for (int q = 0; q < 3; ++q) {
+            const double d1 = s[3 * (k + 1) + q] - s[3 * k + q];
+            const double d0 = s[3 * k + q] - s[3 * (k - 1) + q];
+            const double d2 = d1 - d0;
+            n1 += d1 * d1;
+            n0 += d0 * d0;
+            n2 += d2 * d2;
+        }
+        if (!(n1 + n0 > 4.0 * rbound * std::sqrt(n2))) return false;
+    }
+    return true;
+}
+
 bool all_finite(const double *v, size_t n) {
     for (size_t i = 0; i < n; ++i)
         if (!std::isfinite(v[i])) return false;
@@ -160,9 +192,13 @@ bool all_finite(const double *v, size_t n) {
 int validate_desc(const srg_burst_desc &d) {
     if (!d.burst || !d.satloc || !d.dem || !d.out)
         return fail(SRG_E_ARG, "null device pointer in burst descriptor");
-    if (d.P < 1 || d.S < 2 || d.ldb < d.S || d.demwidth < 1 || d.nlines < 1)
-        return fail(SRG_E_ARG, "bad sizes: P=%d S=%d ldb=%lld W=%d nlines=%d", d.P, d.S,
-                    (long long)d.ldb, d.demwidth, d.nlines);
+    const int nbins = d.nbins > 0 ? d.nbins : d.S;
+    if (d.P < 1 || d.S < 2 || d.ldb < nbins || d.demwidth < 1 || d.nlines < 1)
+        return fail(SRG_E_ARG, "bad sizes: P=%d S=%d ldb=%lld nbins=%d W=%d nlines=%d", d.P, d.S,
+                    (long long)d.ldb, nbins, d.demwidth, d.nlines);
+    if (d.bin0 < 0 || (d.bin0 & 1) || d.nbins < 0 || (long long)d.bin0 + nbins > d.S)
+        return fail(SRG_E_ARG, "bad bin window bin0=%d nbins=%d of S=%d (bin0 even)", d.bin0,
+                    d.nbins, d.S);
     if (d.P > 100000000 || d.S > (1 << 28))
         return fail(SRG_E_ARG, "burst too large: P=%d S=%d", d.P, d.S);
     if (!(d.dmrg > 0) || !(d.wvl > 0) || d.aperture < 0)
@@ -183,6 +219,8 @@ BurstDev make_burst_dev(const srg_burst_desc &d, const double *coef) {
     B.out = reinterpret_cast<float2 *>(d.out);
     B.coef = coef;
     B.ldb = d.ldb;
+    B.bin0 = d.bin0;
+    B.nbins = d.nbins > 0 ? d.nbins : d.S;
     B.dem_ld = d.dem_ld;
     B.out_ld = d.out_ld;
     B.P = d.P;
@@ -221,8 +259,8 @@ int make_tmap(const BurstDev &B, int box_x, int box_y, CUtensorMap *out) {
     auto enc = get_encode();
     if (!enc) return -1;
     const uintptr_t base = reinterpret_cast<uintptr_t>(B.burst);
-    if ((base & 15) || ((B.ldb * 8) & 15) || (box_x & 1)) return -1;
-    cuuint64_t dims[2] = {(cuuint64_t)B.S, (cuuint64_t)B.P};
+    if ((base & 15) || ((B.ldb * 8) & 15) || (box_x & 1) || (B.bin0 & 1)) return -1;
+    cuuint64_t dims[2] = {(cuuint64_t)B.nbins, (cuuint64_t)B.P};
     cuuint64_t strides[1] = {(cuuint64_t)(B.ldb * 8)};
     cuuint32_t box[2] = {(cuuint32_t)box_x, (cuuint32_t)box_y};
     cuuint32_t estr[2] = {1, 1};
@@ -460,6 +498,7 @@ void srg_bp_default_options(srg_bp_options *o) {
     o->centres_on_host = 0;
     o->verbose = 0;
     o->spin_limit = 0;
+    o->full_lines = 0;
     o->scratch_limit = 0;
 }
 
@@ -523,6 +562,16 @@ int srg_bp_burst_device_gated(const srg_burst_desc *b, const int *ready_word, in
     std::lock_guard<std::mutex> g(c->mu);
     UploadGate gate{ready_word, ready_base, ready_rows};
     return run_bursts(*c, b, 1, o, static_cast<cudaStream_t>(stream), nullptr, &gate);
+}
+
+int srg_dropin_last_bytes(int device, long long *h2d, long long *d2h) {
+    DevCtx *c = nullptr;
+    int rc = get_ctx(device, &c);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> g(c->mu);
+    if (h2d) *h2d = c->last_h2d;
+    if (d2h) *d2h = c->last_d2h;
+    return SRG_OK;
 }
 
 int srg_test_set_dropin_sequence(int device, int seq) {
@@ -641,6 +690,8 @@ int srg_forward_project_device(const srg_burst_desc *b, const float *refl, int64
     if (!b || !refl || !satvel) return fail(SRG_E_ARG, "bad arguments");
     int rc = validate_desc(*b);
     if (rc) return rc;
+    if (b->bin0 != 0 || (b->nbins != 0 && b->nbins != b->S))
+        return fail(SRG_E_ARG, "forward projection writes whole lines (bin0 0, nbins 0 or S)");
     DevCtx *c = nullptr;
     rc = get_ctx(-1, &c);
     if (rc) return rc;
@@ -813,15 +864,28 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     }
     ++c->upload_seq;
     const int ready_base = c->upload_seq * 64;
-    const size_t row_bytes = (size_t)samplesPerBurst * 8;
+    // The lines go up cropped to the range bins the sum can read (the range
+    // band, known once the DEM box and the azimuth centres are on the device):
+    // rows of nbins samples from bin bin0, row pitch ldbc samples.
+    int bin0 = 0, nbins = samplesPerBurst;
+    long long ldbc = (samplesPerBurst + 1) & ~1;
     auto upload = [&](int kb, int ke) -> int {
+        const size_t spitch = (size_t)samplesPerBurst * 8, dpitch = (size_t)ldbc * 8;
+        const size_t width = (size_t)nbins * 8;
         for (int k = kb; k < ke; ++k) {
             const int g0 = k ? std::min(kBlockEnd[k - 1], ngran) : 0, g1 = std::min(kBlockEnd[k], ngran);
             const int r0 = std::min(rawdatalines, g0 * up_rows), r1 = std::min(rawdatalines, g1 * up_rows);
-            if (r0 < r1)
-                CK(cudaMemcpyAsync(static_cast<char *>(c->in_burst.p) + r0 * row_bytes,
-                                   reinterpret_cast<const char *>(burstdata) + r0 * row_bytes,
-                                   (r1 - r0) * row_bytes, cudaMemcpyHostToDevice, c->s_copy));
+            if (r0 < r1) {
+                char *dst = static_cast<char *>(c->in_burst.p) + (size_t)r0 * dpitch;
+                const char *src = reinterpret_cast<const char *>(burstdata) + (size_t)r0 * spitch +
+                                  (size_t)bin0 * 8;
+                if (dpitch == spitch && width == spitch)
+                    CK(cudaMemcpyAsync(dst, src, (size_t)(r1 - r0) * spitch, cudaMemcpyHostToDevice,
+                                       c->s_copy));
+                else
+                    CK(cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, r1 - r0,
+                                         cudaMemcpyHostToDevice, c->s_copy));
+            }
             c->host_flags[DevCtx::kReadyHost + k] = ready_base + g1;
             CK(cudaMemcpyAsync(ready_word, c->host_flags + DevCtx::kReadyHost + k, sizeof(int),
                                cudaMemcpyHostToDevice, c->s_copy));
@@ -830,10 +894,10 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     };
     UploadGate gate{ready_word, ready_base, up_rows};
     // Host-to-device copies leave the copy engine in the order they are
-    // issued, whatever their stream: with a gated kernel the small inputs go
-    // first, then the first block, then (while it travels) the DEM box and the
-    // launch, and the other blocks last; without one, every block before the
-    // launch, which waits for them all.
+    // issued, whatever their stream: the small inputs and the DEM box go
+    // first; with a gated kernel then the first block and the launch, and the
+    // other blocks last; without one, every block before the launch, which
+    // waits for them all.
     const KernelEntry *ke0 = pick_kernel(o.form, o.tile_cfg);
     const bool pipelined = ke0 && gated_twin(*ke0) != nullptr;
     // With the gated kernel the output also comes back while the sum runs: the
@@ -861,11 +925,6 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
         CK(cudaMemsetAsync(rbw, 0, (2 * K + 1) * sizeof(int), st));
     }
     CK(cudaMemcpyAsync(c->in_sat.p, satloc, 24 * (size_t)rawdatalines, cudaMemcpyHostToDevice, st));
-    if ((rc = upload(0, pipelined ? 1 : nup))) {
-        drain();  // the caller's buffer stays in use until then
-        return rc;
-    }
-    if (!pipelined) CKD(cudaEventRecord(c->ev_burst, c->s_copy));
     // DEM box of rows [fl, fl + nl) (azimuth_compress.cu:399-408), read by the
     // pool's threads; a file that ends before the box does is an error (the
     // reference would use whatever its buffer held)
@@ -904,7 +963,7 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     d.dem = static_cast<const int16_t *>(c->in_dem.p) - fp_eff;
     d.out = static_cast<float *>(c->out.p);
     d.coef = nullptr;
-    d.ldb = samplesPerBurst;
+    d.ldb = ldbc;
     d.dem_ld = ncols;
     d.out_ld = ncols;
     d.P = rawdatalines;
@@ -936,6 +995,54 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     d.angc0 = angc0;
     d.angc1 = angc1;
     d.prf = prf;
+    // azimuth centres (azimuth_compress.cu:438-481) on the device, before the
+    // lines: the range band needs them, and so does the sum
+    if ((rc = c->coef.ensure(sizeof(double) * 3 * (size_t)nl))) {
+        drain();
+        return rc;
+    }
+    double *coef = static_cast<double *>(c->coef.p);
+    if ((rc = centres_device(*c, d, make_burst_dev(d, coef), coef, st))) {
+        drain();
+        return rc;
+    }
+    d.coef = coef;
+    // The range band: every bin a term of a formed pixel can read, with a
+    // margin; the whole line unless the pulses satisfy the convexity test
+    // the band's bisection relies on (pulses_convex).
+    if (!o.full_lines && pulses_convex(satloc, rawdatalines, rngend)) {
+        int *rw = static_cast<int *>(c->flags.p) + DevCtx::kRangeWord;
+        CKD(cudaMemsetAsync(rw, 0x7f, sizeof(int), st));      // INT_MAX-like
+        CKD(cudaMemsetAsync(rw + 1, 0x80, sizeof(int), st));  // INT_MIN-like
+        CKD(launch_range_band(make_burst_dev(d, coef), rw, c->sms, st));
+        CKD(cudaMemcpyAsync(c->host_flags + DevCtx::kRangeHost, rw, 2 * sizeof(int),
+                            cudaMemcpyDeviceToHost, st));
+        CKD(cudaStreamSynchronize(st));
+        const int lo = c->host_flags[DevCtx::kRangeHost], hi = c->host_flags[DevCtx::kRangeHost + 1];
+        if (lo <= hi) {
+            const long long b0 = std::max<long long>(0, (long long)lo - kBandMargin) & ~1LL;
+            const long long b1 = std::min<long long>(samplesPerBurst - 1, (long long)hi + kBandMargin);
+            if (b1 > b0 && b0 < samplesPerBurst) {
+                bin0 = (int)b0;
+                nbins = (int)(b1 - b0 + 1);
+            }
+        } else {  // no formed pixel: nothing is read
+            bin0 = 0;
+            nbins = std::min(samplesPerBurst, 2);
+        }
+        ldbc = (nbins + 1) & ~1;
+    }
+    d.ldb = ldbc;
+    d.bin0 = bin0;
+    d.nbins = nbins;
+    c->last_h2d = (long long)rawdatalines * nbins * 8 + 24LL * rawdatalines + (long long)dem_bytes +
+                  56LL * numstatevec;
+    c->last_d2h = 0;
+    if ((rc = upload(0, pipelined ? 1 : nup))) {
+        drain();  // the caller's buffer stays in use until then
+        return rc;
+    }
+    if (!pipelined) CKD(cudaEventRecord(c->ev_burst, c->s_copy));
     // rows of the kept tiles (the band): rows outside it have no formed pixel
     int *band = static_cast<int *>(c->flags.p) + DevCtx::kBandWord;
     CKD(cudaMemsetAsync(band, 0x7f, sizeof(int), st));      // INT_MAX-like
@@ -983,6 +1090,7 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     int nblk = 0;
     auto copy_back = [&](int r0, int r1, cudaStream_t s) {
         const size_t off = (size_t)r0 * ncols * 2, n = (size_t)(r1 - r0) * ncols * 8;
+        c->last_d2h += (long long)n;
         return cudaMemcpyAsync(win + off, static_cast<float *>(c->out.p) + off, n,
                                cudaMemcpyDeviceToHost, s);
     };

@@ -19,7 +19,7 @@ enum : int {
 // Everything a kernel needs about one burst, prepared on the host.  Field
 // names follow the reference's (sentinel/azimuth_compress.cu).
 struct BurstDev {
-    const float2 *burst;      // [P][ldb] complex64
+    const float2 *burst;      // [P][ldb] complex64: bins [bin0, bin0 + nbins) of each line
     const double *satloc;     // [P][3]
     const short *dem;         // row 0 = grid line firstline; stride dem_ld
     float2 *out;              // row 0 = grid line firstline; stride out_ld
@@ -33,6 +33,10 @@ struct BurstDev {
     int tiles_x, tiles_y, tile_base;
     int tmap;                 // index of this burst's TMA descriptor, -1 = none
     unsigned spin;            // polls of a bounded device-side wait (the launch's first burst's)
+    // The lines held in device memory: logical range bins [bin0, bin0 + nbins)
+    // of [0, S) (bin0 even; the whole line: 0 and S).  Bin b of pulse k is at
+    // burst[k * ldb + b - bin0]; bins outside read as zero.
+    int bin0, nbins;
     double firstlat, deltalat, firstlon, deltalon, deg2rad;
     double rngstart, rmax;    // rmax = rngend - dmrg (the reference's upper range test)
     double dmrg, k4pi;        // k4pi = 4*pi/wvl, grouped as the reference

@@ -14,6 +14,9 @@
 namespace srg {
 namespace detail {
 
+// Range bins of margin on each side of the drop-in's range band.
+constexpr int kBandMargin = 8;
+
 // Record a one-line error message for srg_last_error() and return `code`.
 int fail(int code, const char *fmt, ...);
 
@@ -64,6 +67,11 @@ struct DevCtx {
     // tiles, [kReadyWord] rows-uploaded word; host_flags[kReadyHost + k] holds
     // the value the copy stream writes after upload block k
     static constexpr int kBandWord = 4, kReadyWord = 6, kReadyHost = 8, kUploadBlocks = 8;
+    // the range band of the drop-in's lines: device words [kRangeWord, +1],
+    // their host copy host_flags[kRangeHost, +1]; bins of margin on each side
+    static constexpr int kRangeWord = 8, kRangeHost = 2;
+    // bytes the last drop-in call copied to and from the device
+    long long last_h2d = 0, last_d2h = 0;
     // row blocks copied back while the sum still runs (gated kernel): device
     // words rb[k] stored-tile counts, rb[kRowBlocks + k] kept-tile counts,
     // rb[2 kRowBlocks] the order word, rb[3 kRowBlocks + k] done words;
@@ -104,6 +112,9 @@ BurstDev make_burst_dev(const srg_burst_desc &d, const double *coef);
 // 0 and *out filled when a TMA descriptor can describe the burst, else -1.
 int make_tmap(const BurstDev &B, int box_x, int box_y, CUtensorMap *out);
 double ref_pi();
+// |x - s_k|^2 is convex in the pulse index k for every pixel x that can have
+// a term in range (the range band's bisection relies on it).
+bool pulses_convex(const double *satloc, int P, double rngend);
 // Every one of the n values is finite.
 bool all_finite(const double *v, size_t n);
 

@@ -115,6 +115,54 @@ __global__ void count_terms_kernel(BurstDev B, unsigned long long *terms) {
 }
 
 // ---------------------------------------------------------------------------
+// Range bins a burst's sum can read.  For every formed pixel of the box the
+// terms run over its aperture window [azs, aze) (azimuth_compress.cu:54-58)
+// and read bins floor((R_k - rngstart) / dmrg) and the next one (:65-69).
+// Where R_k^2 is convex in the pulse index k (the host checks the pulses for
+// it) R_k is largest at an end of the window and smallest where the forward
+// difference of R_k^2 turns non-negative, found by bisection; the pixel's
+// bins lie between those of its smallest and largest range (+1 for the
+// second tap).  band[0] / band[1] are lowered / raised to the extremes over
+// all formed pixels (preset to INT_MAX / INT_MIN by the caller).
+__global__ void range_band_kernel(BurstDev B, int *band) {
+    const int nx = B.lastpix_eff - B.firstpix + 1;
+    const long long npix = (long long)nx * B.nlines;
+    int lo = INT_MAX, hi = INT_MIN;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < npix;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int line = (int)(idx / nx);
+        const int px = B.firstpix + (int)(idx - (long long)line * nx);
+        int azs, aze;
+        pixel_window(B, pixel_azoff(B, B.coef + 3 * line, px), azs, aze);
+        if (aze <= azs) continue;
+        double X[3];
+        pixel_ecef(B, line, px, (double)B.dem[(long long)line * B.dem_ld + px], X[0], X[1], X[2]);
+        auto r2 = [&](int k) {
+            const double *s = B.satloc + 3 * k;
+            const double vx = X[0] - s[0], vy = X[1] - s[1], vz = X[2] - s[2];
+            return vx * vx + vy * vy + vz * vz;
+        };
+        int a = azs, b = aze - 1;
+        while (a < b) {
+            const int m = (a + b) >> 1;
+            if (r2(m + 1) < r2(m)) a = m + 1;
+            else b = m;
+        }
+        const double rmin = sqrt(r2(a)), rmax = sqrt(fmax(r2(azs), r2(aze - 1)));
+        const double blo = fmin(fmax(floor((rmin - B.rngstart) * B.inv_dmrg), -1e9), 1e9);
+        const double bhi = fmin(fmax(floor((rmax - B.rngstart) * B.inv_dmrg) + 1.0, -1e9), 1e9);
+        lo = min(lo, (int)blo);
+        hi = max(hi, (int)bhi);
+    }
+    lo = warp_min(lo);
+    hi = warp_max(hi);
+    if ((threadIdx.x & 31) == 0 && lo <= hi) {
+        atomicMin(band, lo);
+        atomicMax(band + 1, hi);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Ordered merge (azimuth_compress.cu:527-531): replace where |Re(src)| > 1e-18.
 __global__ void merge_kernel(float2 *dst, long long dst_ld, const float2 *src, long long src_ld,
                              int rows, int cols) {
@@ -535,6 +583,14 @@ cudaError_t launch_merge_scene(const BurstDev *bursts, int n, float2 *dst, long 
     dim3 grid((cols + 31) / 32, (lines + 31) / 32);
     merge_scene_kernel<<<grid, dim3(32, 8), 0, st>>>(bursts, n, dst, dst_ld, lines, cols, tile_mask,
                                                      txl, tyl);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_range_band(const BurstDev &B, int *band, int sms, cudaStream_t st) {
+    const long long npix = (long long)(B.lastpix_eff - B.firstpix + 1) * B.nlines;
+    if (npix <= 0) return cudaSuccess;
+    const long long blocks = std::min<long long>((npix + 255) / 256, (long long)sms * 8);
+    range_band_kernel<<<(int)blocks, 256, 0, st>>>(B, band);
     return cudaGetLastError();
 }
 

@@ -73,6 +73,10 @@ cudaError_t launch_merge_scene(const BurstDev *bursts, int n, float2 *dst, long 
                                const unsigned char *tile_mask = nullptr, int tx = 0, int ty = 0);
 cudaError_t launch_count_terms(const BurstDev &B, unsigned long long *terms, int sms,
                                cudaStream_t st);
+// Lowest and highest range bin (band[0], band[1], preset to INT_MAX / INT_MIN)
+// that the terms of the burst's formed pixels can read, given R^2 convex in
+// the pulse index (kernels.cu: range_band_kernel).
+cudaError_t launch_range_band(const BurstDev &B, int *band, int sms, cudaStream_t st);
 cudaError_t launch_merge(float2 *dst, long long dst_ld, const float2 *src, long long src_ld,
                          int rows, int cols, int sms, cudaStream_t st);
 cudaError_t launch_pulse_orbit(const double *times, int P, const Orbit &o, double *pos,
