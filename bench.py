@@ -426,7 +426,7 @@ def reference_cpu(workload: str, steps: int, warmup: int):
         b.burst = np.zeros((0, S), np.complex64)   # free the lines
     desc = (f"reference azimuth_compress_cpu_ (OpenMP, {cores} threads) end to end on whole "
             f"bursts {used} of the workload, one per step ({terms_tot} terms, {secs_tot:.1f} s)")
-    return terms_tot / secs_tot, cores, desc
+    return terms_tot / secs_tot, cores, desc, secs_tot / max(1, len(used))
 
 
 # ---------------------------------------------------------------------------
@@ -504,10 +504,11 @@ def main():
         if rank != 0:
             return  # the reference arm runs on rank 0 only
         # host only: neither torch.cuda nor the CUDA library is loaded here
-        value, cores, sample = reference_cpu(args.workload, max(1, args.steps), args.warmup)
+        value, cores, sample, s_step = reference_cpu(args.workload, max(1, args.steps), args.warmup)
         value /= 1e9
         line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
                 "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": s_step * 1e3,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic", "config": config,
                 "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
@@ -609,7 +610,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(
             os.path.join(ROOT, "oracle", "_ref", "libref_cpu.so")):
         # a bounded sample: one whole burst per subswath (c3) or the burst
-        v, cores, sample = reference_cpu(args.workload, 3 if args.workload == "c3" else 1, 0)
+        v, cores, sample, _ = reference_cpu(args.workload, 3 if args.workload == "c3" else 1, 0)
         cpu = {"value": v / 1e9, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample}
     if rank != 0:
         if world > 1:

@@ -39,8 +39,9 @@ typedef struct srg_bp_options {
     int form;          /* SRG_FORM_FP64 or SRG_FORM_SPLIT */
     int tile_cfg;      /* kernel shape index (srg_tile_config_count()); -1: tuned default */
     int device;        /* CUDA device ordinal; -1: current device */
-    int centres_on_host; /* 1: per-line azimuth centres solved on the host CPU,
-                            0: on the GPU (default) */
+    int centres_on_host; /* must be 0: the per-line azimuth centres are solved
+                            on the GPU (1 is SRG_E_UNSUPPORTED wherever the
+                            entry would solve them) */
     int verbose;       /* 1: print the reference's "Burst line limits" line */
     int spin_limit;    /* polls of a bounded device-side wait (for range lines
                           still uploading, or for a staged tile) before the
@@ -235,8 +236,57 @@ int srg_scene_sync(srg_scene *s, void *stream);
 /* Exact executed-term count of one pass (computed once, blocking). */
 int srg_scene_terms(srg_scene *s, int64_t *terms);
 /* Autotuner: time every compiled kernel shape of the plan's form on this
- * scene (`iters` timed launches each) and keep the fastest. */
+ * scene (`iters` timed launches each) and keep the fastest, or take the
+ * cached best shape of a scene of the same shape (srg_scene_autotune). */
 int srg_scene_tune(srg_scene *s, int iters, int *best_cfg, double *best_ms);
+/* Autotuner with the range interpolation in its search.  With
+ * interp_budget > 0 it first estimates, from a sample of every burst's lines,
+ * the RMS phase error (rad) each interpolation adds (srg_interp_error): the
+ * reference's linear interpolation of the original lines when that is within
+ * the budget, else linear interpolation between the bins of 2x-oversampled
+ * lines, which the plan then makes in every pass (srg_oversample_range_device
+ * into buffers of its own; the lines must be whole, bin0 = 0).  It then times
+ * the kernel shapes of the plan's form, unless use_cache finds the best shape
+ * of an earlier tuning of a scene of the same shape (same form,
+ * interpolation, and bursts' pulses, samples, grid lines and columns to
+ * within 64, 1024, 64, 64); results are kept for the process and, when the
+ * environment variable SRG_TUNE_CACHE names a file, appended to it and read
+ * back by later processes.  srg_scene_tune is this with no interpolation
+ * budget and the cache on.  No reference counterpart. */
+#define SRG_INTERP_LINEAR       0  /* the original lines (azimuth_compress.cu:65-69) */
+#define SRG_INTERP_OVERSAMPLED2 1  /* 2x-oversampled lines, 8-tap half samples */
+typedef struct srg_tune_request {
+    int iters;             /* timed launches per shape (< 1: 3) */
+    int use_cache;         /* 1: take a cached shape without timing */
+    double interp_budget;  /* RMS phase error (rad) the interpolation may add;
+                              <= 0: keep the plan's interpolation */
+} srg_tune_request;
+typedef struct srg_tune_result {
+    int tile_cfg;          /* shape in use */
+    int interp;            /* SRG_INTERP_* in use */
+    int from_cache;        /* 1: the shape came from the cache (nothing timed) */
+    int pad;
+    double ms;             /* mean backprojection time of the shape (-1: cached) */
+    double err_linear, err_oversampled; /* estimated RMS phase error (rad) of
+                              each interpolation (-1: not estimated) */
+} srg_tune_result;
+int srg_scene_autotune(srg_scene *s, const srg_tune_request *req, srg_tune_result *res);
+/* Use an interpolation (SRG_INTERP_*) without tuning, and read it back. */
+int srg_scene_set_interp(srg_scene *s, int interp);
+int srg_scene_interp(const srg_scene *s);
+
+/* Expected RMS phase error (rad) that linear interpolation adds to a term,
+ * on the lines as they are (*err_linear) and after 2x oversampling
+ * (*err_oversampled), from the mean power spectrum of `sample_lines` lines
+ * spread over the nlines lines ([nlines][ld] complex64, nsamps samples,
+ * device).  For a fractional offset u the linear interpolant differs from
+ * the band-limited line by (1-u) + u e^{i 2 pi nu} - e^{i 2 pi nu u} per unit
+ * of spectrum at nu cycles/sample (on the oversampled line, the same between
+ * an original and a filtered half sample); half that error power lies across
+ * the signal.  Blocking; allocates scratch (cuFFT). */
+int srg_interp_error(const float *lines, long long ld, int nlines, int nsamps, int sample_lines,
+                     double *err_linear, double *err_oversampled, void *stream);
+
 /* Select a kernel shape, or a form and shape (-1: that form's default). */
 int srg_scene_set_shape(srg_scene *s, int tile_cfg);
 int srg_scene_set_form(srg_scene *s, int form, int tile_cfg);

@@ -61,6 +61,20 @@ class BurstParams(C.Structure):
                                                                  ("pad", C.c_int)]
 
 
+INTERP_LINEAR = 0
+INTERP_OVERSAMPLED2 = 1
+
+
+class TuneRequest(C.Structure):
+    _fields_ = [("iters", C.c_int), ("use_cache", C.c_int), ("interp_budget", C.c_double)]
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("tile_cfg", C.c_int), ("interp", C.c_int), ("from_cache", C.c_int),
+                ("pad", C.c_int), ("ms", C.c_double), ("err_linear", C.c_double),
+                ("err_oversampled", C.c_double)]
+
+
 class SrgError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"srg error {code}: {msg}")
@@ -97,6 +111,11 @@ _SIGS = {
     "srg_scene_run_stages": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "srg_scene_terms": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "srg_scene_tune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+    "srg_scene_autotune": (C.c_int, [C.c_void_p, C.POINTER(TuneRequest), C.POINTER(TuneResult)]),
+    "srg_scene_set_interp": (C.c_int, [C.c_void_p, C.c_int]),
+    "srg_scene_interp": (C.c_int, [C.c_void_p]),
+    "srg_interp_error": (C.c_int, [C.c_void_p, C.c_longlong, C.c_int, C.c_int, C.c_int,
+                                   C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p]),
     "srg_scene_set_shape": (C.c_int, [C.c_void_p, C.c_int]),
     "srg_scene_set_form": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "srg_scene_shape": (C.c_int, [C.c_void_p]),

@@ -99,6 +99,17 @@ def azimuth_compress_status(b: Burst, fdout: int, fddem: int, form: int = FORM_S
     return rc
 
 
+def interp_error(lines, nsamps: Optional[int] = None, sample_lines: int = 64, stream=None):
+    """(linear, 2x-oversampled) expected RMS phase error (rad) of the range
+    interpolation on device lines ([nlines][ld] complex64 tensor)."""
+    el, eo = C.c_double(), C.c_double()
+    nsamps = lines.shape[1] if nsamps is None else nsamps
+    check(lib().srg_interp_error(C.c_void_p(lines.data_ptr()), lines.stride(0), lines.shape[0],
+                                 nsamps, sample_lines, C.byref(el), C.byref(eo),
+                                 C.c_void_p(_stream_ptr(stream))))
+    return float(el.value), float(eo.value)
+
+
 def dropin_last_bytes(device: int = -1):
     """(host-to-device, device-to-host) bytes of the last drop-in call."""
     h, d = C.c_longlong(), C.c_longlong()
@@ -448,6 +459,21 @@ class Scene:
         cfg, ms = C.c_int(), C.c_double()
         check(lib().srg_scene_tune(self.handle, iters, C.byref(cfg), C.byref(ms)))
         return int(cfg.value), float(ms.value)
+
+    def autotune(self, interp_budget: float = 0.0, iters: int = 3, use_cache: bool = True) -> dict:
+        """srg_scene_autotune: the interpolation within `interp_budget` (RMS
+        phase error in rad; 0 keeps the plan's), then the fastest shape
+        (or the cached one).  Returns the srg_tune_result fields."""
+        q = _lib.TuneRequest(iters, int(bool(use_cache)), float(interp_budget))
+        r = _lib.TuneResult()
+        check(lib().srg_scene_autotune(self.handle, C.byref(q), C.byref(r)))
+        return {k: getattr(r, k) for k, _ in r._fields_ if k != "pad"}
+
+    def set_interp(self, interp: int) -> None:
+        check(lib().srg_scene_set_interp(self.handle, interp))
+
+    def interp(self) -> int:
+        return int(lib().srg_scene_interp(self.handle))
 
     def set_form(self, form: int, tile_cfg: int = -1) -> None:
         check(lib().srg_scene_set_form(self.handle, form, tile_cfg))

@@ -9,7 +9,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsrg_bp.so")
 SOURCES = ["capi.cu", "kernels.cu", "noalloc.cu", "scene.cu", "crossmul.cu", "rangecomp.cu",
-           "burstparams.cu"]
+           "burstparams.cu", "interp.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -767,6 +767,8 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
         std::lock_guard<std::mutex> g(g_opts_mu);
         o = g_default_opts;
     }
+    if (o.centres_on_host)
+        return fail(SRG_E_UNSUPPORTED, "azimuth centres are solved on the device only");
     int fl, ll, fp_, lp_;
     ref_limits(latlons, firstlat, deltalat, firstlon, deltalon, demwidth, demlength, &fl, &ll, &fp_,
                &lp_);
@@ -790,7 +792,7 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
         const KernelEntry *kc = pick_kernel(o.form, o.tile_cfg);
         const int tx = kc ? kc->shape.tx : 32, ty = kc ? kc->shape.ty : 4;
         const long long tiles = (long long)((ncols + tx - 1) / tx) * ((nl + ty - 1) / ty);
-        const long long need = (long long)rawdatalines * samplesPerBurst * 8 +
+        const long long need = (long long)rawdatalines * ((samplesPerBurst + 1) & ~1) * 8 +
                                24LL * rawdatalines + (long long)dem_bytes + (long long)win_bytes +
                                24LL * nl + 56LL * numstatevec +
                                (long long)tile_list_bytes((int)std::min<long long>(tiles, INT_MAX)) +
@@ -816,7 +818,8 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
         }
         c->host_cap = stage_bytes;
     }
-    const size_t bbytes = (size_t)rawdatalines * samplesPerBurst * 8;
+    // room for whole lines at an even row pitch (the range band needs less)
+    const size_t bbytes = (size_t)rawdatalines * (size_t)((samplesPerBurst + 1) & ~1) * 8;
     if ((rc = c->in_burst.ensure(bbytes)) || (rc = c->in_sat.ensure(24 * (size_t)rawdatalines)) ||
         (rc = c->in_dem.ensure(dem_bytes)) || (rc = c->out.ensure(win_bytes)) ||
         (rc = c->flags.ensure(64)))

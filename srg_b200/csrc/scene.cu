@@ -11,7 +11,12 @@
 // given, the ordered merge of every burst into it (one launch).  On a non-default stream the
 // first pass is captured into a CUDA graph and later passes replay it.
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "host_internal.h"
@@ -45,6 +50,12 @@ struct srg_scene {
     bool mask_valid = false;         // d_tiles holds the mask of the outputs' last backprojection
     cudaGraphExec_t graph = nullptr;
     cudaStream_t graph_stream = nullptr;
+    // range interpolation: SRG_INTERP_LINEAR on the caller's lines, or
+    // SRG_INTERP_OVERSAMPLED2 on 2x-oversampled copies the plan makes in
+    // every pass (os_lines: one [P][os_ld] buffer per burst)
+    int interp = SRG_INTERP_LINEAR;
+    std::vector<float2 *> os_lines;
+    std::vector<long long> os_ld;
 };
 
 namespace {
@@ -113,6 +124,34 @@ int set_kernel(srg_scene *s, int idx) {
     return SRG_OK;
 }
 
+// Burst descriptor of burst i as the kernels see it: the caller's lines, or
+// the plan's oversampled copy (2S - 1 samples at dmrg / 2 over the same
+// rngstart .. rngend, as srg_oversample_range_device documents).
+srg_burst_desc kernel_desc(const srg_scene *s, int i) {
+    srg_burst_desc d = s->descs[i];
+    if (s->interp == SRG_INTERP_OVERSAMPLED2) {
+        d.burst = reinterpret_cast<const float *>(s->os_lines[i]);
+        d.ldb = s->os_ld[i];
+        d.S = 2 * s->descs[i].S - 1;
+        d.dmrg = s->descs[i].dmrg / 2.0;
+        d.bin0 = d.nbins = 0;
+    }
+    return d;
+}
+
+// The 2x oversampling of every burst's lines into the plan's copies.
+int enqueue_oversample(srg_scene *s, cudaStream_t st) {
+    if (s->interp != SRG_INTERP_OVERSAMPLED2) return SRG_OK;
+    for (int i = 0; i < s->n; ++i) {
+        const srg_burst_desc &d = s->descs[i];
+        const int rc = srg_oversample_range_device(d.burst, d.ldb, d.P, d.S,
+                                                   reinterpret_cast<float *>(s->os_lines[i]),
+                                                   s->os_ld[i], st);
+        if (rc) return rc;
+    }
+    return SRG_OK;
+}
+
 int enqueue_centres(srg_scene *s, cudaStream_t st) {
     SCK(launch_line_centres_batch(s->d_bursts, s->d_jobs, s->n, s->total_lines, st));
     return SRG_OK;
@@ -151,10 +190,106 @@ cudaError_t merge(srg_scene *s, cudaStream_t st) {
 int enqueue_pass(srg_scene *s, cudaStream_t st) {
     int rc = enqueue_centres(s, st);
     if (rc) return rc;
+    rc = enqueue_oversample(s, st);
+    if (rc) return rc;
     rc = enqueue_backprojection(s, st);
     if (rc) return rc;
     if (s->scene) SCK(merge(s, st));
     return SRG_OK;
+}
+
+// Rebuild the kernels' burst table for the plan's interpolation (keeps the
+// azimuth-centre pointers and the poll limit) and the shape's tiles.
+int rebuild_bursts(srg_scene *s) {
+    for (int i = 0; i < s->n; ++i) {
+        const double *coef = s->hb[i].coef;
+        const unsigned spin = s->hb[i].spin;
+        s->hb[i] = make_burst_dev(kernel_desc(s, i), coef);
+        s->hb[i].spin = spin;
+    }
+    s->terms = -1;
+    return set_kernel(s, s->kernel);
+}
+
+int set_interp(srg_scene *s, int interp) {
+    if (interp != SRG_INTERP_LINEAR && interp != SRG_INTERP_OVERSAMPLED2)
+        return fail(SRG_E_ARG, "unknown interpolation %d", interp);
+    if (interp == s->interp) return SRG_OK;
+    if (interp == SRG_INTERP_OVERSAMPLED2) {
+        for (int i = 0; i < s->n; ++i)
+            if (s->descs[i].bin0 != 0 || (s->descs[i].nbins != 0 && s->descs[i].nbins != s->descs[i].S))
+                return fail(SRG_E_UNSUPPORTED, "burst %d: oversampling needs whole lines", i);
+        if (s->os_lines.empty()) {
+            s->os_lines.assign(s->n, nullptr);
+            s->os_ld.assign(s->n, 0);
+            for (int i = 0; i < s->n; ++i) {
+                const long long ld = 2LL * s->descs[i].S;  // even: 16-byte rows for TMA
+                void *p = nullptr;
+                const int rc = alloc(&p, sizeof(float2) * (size_t)s->descs[i].P * (size_t)ld);
+                if (rc) return rc;
+                s->os_lines[i] = static_cast<float2 *>(p);
+                s->os_ld[i] = ld;
+            }
+        }
+    }
+    s->interp = interp;
+    return rebuild_bursts(s);
+}
+
+// Tuning results of this process (and, with SRG_TUNE_CACHE naming a file, of
+// earlier ones): the best shape per form, interpolation and scene shape.
+std::mutex g_tune_mu;
+std::map<std::string, int> g_tune;
+bool g_tune_loaded = false;
+
+const char *tune_file() {
+    const char *f = std::getenv("SRG_TUNE_CACHE");
+    return f && *f ? f : nullptr;
+}
+
+// Scene shape: the multiset of (pulses / 64, samples / 1024, lines / 64,
+// columns / 64) of its bursts, with the form and the interpolation.
+std::string tune_key(const srg_scene *s) {
+    std::vector<std::string> parts;
+    for (int i = 0; i < s->n; ++i) {
+        const BurstDev &B = s->hb[i];
+        char buf[96];
+        snprintf(buf, sizeof buf, "%d/%d/%d/%d", B.P / 64, B.S / 1024, B.nlines / 64,
+                 (B.lastpix_eff - B.firstpix + 1) / 64);
+        parts.emplace_back(buf);
+    }
+    std::sort(parts.begin(), parts.end());
+    std::string k = "f" + std::to_string(s->opts.form) + ":i" + std::to_string(s->interp) + ":";
+    for (const std::string &p : parts) k += p + ",";
+    return k;
+}
+
+int tune_lookup(const std::string &key) {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    if (!g_tune_loaded) {
+        g_tune_loaded = true;
+        if (const char *f = tune_file()) {
+            if (FILE *fp = std::fopen(f, "r")) {
+                char key_buf[4096];
+                int cfg;
+                while (std::fscanf(fp, "%4095s %d", key_buf, &cfg) == 2) g_tune[key_buf] = cfg;
+                std::fclose(fp);
+            }
+        }
+    }
+    auto it = g_tune.find(key);
+    return it == g_tune.end() ? -1 : it->second;
+}
+
+void tune_record(const std::string &key, int cfg) {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    g_tune[key] = cfg;
+    if (const char *f = tune_file()) {
+        if (FILE *fp = std::fopen(f, "a")) {
+            std::fprintf(fp, "%s %d\n", key.c_str(), cfg);
+            std::fclose(fp);
+        }
+    }
 }
 
 }  // namespace
@@ -290,6 +425,7 @@ int srg_scene_run_stages(srg_scene *s, int stages, void *stream) {
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     int rc = SRG_OK;
     if (stages & 1) rc = enqueue_centres(s, st);
+    if (!rc && (stages & 2)) rc = enqueue_oversample(s, st);
     if (!rc && (stages & 2)) rc = enqueue_backprojection(s, st);
     if (!rc && (stages & 4) && s->scene) SCK(merge(s, st));
     return rc;
@@ -327,15 +463,60 @@ int srg_scene_terms(srg_scene *s, int64_t *terms) {
     return SRG_OK;
 }
 
-int srg_scene_tune(srg_scene *s, int iters, int *best_cfg, double *best_ms) {
+int srg_scene_autotune(srg_scene *s, const srg_tune_request *req, srg_tune_result *res) {
     if (!s) return fail(SRG_E_ARG, "null plan");
-    if (iters < 1) iters = 3;
+    srg_tune_request q{};
+    q.iters = 3;
+    q.use_cache = 1;
+    if (req) q = *req;
+    if (q.iters < 1) q.iters = 3;
+    srg_tune_result r{};
+    r.tile_cfg = -1;
+    r.ms = -1.0;
+    r.err_linear = r.err_oversampled = -1.0;
     cudaStream_t st = nullptr;
     SCK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    int rc = SRG_OK;
+    // Interpolation: the reference's linear interpolation of the original
+    // lines when its estimated phase error is within the budget, else the
+    // 2x-oversampled lines (srg_interp_error, from a sample of every burst's
+    // lines; the error powers of the bursts are averaged).
+    if (q.interp_budget > 0.0) {
+        double pl = 0.0, po = 0.0;
+        for (int i = 0; i < s->n && rc == SRG_OK; ++i) {
+            const srg_burst_desc &d = s->descs[i];
+            const int S = d.nbins > 0 ? d.nbins : d.S;
+            double el = 0.0, eo = 0.0;
+            rc = srg_interp_error(d.burst, d.ldb, d.P, S, std::max(4, 64 / s->n), &el, &eo, st);
+            pl += el * el;
+            po += eo * eo;
+        }
+        if (rc == SRG_OK) {
+            r.err_linear = std::sqrt(pl / s->n);
+            r.err_oversampled = std::sqrt(po / s->n);
+            rc = set_interp(s, r.err_linear <= q.interp_budget ? SRG_INTERP_LINEAR
+                                                               : SRG_INTERP_OVERSAMPLED2);
+        }
+    }
+    r.interp = s->interp;
+    const std::string key = rc == SRG_OK ? tune_key(s) : std::string();
+    const int cached = rc == SRG_OK && q.use_cache ? tune_lookup(key) : -1;
+    if (cached >= 0 && cached < kNumKernels && kKernels[cached].form == s->opts.form) {
+        rc = set_kernel(s, cached);
+        if (rc == SRG_OK) {
+            s->opts.tile_cfg = cached;
+            r.tile_cfg = cached;
+            r.from_cache = 1;
+        }
+        cudaStreamDestroy(st);
+        if (res) *res = r;
+        return rc;
+    }
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    int rc = enqueue_centres(s, st);
+    if (rc == SRG_OK) rc = enqueue_centres(s, st);
+    if (rc == SRG_OK) rc = enqueue_oversample(s, st);
     if (rc == SRG_OK && cudaStreamSynchronize(st) != cudaSuccess)
         rc = fail(SRG_E_CUDA, "azimuth centres failed: %s", cudaGetErrorString(cudaGetLastError()));
     int best = -1;
@@ -345,7 +526,7 @@ int srg_scene_tune(srg_scene *s, int iters, int *best_cfg, double *best_ms) {
         if ((rc = set_kernel(s, idx))) break;
         if ((rc = enqueue_backprojection(s, st))) break;  // warm-up
         float tot = 0.f;
-        for (int it = 0; it < iters && rc == SRG_OK; ++it) {
+        for (int it = 0; it < q.iters && rc == SRG_OK; ++it) {
             cudaEventRecord(e0, st);
             rc = enqueue_backprojection(s, st);
             cudaEventRecord(e1, st);
@@ -355,7 +536,7 @@ int srg_scene_tune(srg_scene *s, int iters, int *best_cfg, double *best_ms) {
             tot += ms;
         }
         if (rc) break;
-        const float t = tot / iters;
+        const float t = tot / q.iters;
         if (t < best_t) {
             best_t = t;
             best = idx;
@@ -371,10 +552,31 @@ int srg_scene_tune(srg_scene *s, int iters, int *best_cfg, double *best_ms) {
     rc = set_kernel(s, best);
     if (rc) return rc;
     s->opts.tile_cfg = best;
-    if (best_cfg) *best_cfg = best;
-    if (best_ms) *best_ms = best_t;
+    tune_record(key, best);
+    r.tile_cfg = best;
+    r.ms = best_t;
+    if (res) *res = r;
     return SRG_OK;
 }
+
+int srg_scene_tune(srg_scene *s, int iters, int *best_cfg, double *best_ms) {
+    srg_tune_request q{};
+    q.iters = iters;
+    q.use_cache = 1;
+    srg_tune_result r{};
+    const int rc = srg_scene_autotune(s, &q, &r);
+    if (rc) return rc;
+    if (best_cfg) *best_cfg = r.tile_cfg;
+    if (best_ms) *best_ms = r.ms;
+    return SRG_OK;
+}
+
+int srg_scene_set_interp(srg_scene *s, int interp) {
+    if (!s) return fail(SRG_E_ARG, "null plan");
+    return set_interp(s, interp);
+}
+
+int srg_scene_interp(const srg_scene *s) { return s ? s->interp : -1; }
 
 int srg_scene_set_shape(srg_scene *s, int tile_cfg) {
     if (!s) return fail(SRG_E_ARG, "null plan");
@@ -398,6 +600,7 @@ int srg_scene_shape(const srg_scene *s) { return s ? s->kernel : -1; }
 void srg_scene_destroy(srg_scene *s) {
     if (!s) return;
     drop_graph(s);
+    for (float2 *p : s->os_lines) cudaFree(p);
     cudaFree(s->d_bursts);
     cudaFree(s->d_tmaps);
     cudaFree(s->d_jobs);

@@ -1,0 +1,88 @@
+"""Parity at the benchmark's own sizes: the IW1-sized burst (configuration 1:
+1,500 pulses x 21,000 bins onto 2,400 x 1,200 over the volcano DEM with fBm
+relief, forward-projected scatterers) and one burst of each subswath of the
+IW scene (configuration 3: S = 18,000 / 21,500 / 25,600, uneven P, their
+sub-grids of the shared DEM), every compiled kernel shape of both forms
+against the oracle's C restatement of the reference (GPU arithmetic:
+FP32 interpolation, 1/(azend - azstart) scaling; OpenMP on every host core).
+
+Bounds, as for the small cases: the FP64 form to FP32 rounding (rel 2e-6)
+with the identical set of formed pixels, and exact term counts; the split
+form within the design's 1 mrad RMS phase error.  The split form's largest
+errors sit at pixels of low amplitude (its absolute error is uniform, so the
+phase error scales as 1 / amplitude): the test bounds the largest phase
+error at pixels above half the RMS amplitude, and the largest absolute error
+relative to the RMS amplitude, each by the measured value with room."""
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import phase_amp_errors, rel_err
+from srg_b200 import _lib, api, workloads
+
+pytestmark = pytest.mark.gpu
+SPLIT_CFGS = [c[0] for c in _lib.tile_configs() if c[1] == _lib.FORM_SPLIT]
+FP64_CFGS = [c[0] for c in _lib.tile_configs() if c[1] == _lib.FORM_FP64]
+CASES = ["c1", "iw0", "iw1", "iw2"]
+
+FP64_REL = 2e-6
+SPLIT_PH_RMS_MRAD = 1.0
+SPLIT_PH_MAX_HALF_RMS_MRAD = 1.0     # largest phase error at pixels above 0.5 x RMS amplitude
+SPLIT_ABS_MAX_OVER_RMS = 1e-4        # largest |split - oracle| / RMS amplitude
+
+
+@pytest.fixture(scope="module")
+def cases():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("the CUDA path needs a GPU; none is visible")
+    orc = O.Oracle()
+    out = {}
+    wl = workloads.config1()
+    grid, iw = workloads.iw_bursts((0, 1, 2))
+    for name, db in zip(CASES, [wl.bursts[0]] + iw):
+        b = db.b
+        b.burst = db.burst.cpu().numpy()
+        st = orc.stages(b, gpu_lerp=1, gpu_scale=1)
+        b.burst = np.zeros((0, b.burst.shape[1]), np.complex64)   # free the host copy
+        fp = db.out_pix0
+        ref = np.ascontiguousarray(st["out"][:, fp:fp + db.out.shape[1]])
+        out[name] = (db, ref, st["terms"])
+    return out
+
+
+def run(db, form, cfg):
+    db.out.fill_(complex(7.0, 7.0))
+    api.backproject([db], form=form, tile_cfg=cfg)
+    return db.out.cpu().numpy()
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_term_count_full_size(cases, name):
+    db, ref, terms = cases[name]
+    assert terms > 1e8
+    assert api.count_terms([db]) == terms
+
+
+@pytest.mark.parametrize("cfg", FP64_CFGS)
+@pytest.mark.parametrize("name", CASES)
+def test_fp64_form_full_size(cases, name, cfg):
+    db, ref, _ = cases[name]
+    got = run(db, _lib.FORM_FP64, cfg)
+    assert np.array_equal(got != 0, ref != 0)
+    assert rel_err(got, ref) < FP64_REL
+
+
+@pytest.mark.parametrize("cfg", SPLIT_CFGS)
+@pytest.mark.parametrize("name", CASES)
+def test_split_form_full_size(cases, name, cfg):
+    db, ref, _ = cases[name]
+    got = run(db, _lib.FORM_SPLIT, cfg)
+    assert np.array_equal(got != 0, ref != 0)
+    e = phase_amp_errors(got, ref)
+    assert e["ph_rms"] < SPLIT_PH_RMS_MRAD, e
+    h = phase_amp_errors(got, ref, floor_frac=0.5)
+    assert h["ph_max"] < SPLIT_PH_MAX_HALF_RMS_MRAD, h
+    amp = np.abs(ref)
+    rms = np.sqrt(np.mean(amp[amp > 0] ** 2))
+    assert np.abs(got.astype(np.complex128) - ref).max() / rms < SPLIT_ABS_MAX_OVER_RMS

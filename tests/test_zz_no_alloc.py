@@ -66,6 +66,40 @@ def test_noalloc_matches_allocating_entry_on_consecutive_calls(torch_cuda, form)
             assert np.all(full[:, outside] == sentinel)
 
 
+def test_noalloc_allocates_nothing(torch_cuda):
+    """After the first call on a device (which may load the kernels), calls
+    leave the device's free memory exactly as they found it: nothing is
+    allocated, by the library or by torch (the buffers exist before the
+    calls, and the calls go through ctypes)."""
+    torch = torch_cuda
+    b = mini_case("tops")
+    db = api.to_device(b)
+    for form in (_lib.FORM_SPLIT, _lib.FORM_FP64):
+        assert call_noalloc(torch, db, form) == _lib.SRG_OK, _lib.last_error()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(3):
+        for form in (_lib.FORM_SPLIT, _lib.FORM_FP64):
+            assert call_noalloc(torch, db, form) == _lib.SRG_OK, _lib.last_error()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+
+
+def test_noalloc_refuses_host_centres_like_the_allocating_entry(torch_cuda):
+    torch = torch_cuda
+    b = mini_case("flat")
+    db = api.to_device(b)
+    o = _lib.default_options(_lib.FORM_SPLIT)
+    o.centres_on_host = 1
+    d = db.desc()
+    st = torch.cuda.current_stream().cuda_stream
+    rc = _lib.lib().srg_bp_burst_device_noalloc(C.byref(d), C.byref(o), C.c_void_p(st))
+    assert rc == _lib.SRG_E_UNSUPPORTED
+    rc2 = _lib.lib().srg_bp_bursts_device(C.byref(d), 1, C.byref(o), C.c_void_p(st))
+    assert rc2 == _lib.SRG_E_UNSUPPORTED
+
+
 def test_noalloc_rejects_bursts_beyond_its_scratch(torch_cuda):
     torch = torch_cuda
     b = mini_case("flat")
