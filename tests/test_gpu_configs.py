@@ -42,6 +42,7 @@ def cases():
     grid, iw = workloads.iw_bursts((0, 1, 2))
     for name, db in zip(CASES, [wl.bursts[0]] + iw):
         b = db.b
+        b.pulses = b.rawdatalines
         b.burst = db.burst.cpu().numpy()
         st = orc.stages(b, gpu_lerp=1, gpu_scale=1)
         b.burst = np.zeros((0, b.burst.shape[1]), np.complex64)   # free the host copy
