@@ -180,8 +180,16 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 // GATE: the range lines may still be uploading (BurstDev::ready); the
 // producer waits for each chunk's rows.  A separate instantiation, because
 // the wait's code alone costs the ungated kernel ~4 % (measured).
+// Registers per thread that let MINB blocks of (NC + 1) warps share an SM's
+// 65,536 (a multiple of 8, the allocation unit): 136 for 3 blocks of 5 warps,
+// where __launch_bounds__'s minimum-blocks form allowed 128 and spilled.
+template <int NC, int MINB>
+constexpr int ws_max_regs() {
+    return (65536 / (MINB * (NC + 1) * 32)) / 8 * 8;
+}
+
 template <int FORM, int TX, int TY, int NC, int CK, int NS, int WB, int MINB, bool GATE = false>
-__global__ void __launch_bounds__((NC + 1) * 32, MINB)
+__global__ void __launch_bounds__((NC + 1) * 32) __maxnreg__((ws_max_regs<NC, MINB>()))
 bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
       const CUtensorMap *__restrict__ tmaps, int *__restrict__ work_counter,
       int *__restrict__ err, int /* window, = WB */, const int *__restrict__ tile_list) {

@@ -8,11 +8,12 @@ FP32 interpolation, 1/(azend - azstart) scaling; OpenMP on every host core).
 
 Bounds, as for the small cases: the FP64 form to FP32 rounding (rel 2e-6)
 with the identical set of formed pixels, and exact term counts; the split
-form within the design's 1 mrad RMS phase error.  The split form's largest
-errors sit at pixels of low amplitude (its absolute error is uniform, so the
-phase error scales as 1 / amplitude): the test bounds the largest phase
-error at pixels above half the RMS amplitude, and the largest absolute error
-relative to the RMS amplitude, each by the measured value with room."""
+form within the design's 1 mrad RMS phase error (measured 0.009 mrad RMS on
+the IW1 burst, 0.02 on the IW bursts).  Its largest phase errors sit at
+pixels of low amplitude, 5-15 % of the RMS (a phase error is the absolute
+error over the amplitude): over every shape and case the measured maxima
+were 2.2 mrad at pixels above 5 % of the RMS amplitude and 0.41 mrad above
+half of it, bounded here by 5 and 1 mrad."""
 import numpy as np
 import pytest
 
@@ -27,8 +28,9 @@ CASES = ["c1", "iw0", "iw1", "iw2"]
 
 FP64_REL = 2e-6
 SPLIT_PH_RMS_MRAD = 1.0
+SPLIT_PH_MAX_MRAD = 5.0              # largest phase error at pixels above 0.05 x RMS amplitude
 SPLIT_PH_MAX_HALF_RMS_MRAD = 1.0     # largest phase error at pixels above 0.5 x RMS amplitude
-SPLIT_ABS_MAX_OVER_RMS = 1e-4        # largest |split - oracle| / RMS amplitude
+SPLIT_AMP_RMS = 1e-3                 # RMS relative amplitude error
 
 
 @pytest.fixture(scope="module")
@@ -82,8 +84,7 @@ def test_split_form_full_size(cases, name, cfg):
     assert np.array_equal(got != 0, ref != 0)
     e = phase_amp_errors(got, ref)
     assert e["ph_rms"] < SPLIT_PH_RMS_MRAD, e
+    assert e["ph_max"] < SPLIT_PH_MAX_MRAD, e
+    assert e["amp_rms"] < SPLIT_AMP_RMS, e
     h = phase_amp_errors(got, ref, floor_frac=0.5)
     assert h["ph_max"] < SPLIT_PH_MAX_HALF_RMS_MRAD, h
-    amp = np.abs(ref)
-    rms = np.sqrt(np.mean(amp[amp > 0] ** 2))
-    assert np.abs(got.astype(np.complex128) - ref).max() / rms < SPLIT_ABS_MAX_OVER_RMS
