@@ -180,16 +180,8 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 // GATE: the range lines may still be uploading (BurstDev::ready); the
 // producer waits for each chunk's rows.  A separate instantiation, because
 // the wait's code alone costs the ungated kernel ~4 % (measured).
-// Registers per thread that let MINB blocks of (NC + 1) warps share an SM's
-// 65,536 (a multiple of 8, the allocation unit): 136 for 3 blocks of 5 warps,
-// where __launch_bounds__'s minimum-blocks form allowed 128 and spilled.
-template <int NC, int MINB>
-constexpr int ws_max_regs() {
-    return (65536 / (MINB * (NC + 1) * 32)) / 8 * 8;
-}
-
 template <int FORM, int TX, int TY, int NC, int CK, int NS, int WB, int MINB, bool GATE = false>
-__global__ void __launch_bounds__((NC + 1) * 32) __maxnreg__((ws_max_regs<NC, MINB>()))
+__global__ void __launch_bounds__((NC + 1) * 32, MINB)
 bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
       const CUtensorMap *__restrict__ tmaps, int *__restrict__ work_counter,
       int *__restrict__ err, int /* window, = WB */, const int *__restrict__ tile_list) {
@@ -469,6 +461,11 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
             const double dev_scale = (double)__int_as_float(ctl.dmax_bits) * B.inv_dmrg;
             const double *satl = B.satloc;
             const int Pm1 = B.P - 1;
+            // burst constants of the chunk loop held in registers: the loop's
+            // barrier waits clobber memory, so fields read from the descriptor
+            // inside it would be loaded again on every chunk
+            const double rng0 = B.rngstart, idmrg = B.inv_dmrg, Kc = B.K;
+            const int tmap_i = B.tmap, bin0 = B.bin0;
             // upload gate (GATE only), held in registers with the last value seen
             const int *const ready = GATE ? B.ready : nullptr;
             const int ready_base = GATE ? B.ready_base : 0, ready_rows = GATE ? B.ready_rows : 1;
@@ -507,7 +504,7 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                 const double nx = __shfl_down_sync(0xffffffffu, ex, 1);
                 const double ny = __shfl_down_sync(0xffffffffu, ey, 1);
                 const double nz = __shfl_down_sync(0xffffffffu, ez, 1);
-                const double rbabs = (R - B.rngstart) * B.inv_dmrg;
+                const double rbabs = (R - rng0) * idmrg;
                 const bool act = lane < nk;
                 // deviation of the look vector from the tile's straight line
                 const double f = (double)(k - kmin) * span;
@@ -549,7 +546,7 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                 float pb = 0.f;
                 if constexpr (FORM == FORM_SPLIT) {
                     {
-                        const double q = R * B.K;
+                        const double q = R * Kc;
                         pa = make_float4(__double2float_rn(nx - ex), __double2float_rn(ny - ey),
                                          __double2float_rn(nz - ez), __double2float_rn(kTwoPi * (q - rint(q))));
                         pb = __double2float_rn(rbabs - (double)x0);
@@ -592,13 +589,13 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                     const double cR = Ra + (((double)c2 * djc - (double)c1) * djc + (double)c0);
                     const double cD1 = (double)c1 + (double)c2 * (1.0 - 2.0 * djc);
                     const double cD2 = 2.0 * (double)c2;
-                    const double q = cR * B.K;
-                    hv.r0 = __double2float_rn((cR - B.rngstart) * B.inv_dmrg - (double)x0);
-                    hv.r1 = __double2float_rn(cD1 * B.inv_dmrg);
-                    hv.r2 = __double2float_rn(cD2 * B.inv_dmrg);
+                    const double q = cR * Kc;
+                    hv.r0 = __double2float_rn((cR - rng0) * idmrg - (double)x0);
+                    hv.r1 = __double2float_rn(cD1 * idmrg);
+                    hv.r2 = __double2float_rn(cD2 * idmrg);
                     hv.p0 = __double2float_rn(kTwoPi * (q - rint(q)));
-                    hv.p1 = __double2float_rn(kTwoPi * B.K * cD1);
-                    hv.p2 = __double2float_rn(kTwoPi * B.K * cD2);
+                    hv.p1 = __double2float_rn(kTwoPi * Kc * cD1);
+                    hv.p2 = __double2float_rn(kTwoPi * Kc * cD2);
                     hv.u0x = u0[0];
                     hv.u0y = u0[1];
                     hv.u0z = u0[2];
@@ -607,7 +604,7 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                     hv.usz = us[2];
                     const float resmax =
                         __int_as_float(__reduce_max_sync(0xffffffffu, __float_as_int(act ? err : 0.f)));
-                    hv.poly = (nk >= 3 && (double)resmax * kTwoPi * B.K < kPolyTolRad) ? 1 : 0;
+                    hv.poly = (nk >= 3 && (double)resmax * kTwoPi * Kc < kPolyTolRad) ? 1 : 0;
                 }
                 if (!mbar_wait_bounded(&ctl.empty[s], (r & 1) ^ 1, ctl.spin)) {
                     ctl.abort = 1;
@@ -634,11 +631,11 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                 // without arriving; the phase still needs all 32 lane arrivals
                 // below, which follow those writes.
                 if (lane == 0 && use_tma) {
-                    if (c == 0) fence_tensormap_acquire(tmaps + B.tmap);
+                    if (c == 0) fence_tensormap_acquire(tmaps + tmap_i);
                     fence_proxy_async_shared();
                     mbar_expect_tx(&ctl.full[s], (uint32_t)(WB * CK * 8));
-                    tma_load_2d(samp0 + (size_t)s * CK * WB, tmaps + B.tmap, &ctl.full[s],
-                                x0 - B.bin0, k0);
+                    tma_load_2d(samp0 + (size_t)s * CK * WB, tmaps + tmap_i, &ctl.full[s],
+                                x0 - bin0, k0);
                     issued |= 1u << s;
                     issued_par = (issued_par & ~(1u << s)) | ((r & 1u) << s);
                 }
@@ -672,6 +669,9 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
             if (lane == 0) ctl.item = atomicAdd(work_counter, 1);
         } else {
             // ---- consumer warps ----
+            // burst constants in registers (the loop's waits clobber memory)
+            const float invd_c = B.inv_dmrg_f, Kr_c = (float)(kTwoPi * B.K);
+            const double rng0_c = B.rngstart, rmax_c = B.rmax, dmrg_c = B.dmrg, k4pi_c = B.k4pi;
             for (int c = 0; c < nchunks; ++c) {
                 const uint32_t g = gchunk + c;
                 const int s = g % NS;
@@ -686,8 +686,8 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                 const float2 *win = samp0 + (size_t)s * CK * WB;
                 const PP *pp = prm + s * CK;
                 if constexpr (FORM == FORM_SPLIT) {
-                    const float invd = B.inv_dmrg_f;
-                    const float Kr = (float)(kTwoPi * B.K);
+                    const float invd = invd_c;
+                    const float Kr = Kr_c;
                   if (h.fast && h.poly) {
                     // Closed forms.  Within the chunk the pixel's range offset from
                     // R_c advances by dw_j = d.(u0 + j us) + g (g: slope of the folded
@@ -900,7 +900,7 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                         cph[m] = fmaf(-nr, kTwoPiLo, fmaf(-nr, kTwoPiHi, cph[m]));
                     }
                 } else {
-                    const double rs = B.rngstart, rmx = B.rmax, dm = B.dmrg, k4 = B.k4pi;
+                    const double rs = rng0_c, rmx = rmax_c, dm = dmrg_c, k4 = k4pi_c;
                     const int x0 = h.x0;
                     const bool fast = h.fast && h.interior;
                     for (int j = 0; j < nk; ++j) {
