@@ -123,20 +123,40 @@ __global__ void count_terms_kernel(BurstDev B, unsigned long long *terms) {
 // difference of R_k^2 turns non-negative, found by bisection; the pixel's
 // bins lie between those of its smallest and largest range (+1 for the
 // second tap).  band[0] / band[1] are lowered / raised to the extremes over
-// all formed pixels (preset to INT_MAX / INT_MIN by the caller).
-__global__ void range_band_kernel(BurstDev B, int *band) {
+// all formed pixels (preset to INT_MAX / INT_MIN by the caller).  A block
+// takes a patch of kBandLines x kBandCols pixels and evaluates the latitude
+// and longitude sines and cosines once per line and column of it.
+constexpr int kBandLines = 8, kBandCols = 64;
+__global__ void __launch_bounds__(256) range_band_kernel(BurstDev B, int *band) {
+    __shared__ double lt[kBandLines][4], ct[kBandCols][2];
     const int nx = B.lastpix_eff - B.firstpix + 1;
-    const long long npix = (long long)nx * B.nlines;
+    const int l0 = blockIdx.y * kBandLines, c0 = blockIdx.x * kBandCols;
+    const int t = threadIdx.x;
+    if (t < kBandLines) {
+        if (l0 + t < B.nlines) {
+            const LineTrig L = line_trig(B, l0 + t);
+            lt[t][0] = L.slat;
+            lt[t][1] = L.clat;
+            lt[t][2] = L.re;
+            lt[t][3] = L.rez;
+        }
+    } else if (t < kBandLines + kBandCols) {
+        const int c = t - kBandLines;
+        if (c0 + c < nx) col_trig(B, B.firstpix + c0 + c, ct[c][0], ct[c][1]);
+    }
+    __syncthreads();
     int lo = INT_MAX, hi = INT_MIN;
-    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < npix;
-         idx += (long long)gridDim.x * blockDim.x) {
-        const int line = (int)(idx / nx);
-        const int px = B.firstpix + (int)(idx - (long long)line * nx);
+    for (int q = t; q < kBandLines * kBandCols; q += blockDim.x) {
+        const int yl = q / kBandCols, xc = q - yl * kBandCols;
+        const int line = l0 + yl, col = c0 + xc;
+        if (line >= B.nlines || col >= nx) continue;
+        const int px = B.firstpix + col;
         int azs, aze;
         pixel_window(B, pixel_azoff(B, B.coef + 3 * line, px), azs, aze);
         if (aze <= azs) continue;
         double X[3];
-        pixel_ecef(B, line, px, (double)B.dem[(long long)line * B.dem_ld + px], X[0], X[1], X[2]);
+        pixel_ecef_from(lt[yl][0], lt[yl][1], lt[yl][2], lt[yl][3], ct[xc][0], ct[xc][1],
+                        (double)B.dem[(long long)line * B.dem_ld + px], X[0], X[1], X[2]);
         auto r2 = [&](int k) {
             const double *s = B.satloc + 3 * k;
             const double vx = X[0] - s[0], vy = X[1] - s[1], vz = X[2] - s[2];
@@ -587,10 +607,11 @@ cudaError_t launch_merge_scene(const BurstDev *bursts, int n, float2 *dst, long 
 }
 
 cudaError_t launch_range_band(const BurstDev &B, int *band, int sms, cudaStream_t st) {
-    const long long npix = (long long)(B.lastpix_eff - B.firstpix + 1) * B.nlines;
-    if (npix <= 0) return cudaSuccess;
-    const long long blocks = std::min<long long>((npix + 255) / 256, (long long)sms * 8);
-    range_band_kernel<<<(int)blocks, 256, 0, st>>>(B, band);
+    (void)sms;
+    const int nx = B.lastpix_eff - B.firstpix + 1;
+    if (nx <= 0 || B.nlines <= 0) return cudaSuccess;
+    const dim3 grid((nx + kBandCols - 1) / kBandCols, (B.nlines + kBandLines - 1) / kBandLines);
+    range_band_kernel<<<grid, 256, 0, st>>>(B, band);
     return cudaGetLastError();
 }
 
