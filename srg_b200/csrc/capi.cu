@@ -17,6 +17,9 @@
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <unistd.h>
+#if defined(__x86_64__)
+#include <immintrin.h>
+#endif
 
 #include <algorithm>
 #include <climits>
@@ -350,6 +353,29 @@ int ensure_dropin(DevCtx &c) {
 using namespace srg::detail;
 
 namespace {
+
+// Copy of n bytes whose stores bypass the CPU caches (16-byte streaming
+// stores where the target is aligned; plain bytes at the two ends).  The
+// stores are ordered against later ones only after store_fence().
+void copy_nontemporal(char *dst, const char *src, size_t n) {
+#if defined(__x86_64__)
+    size_t i = 0;
+    const size_t head = std::min(n, (16 - (reinterpret_cast<uintptr_t>(dst) & 15)) & 15);
+    for (; i < head; ++i) dst[i] = src[i];
+    for (; i + 16 <= n; i += 16)
+        _mm_stream_si128(reinterpret_cast<__m128i *>(dst + i),
+                         _mm_loadu_si128(reinterpret_cast<const __m128i *>(src + i)));
+    for (; i < n; ++i) dst[i] = src[i];
+#else
+    std::memcpy(dst, src, n);
+#endif
+}
+
+void store_fence() {
+#if defined(__x86_64__)
+    _mm_sfence();
+#endif
+}
 
 // Range lines that are still being copied in granules of `rows` pulse rows:
 // the copy stream raises `*word` to base + n once the first n granules are in.
@@ -934,13 +960,18 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     int16_t *slab = static_cast<int16_t *>(c->host_stage);
     std::atomic<int> io_err{0};
     const int ntask = std::max(1, std::min(nl, 4 * HostPool::threads()));
+    // Each row is read into a small buffer of the thread's own and moved into
+    // the pinned slab with non-temporal stores: a slab written through the CPU
+    // caches leaves its lines dirty in many cores' caches, and the DMA that
+    // follows then copies at about a seventh of the rate it reaches on lines
+    // held in memory only (0.7 ms against 0.1 ms for a 5 MB box).
     pool.run(ntask, [&](int t) {
         const size_t want = (size_t)ncols * 2;
+        std::vector<char> row(want);
         for (int r = (int)((long long)nl * t / ntask); r < (int)((long long)nl * (t + 1) / ntask); ++r) {
-            char *dst = reinterpret_cast<char *>(slab + (size_t)r * ncols);
             size_t done = 0;
             while (done < want) {   // pread may return fewer bytes than asked
-                const ssize_t got = pread(fddem, dst + done, want - done,
+                const ssize_t got = pread(fddem, row.data() + done, want - done,
                                           ((off_t)(fl + r) * W + fp_eff) * 2 + (off_t)done);
                 if (got <= 0) {
                     io_err = got < 0 ? 1 : 2;
@@ -948,7 +979,9 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
                 }
                 done += (size_t)got;
             }
+            copy_nontemporal(reinterpret_cast<char *>(slab + (size_t)r * ncols), row.data(), want);
         }
+        store_fence();
     });
     if (io_err) {
         drain();
