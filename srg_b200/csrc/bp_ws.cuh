@@ -54,7 +54,9 @@
 
 namespace srg {
 
-struct StageHdr {
+// 16-byte aligned: the consumers read it with vector loads (a quarter of the
+// scalar loads per chunk).
+struct __align__(16) StageHdr {
     int x0;        // first staged bin
     int fast;      // 1: every tap of the chunk lies in the staged window and the range limits
     int interior;  // 1: the chunk lies inside every formed pixel's azimuth window
@@ -89,6 +91,15 @@ constexpr float kInvTwoPi = 0.159154943091895336f;
 // (quadratic R_c, linear look-vector increments) before it falls back to the
 // per-pulse form; the fit residuals of a smooth orbit are ~1e-8 rad.
 constexpr double kPolyTolRad = 1e-4;
+
+// 1/n for the pulse counts of a chunk (n <= 32), rounded to nearest: the
+// producer's fits multiply by these instead of dividing (an IEEE division is
+// a dependent sequence of about ten instructions on the producer's path).
+__constant__ float kRecipSmall[33] = {
+    0.f,        1.f / 1,  1.f / 2,  1.f / 3,  1.f / 4,  1.f / 5,  1.f / 6,  1.f / 7,  1.f / 8,
+    1.f / 9,    1.f / 10, 1.f / 11, 1.f / 12, 1.f / 13, 1.f / 14, 1.f / 15, 1.f / 16, 1.f / 17,
+    1.f / 18,   1.f / 19, 1.f / 20, 1.f / 21, 1.f / 22, 1.f / 23, 1.f / 24, 1.f / 25, 1.f / 26,
+    1.f / 27,   1.f / 28, 1.f / 29, 1.f / 30, 1.f / 31, 1.f / 32};
 
 // floor(t) for -2^22 <= t < 2^22 without the conversion pipe: adding 1.5 * 2^23
 // rounded toward -inf leaves floor(t) in the low mantissa bits.
@@ -193,6 +204,9 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
     static_assert(TX % PBX == 0 && TY % PBY == 0 && (TX / PBX) * (TY / PBY) == NC * M, "tile / warp map");
     static_assert(CK < 32, "the producer warp covers CK + 1 pulses");
     static_assert(NS >= 2 && NS <= 4, "stage ring");
+    // every stage's TMA destination on a 128-byte boundary (the first stage
+    // starts on a 1024-byte one), and the box rows a multiple of 16 bytes
+    static_assert((CK * WB * 8) % 128 == 0 && WB % 2 == 0, "stage stride");
     using PP = PulseParams<FORM>;
 
     extern __shared__ __align__(128) unsigned char dsm[];
@@ -466,6 +480,7 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
             // inside it would be loaded again on every chunk
             const double rng0 = B.rngstart, idmrg = B.inv_dmrg, Kc = B.K;
             const int tmap_i = B.tmap, bin0 = B.bin0;
+            const float idmrg_f = (float)idmrg, kpk_f = (float)(kTwoPi * Kc);
             // upload gate (GATE only), held in registers with the last value seen
             const int *const ready = GATE ? B.ready : nullptr;
             const int ready_base = GATE ? B.ready_base : 0, ready_rows = GATE ? B.ready_rows : 1;
@@ -535,9 +550,9 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                     hv.dmx = __double2float_rn(__shfl_sync(0xffffffffu, nx - ex, nk / 2));
                     hv.dmy = __double2float_rn(__shfl_sync(0xffffffffu, ny - ey, nk / 2));
                     hv.dmz = __double2float_rn(__shfl_sync(0xffffffffu, nz - ez, nk / 2));
-                    const float rm = (float)Rmid;
-                    hv.inv2R = 0.5f / rm;
-                    hv.c2 = hv.inv2R / rm;
+                    const float rm = (float)Rmid, irm = __frcp_rn(rm);
+                    hv.inv2R = 0.5f * irm;
+                    hv.c2 = hv.inv2R * irm;
                 }
                 hv.poly = 0;
                 hv.r0 = hv.r1 = hv.r2 = hv.p0 = hv.p1 = hv.p2 = 0.f;
@@ -566,15 +581,15 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                     float u0[3], us[3];
                     const float pq[3] = {pa.x, pa.y, pa.z};
                     if (nk >= 3) {
-                        const float D1 = dRm / (float)jm;
-                        const float D2 = ((dRb - dRm) / (float)(jb - jm) - D1) / (float)jb;
+                        const float D1 = dRm * kRecipSmall[jm];
+                        const float D2 = ((dRb - dRm) * kRecipSmall[jb - jm] - D1) * kRecipSmall[jb];
                         c2 = D2;
                         c1 = fmaf(D2, 2.f * jc - (float)jm, D1);
                         c0 = fmaf(jc * (jc - (float)jm), D2, jc * D1);
                     }
                     const float fj = (float)lane - jc;
                     float err = fabsf(dR - fmaf(fmaf(c2, fj, c1), fj, c0));
-                    const float ij = nk >= 3 ? 1.f / (float)jb : 0.f;
+                    const float ij = nk >= 3 ? kRecipSmall[jb] : 0.f;
                     const float dmaxc = (float)nk * __int_as_float(ctl.dmax_bits);
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
@@ -584,18 +599,20 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                         err = fmaf(fabsf(pq[c] - fmaf((float)lane, us[c], u0[c])), dmaxc, err);
                     }
                     // the fitted R_c at the first pulse (f = -jc), its first and
-                    // second forward differences
-                    const double djc = (double)jc;
-                    const double cR = Ra + (((double)c2 * djc - (double)c1) * djc + (double)c0);
-                    const double cD1 = (double)c1 + (double)c2 * (1.0 - 2.0 * djc);
-                    const double cD2 = 2.0 * (double)c2;
+                    // second forward differences.  Only R_c itself needs FP64 (its
+                    // phase); the differences (|dR| < ~0.1 m per pulse) and the
+                    // fit's offset from Ra (< ~2 m) are FP32 quantities already,
+                    // and FP64 steps on them would only lengthen the producer's
+                    // path, which the consumers wait on (measured 1.9 %).
+                    const double cR = Ra + (double)fmaf(fmaf(c2, jc, -c1), jc, c0);
+                    const float fD1 = fmaf(c2, 1.f - 2.f * jc, c1), fD2 = 2.f * c2;
                     const double q = cR * Kc;
                     hv.r0 = __double2float_rn((cR - rng0) * idmrg - (double)x0);
-                    hv.r1 = __double2float_rn(cD1 * idmrg);
-                    hv.r2 = __double2float_rn(cD2 * idmrg);
+                    hv.r1 = fD1 * idmrg_f;
+                    hv.r2 = fD2 * idmrg_f;
                     hv.p0 = __double2float_rn(kTwoPi * (q - rint(q)));
-                    hv.p1 = __double2float_rn(kTwoPi * Kc * cD1);
-                    hv.p2 = __double2float_rn(kTwoPi * Kc * cD2);
+                    hv.p1 = fD1 * kpk_f;
+                    hv.p2 = fD2 * kpk_f;
                     hv.u0x = u0[0];
                     hv.u0y = u0[1];
                     hv.u0z = u0[2];
