@@ -120,16 +120,18 @@ def load_traffic(kernel: str, workload: str):
 # our arm
 
 
-def e2e_dropin(torch, wl, steps, form, separate=False, bursts=None):
+def e2e_dropin(torch, wl, steps, form, separate=False, bursts=None, overlap=0):
     """End to end through azimuth_compress_ (the drop-in C ABI), one call per
     burst in acquisition order as the reference's driver makes them: burst
     lines in pinned host memory, the DEM and the .geo raster as files on tmpfs
     (when it has room, else the temp dir); `separate`: one .geo file per burst
     (a stack of passes) instead of one scene raster; `bursts`: the bursts to
-    run (default: all of the workload's).  Returns (s per step, h2d, d2h bytes
-    per step)."""
+    run (default: all of the workload's); `overlap`: calls overlap (each
+    returns once its lines are on the device; srg_dropin_flush at the end of
+    every step, inside the timed region, waits for the last merges).  Returns
+    (s per step, h2d, d2h bytes per step)."""
     from srg_b200 import api
-    api.set_default_form(form)
+    api.set_default_form(form, overlap=overlap)
     bursts = wl.bursts if bursts is None else bursts
     if not bursts:
         return 0.0, 0, 0
@@ -168,14 +170,18 @@ def e2e_dropin(torch, wl, steps, form, separate=False, bursts=None):
                 h, d = api.dropin_last_bytes()
                 h2d += h
                 d2h += d
+            api.dropin_flush()
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             for _ in range(steps):
                 for call in calls:
                     call()
+                api.dropin_flush()
             torch.cuda.synchronize()
             dt = (time.perf_counter() - t0) / steps
         finally:
+            api.dropin_flush()
+            api.set_default_form(form, overlap=0)
             os.close(fd_dem)
             for fd in fds:
                 os.close(fd)
@@ -595,12 +601,17 @@ def main():
         launches = (4 if own_bursts else 0) + (len(wl.bursts) if rank == 0 else 0)
     if c2 is not None:
         c2["vs_config1_fp64"] = vs_plain_lines(torch, wl, c2.pop("plain_fp64"))
+    # the drop-in with its calls overlapped (SRG_DROPIN_OVERLAP), and with every
+    # call returning after its merge, as the reference's does
     e2e_s, h2d, d2h = e2e_dropin(torch, wl, args.e2e_steps, _lib.FORM_SPLIT,
-                                 separate=args.workload == "c4", bursts=own_bursts)
+                                 separate=args.workload == "c4", bursts=own_bursts, overlap=1)
+    e2e_seq_s, _, _ = e2e_dropin(torch, wl, args.e2e_steps, _lib.FORM_SPLIT,
+                                 separate=args.workload == "c4", bursts=own_bursts, overlap=0)
     h2d_gbs = pinned_h2d_gbs(torch)
     # whole job: the slowest rank's times, every rank's terms and bytes
-    (s_ms, d_ms, e2e_s), (terms_all, h2d, d2h) = combine_ranks(
-        torch, dist if world > 1 else None, "cuda", [s_ms, d_ms, e2e_s], [terms_rank, h2d, d2h])
+    (s_ms, d_ms, e2e_s, e2e_seq_s), (terms_all, h2d, d2h) = combine_ranks(
+        torch, dist if world > 1 else None, "cuda", [s_ms, d_ms, e2e_s, e2e_seq_s],
+        [terms_rank, h2d, d2h])
     terms_all, h2d, d2h = int(terms_all), int(h2d), int(d2h)
     value = terms_all / (s_ms * 1e-3) / 1e9
     fp64_value = terms_all / (d_ms * 1e-3) / 1e9
@@ -647,8 +658,12 @@ def main():
                 "d2h_bytes_per_step": d2h, "s_per_step": e2e_s,
                 "pinned_h2d_gbs": h2d_gbs,
                 "h2d_bound_s_per_step": h2d / world / (h2d_gbs * 1e9),
-                "path": "azimuth_compress_ (33-arg C ABI), pinned host burst, tmpfs DEM/.geo"
-                        + (" (one .geo per pass)" if args.workload == "c4" else "")},
+                "path": "azimuth_compress_ (33-arg C ABI), pinned host burst, tmpfs DEM/.geo, "
+                        "calls overlapped (SRG_DROPIN_OVERLAP=1: a call returns once its lines "
+                        "are on the device; srg_dropin_flush ends every step)"
+                        + (" (one .geo per pass)" if args.workload == "c4" else ""),
+                "calls_not_overlapped": {"value": terms_all / e2e_seq_s / 1e9,
+                                         "s_per_step": e2e_seq_s}},
         "gpu_launches": launches * args.steps,
         "clocks": clk.summary(),
         "setup_s": wl.setup_s,

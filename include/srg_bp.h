@@ -53,11 +53,24 @@ typedef struct srg_bp_options {
                           hold (range lines, orbit, DEM box, output box, work
                           list); a call needing more returns SRG_E_NOMEM before
                           any GPU work; 0: no limit */
+    int overlap;       /* drop-in: 1 returns once the call's range lines are
+                          on the device; the end of its sum, the copy back and
+                          the merge into *fdout finish behind the caller (in
+                          call order, on a descriptor duplicated from fdout),
+                          while the next call reads its DEM box and uploads.
+                          A failure of that part is returned by the next call
+                          on the device or by srg_dropin_flush().  The merge
+                          into *fdout of a call is complete when the next
+                          call without overlap, srg_dropin_flush() or the
+                          process's normal exit returns.  0 (default): every
+                          call returns with its merge done, as the reference.
+                          The environment variable SRG_DROPIN_OVERLAP=1 sets
+                          it in the process-wide defaults. */
 } srg_bp_options;
 
 /* Fill *o with the defaults (split form, tuned tile, current device,
  * centres on the GPU, quiet, default wait limit, range band, no scratch
- * limit). */
+ * limit, calls not overlapped unless SRG_DROPIN_OVERLAP=1). */
 void srg_bp_default_options(srg_bp_options *o);
 
 /* Message of the last failing call on this thread ("" if none). */
@@ -115,6 +128,12 @@ void srg_set_default_options(const srg_bp_options *o);
  * box and the azimuth centres before the lines go up; the reference uploads
  * every line in full (azimuth_compress.cu:367-368). */
 int srg_dropin_last_bytes(int device, long long *h2d, long long *d2h);
+
+/* Waits until every overlapped drop-in call on `device` (-1: every device)
+ * has finished its merge; returns the first failure among them not yet
+ * returned by a later call (message in srg_last_error()), else SRG_OK.
+ * Runs by itself at the process's normal exit. */
+int srg_dropin_flush(int device);
 
 /* ------------------------------------------------------------------------
  * Per-burst scalars of the azimuth_compress_ call, derived as

@@ -32,7 +32,7 @@ _ip = C.POINTER(C.c_int)
 class Options(C.Structure):
     _fields_ = [("form", C.c_int), ("tile_cfg", C.c_int), ("device", C.c_int),
                 ("centres_on_host", C.c_int), ("verbose", C.c_int), ("spin_limit", C.c_int),
-                ("full_lines", C.c_int), ("scratch_limit", C.c_longlong)]
+                ("full_lines", C.c_int), ("scratch_limit", C.c_longlong), ("overlap", C.c_int)]
 
 
 class BurstDesc(C.Structure):
@@ -98,6 +98,7 @@ _SIGS = {
     "srg_bp_burst_device_gated": (C.c_int, [C.POINTER(BurstDesc), C.c_void_p, C.c_int, C.c_int,
                                             C.POINTER(Options), C.c_void_p]),
     "srg_test_set_dropin_sequence": (C.c_int, [C.c_int, C.c_int]),
+    "srg_dropin_flush": (C.c_int, [C.c_int]),
     "srg_dropin_last_bytes": (C.c_int, [C.c_int, C.POINTER(C.c_longlong),
                                         C.POINTER(C.c_longlong)]),
     "srg_burst_params": (C.c_int, [C.c_void_p, C.c_longlong, C.c_int, C.c_int, _dp,

@@ -110,6 +110,13 @@ def interp_error(lines, nsamps: Optional[int] = None, sample_lines: int = 64, st
     return float(el.value), float(eo.value)
 
 
+def dropin_flush(device: int = -1) -> None:
+    """Wait for the overlapped drop-in calls of `device` (-1: every device) to
+    finish their merges; raises the first failure among them not yet
+    reported."""
+    check(lib().srg_dropin_flush(device))
+
+
 def dropin_last_bytes(device: int = -1):
     """(host-to-device, device-to-host) bytes of the last drop-in call."""
     h, d = C.c_longlong(), C.c_longlong()
@@ -131,8 +138,12 @@ def burst_params(lines: np.ndarray, satvel: np.ndarray) -> dict:
     return {k: getattr(r, k) for k, _ in r._fields_ if k != "pad"}
 
 
-def set_default_form(form: int, tile_cfg: int = -1) -> None:
+def set_default_form(form: int, tile_cfg: int = -1, overlap: Optional[int] = None) -> None:
+    """Options of azimuth_compress_ (srg_set_default_options): form, shape and,
+    when given, whether calls overlap (else the environment's default)."""
     o = default_options(form, tile_cfg)
+    if overlap is not None:
+        o.overlap = int(overlap)
     lib().srg_set_default_options(C.byref(o))
 
 

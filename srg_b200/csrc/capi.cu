@@ -27,7 +27,11 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <cstdlib>
 #include <atomic>
+#include <condition_variable>
+#include <deque>
+#include <functional>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -62,7 +66,15 @@ int fail(int code, const char *fmt, ...) {
             return fail(SRG_E_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));   \
     } while (0)
 
-srg_bp_options g_default_opts = {SRG_FORM_SPLIT, -1, -1, 0, 0, 0, 0, 0};
+// SRG_DROPIN_OVERLAP=1 in the environment: drop-in calls overlap by default
+int env_overlap() {
+    static const int v = [] {
+        const char *e = std::getenv("SRG_DROPIN_OVERLAP");
+        return e && e[0] == '1' ? 1 : 0;
+    }();
+    return v;
+}
+srg_bp_options g_default_opts = {SRG_FORM_SPLIT, -1, -1, 0, 0, 0, 0, 0, env_overlap()};
 std::mutex g_opts_mu;
 
 DevCtx g_ctx[64];
@@ -80,6 +92,224 @@ int get_ctx(int device, DevCtx **out) {
         c.dev = dev;
     }
     *out = &c;
+    return SRG_OK;
+}
+
+// Drop-in contexts of a device: two, used in turn by overlapped calls (a
+// call's tail still holds its context while the next call fills the other),
+// and the worker thread that runs the overlapped calls' tails in call order.
+struct DropinDev {
+    std::mutex call_mu;  // one drop-in call at a time on the device
+    DevCtx slot[2];
+    int next = 0;
+    std::mutex q_mu;
+    std::condition_variable q_cv;
+    std::deque<std::function<void()>> q;
+    bool busy[2] = {false, false};  // a queued or running tail holds the slot
+    bool worker = false;
+    int pending_rc = SRG_OK;  // first failure of a tail not yet returned
+    std::string pending_err;
+    long long last_h2d = 0, last_d2h = 0;
+};
+// Never destroyed: the worker threads wait on these at exit (destroying a
+// condition variable with a waiter blocks the exit).
+DropinDev *const g_dropin = new DropinDev[64];
+std::mutex g_dropin_mu;
+
+int get_dropin(int device, DropinDev **out) {
+    int dev = device;
+    if (dev < 0) CK(cudaGetDevice(&dev));
+    if (dev >= 64) return fail(SRG_E_ARG, "device ordinal %d out of range", dev);
+    CK(cudaSetDevice(dev));
+    std::lock_guard<std::mutex> g(g_dropin_mu);
+    DropinDev &d = g_dropin[dev];
+    for (DevCtx &c : d.slot) {
+        if (c.dev < 0) {
+            CK(cudaDeviceGetAttribute(&c.sms, cudaDevAttrMultiProcessorCount, dev));
+            c.dev = dev;
+        }
+    }
+    *out = &d;
+    return SRG_OK;
+}
+
+// Waits until no tail is queued or running on the device.
+void dropin_wait_idle(DropinDev &d) {
+    std::unique_lock<std::mutex> lk(d.q_mu);
+    d.q_cv.wait(lk, [&] { return d.q.empty() && !d.busy[0] && !d.busy[1]; });
+}
+
+// The first failure of an overlapped call's tail not yet returned (cleared).
+int dropin_take_pending(DropinDev &d) {
+    std::lock_guard<std::mutex> lk(d.q_mu);
+    const int rc = d.pending_rc;
+    if (rc) {
+        g_err = d.pending_err;
+        d.pending_rc = SRG_OK;
+        d.pending_err.clear();
+    }
+    return rc;
+}
+
+void dropin_flush_all();
+
+// Queues an overlapped call's tail; the worker (started on first use) runs
+// the tails one after the other.
+void dropin_enqueue(DropinDev &d, int slot, std::function<void()> job) {
+    static std::once_flag at_exit;
+    std::call_once(at_exit, [] { std::atexit(dropin_flush_all); });
+    std::lock_guard<std::mutex> lk(d.q_mu);
+    d.busy[slot] = true;
+    d.q.push_back([&d, slot, job = std::move(job)] {
+        job();
+        std::lock_guard<std::mutex> g(d.q_mu);
+        d.busy[slot] = false;
+    });
+    if (!d.worker) {
+        d.worker = true;
+        std::thread([&d] {
+            for (;;) {
+                std::function<void()> f;
+                {
+                    std::unique_lock<std::mutex> lk2(d.q_mu);
+                    d.q_cv.wait(lk2, [&] { return !d.q.empty(); });
+                    f = std::move(d.q.front());
+                }
+                f();  // the entry stays queued while it runs
+                {
+                    std::lock_guard<std::mutex> g(d.q_mu);
+                    d.q.pop_front();
+                }
+                d.q_cv.notify_all();
+            }
+        }).detach();
+    }
+    d.q_cv.notify_all();
+}
+
+void dropin_flush_all() {
+    for (int i = 0; i < 64; ++i) {
+        DropinDev &d = g_dropin[i];
+        bool started;
+        {
+            std::lock_guard<std::mutex> lk(d.q_mu);
+            started = d.worker;
+        }
+        if (started) dropin_wait_idle(d);
+    }
+}
+
+// A row block of a drop-in call's output box.
+struct OutBlock {
+    int r0, r1;  // rows [r0, r1) of the box
+    int rb;      // row block whose stored count came back with it, or -1
+};
+
+// What the end of a drop-in call needs once its copies back are queued.
+struct DropinTail {
+    OutBlock blk[DevCtx::kOutBlocks];
+    int nblk = 0, ntask = 1, ncols = 0, fl = 0, W = 0, fp_eff = 0, fdout = -1;
+    bool overlapped = false;  // runs behind the caller (worker thread)
+};
+
+// The end of a drop-in call: each row block of the output box is merged into
+// the .geo rows as soon as it is back (azimuth_compress.cu:510-537; pixels
+// outside the box are never replaced, so only the box is read and written);
+// then the call's streams are waited for and its status reported.
+int dropin_tail(DevCtx *c, const DropinTail &t) {
+    constexpr int K = DevCtx::kRowBlocks;
+    cudaStream_t st = c->s_main;
+    const float *win = static_cast<const float *>(c->host_stage);
+    HostPool &pool = HostPool::get();
+    std::atomic<int> cuda_err{0}, io_err{0};
+    const int ncols = t.ncols;
+    // merge rows [r0, r1) of the box (azimuth_compress.cu:510-537)
+    auto merge_rows = [&](int r0, int r1) {
+        std::vector<float> cur(2 * (size_t)ncols);
+        auto replaced = [](const float *v) { return std::fabs((double)v[0]) > 1.e-18; };
+        for (int r = r0; r < r1; ++r) {
+            // only the span [i0, i1] of replaced pixels is read and written back
+            // (most rows of a burst's box have none: they are left untouched)
+            const float *o2 = win + 2 * (size_t)r * ncols;
+            int i0 = 0;
+            while (i0 < ncols && !replaced(o2 + 2 * i0)) ++i0;
+            if (i0 == ncols) continue;
+            int i1 = ncols - 1;
+            while (!replaced(o2 + 2 * i1)) --i1;
+            const ssize_t want = (ssize_t)(i1 - i0 + 1) * 8;
+            const off_t off = ((off_t)(t.fl + r) * t.W + t.fp_eff + i0) * 8;
+            const ssize_t got = pread(t.fdout, cur.data(), want, off);
+            if (got < 0) {
+                io_err = 1;
+                return;
+            }
+            if (got < want) std::memset(reinterpret_cast<char *>(cur.data()) + got, 0, want - got);
+            for (int i = i0; i <= i1; ++i) {
+                if (replaced(o2 + 2 * i)) {
+                    cur[2 * (i - i0)] = o2[2 * i];
+                    cur[2 * (i - i0) + 1] = o2[2 * i + 1];
+                }
+            }
+            if (pwrite(t.fdout, cur.data(), want, off) != want) {
+                io_err = 2;
+                return;
+            }
+        }
+    };
+    // a block is merged once it is back: a row block that came back with
+    // every kept tile stored at once; any other block after the kernel's end,
+    // and only with the error word clear
+    auto mergeable = [&](int k) {
+        if (cudaEventSynchronize(c->ev_blk[k]) != cudaSuccess) return false;
+        const bool whole = t.blk[k].rb >= 0 && c->host_rb[2 * K + t.blk[k].rb] == c->host_rb[t.blk[k].rb];
+        return whole || (cudaEventSynchronize(c->ev_flags) == cudaSuccess && !c->host_flags[1]);
+    };
+    if (!t.overlapped) {
+        // every block's tasks at once on the pool, each waiting for its block
+        const int per_blk = std::max(1, t.ntask / std::max(t.nblk, 1));
+        if (t.nblk > 0) pool.run(t.nblk * per_blk, [&](int task) {
+            const int k = task / per_blk, part = task % per_blk;
+            if (!mergeable(k)) {
+                cuda_err = 1;
+                return;
+            }
+            const int b0 = t.blk[k].r0, b1 = t.blk[k].r1;
+            merge_rows(b0 + (int)((long long)(b1 - b0) * part / per_blk),
+                       b0 + (int)((long long)(b1 - b0) * (part + 1) / per_blk));
+        });
+    } else {
+        // Overlapped calls: the blocks are waited for here, in the order they
+        // come back, and only the merge of a block that is back goes to the
+        // pool, so no pool thread waits on the device while the next call's
+        // DEM read needs the pool.
+        for (int k = 0; k < t.nblk; ++k) {
+            if (!mergeable(k)) {
+                cuda_err = 1;
+                continue;
+            }
+            const int b0 = t.blk[k].r0, b1 = t.blk[k].r1;
+            const int parts = std::max(1, std::min(b1 - b0, std::max(1, t.ntask / 4)));
+            pool.run(parts, [&](int part) {
+                merge_rows(b0 + (int)((long long)(b1 - b0) * part / parts),
+                           b0 + (int)((long long)(b1 - b0) * (part + 1) / parts));
+            });
+        }
+    }
+    // the upload may end after the last chunk that needed it: the caller's
+    // buffer stays in use until then
+    const cudaError_t e1 = cudaStreamSynchronize(st), e2 = cudaStreamSynchronize(c->s_copy),
+                      e3 = cudaStreamSynchronize(c->s_back);
+    const cudaError_t e = e1 ? e1 : e2 ? e2 : e3 ? e3 : cudaGetLastError();
+    if (e != cudaSuccess) return fail(SRG_E_CUDA, "drop-in streams: %s", cudaGetErrorString(e));
+    if (c->host_flags[1]) {  // only row blocks whose every tile was stored were merged
+        const int word = c->host_flags[1];
+        cudaMemsetAsync(static_cast<int *>(c->flags.p) + 1, 0, sizeof(int), st);
+        cudaStreamSynchronize(st);
+        return fail(SRG_E_TIMEOUT, "device error word 0x%x (a bounded device wait gave up)", word);
+    }
+    if (cuda_err) return fail(SRG_E_CUDA, "copy of the output box failed");
+    if (io_err == 1) return fail(SRG_E_IO, "output read failed (fd %d)", t.fdout);
+    if (io_err == 2) return fail(SRG_E_IO, "output write failed (fd %d)", t.fdout);
     return SRG_OK;
 }
 
@@ -526,6 +756,7 @@ void srg_bp_default_options(srg_bp_options *o) {
     o->spin_limit = 0;
     o->full_lines = 0;
     o->scratch_limit = 0;
+    o->overlap = env_overlap();
 }
 
 const char *srg_last_error(void) { return g_err.c_str(); }
@@ -591,23 +822,53 @@ int srg_bp_burst_device_gated(const srg_burst_desc *b, const int *ready_word, in
 }
 
 int srg_dropin_last_bytes(int device, long long *h2d, long long *d2h) {
-    DevCtx *c = nullptr;
-    int rc = get_ctx(device, &c);
+    DropinDev *D = nullptr;
+    int rc = get_dropin(device, &D);
     if (rc) return rc;
-    std::lock_guard<std::mutex> g(c->mu);
-    if (h2d) *h2d = c->last_h2d;
-    if (d2h) *d2h = c->last_d2h;
+    std::lock_guard<std::mutex> g(D->call_mu);
+    if (h2d) *h2d = D->last_h2d;
+    if (d2h) *d2h = D->last_d2h;
     return SRG_OK;
+}
+
+int srg_dropin_flush(int device) {
+    if (device >= 0) {
+        DropinDev *D = nullptr;
+        int rc = get_dropin(device, &D);
+        if (rc) return rc;
+        dropin_wait_idle(*D);
+        return dropin_take_pending(*D);
+    }
+    int first = SRG_OK;
+    std::string msg;
+    for (int i = 0; i < 64; ++i) {
+        DropinDev &d = g_dropin[i];
+        bool started;
+        {
+            std::lock_guard<std::mutex> lk(d.q_mu);
+            started = d.worker;
+        }
+        if (!started) continue;
+        dropin_wait_idle(d);
+        const int rc = dropin_take_pending(d);
+        if (rc && !first) {
+            first = rc;
+            msg = g_err;
+        }
+    }
+    if (first) g_err = msg;
+    return first;
 }
 
 int srg_test_set_dropin_sequence(int device, int seq) {
     if (seq < 0 || seq > DevCtx::kSeqLimit)
         return fail(SRG_E_ARG, "sequence %d outside [0, %d]", seq, DevCtx::kSeqLimit);
-    DevCtx *c = nullptr;
-    int rc = get_ctx(device, &c);
+    DropinDev *D = nullptr;
+    int rc = get_dropin(device, &D);
     if (rc) return rc;
-    std::lock_guard<std::mutex> g(c->mu);
-    c->upload_seq = seq;
+    std::lock_guard<std::mutex> g(D->call_mu);
+    dropin_wait_idle(*D);
+    for (DevCtx &c : D->slot) c.upload_seq = seq;
     return SRG_OK;
 }
 
@@ -827,10 +1088,22 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
             return fail(SRG_E_NOMEM, "the call needs %lld bytes of device scratch, the limit is %lld",
                         need, (long long)o.scratch_limit);
     }
-    DevCtx *c = nullptr;
-    int rc = get_ctx(o.device, &c);
+    DropinDev *D = nullptr;
+    int rc = get_dropin(o.device, &D);
     if (rc) return rc;
-    std::lock_guard<std::mutex> g(c->mu);
+    std::lock_guard<std::mutex> g(D->call_mu);
+    // An overlapped call takes the context the call before last used, once
+    // that call's tail is done; a call without overlap waits for every tail.
+    int si = 0;
+    if (o.overlap) {
+        si = D->next;
+        D->next ^= 1;
+        std::unique_lock<std::mutex> lk(D->q_mu);
+        D->q_cv.wait(lk, [&] { return !D->busy[si]; });
+    } else {
+        dropin_wait_idle(*D);
+    }
+    DevCtx *c = &D->slot[si];
     if ((rc = ensure_dropin(*c))) return rc;
     cudaStream_t st = c->s_main;
     const size_t stage_bytes = std::max(dem_bytes, win_bytes) + 64;
@@ -876,8 +1149,9 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     // word grows from call to call (call number x 64 + granules), so a value
     // left by an earlier call never satisfies a later one; the row blocks'
     // done words hold the call number.  When the call number restarts, both
-    // are cleared first (every earlier call has finished its GPU work: each
-    // call waits for its three streams before it returns).
+    // are cleared first (every earlier call on this context has finished its
+    // GPU work: a call's tail waits for its three streams, and a call takes a
+    // context only once the tail of the call that last held it is done).
     int *ready_word = static_cast<int *>(c->flags.p) + DevCtx::kReadyWord;
     constexpr int kGranules = 32;
     static const int kBlockEnd[DevCtx::kUploadBlocks] = {6, 12, 17, 22, 26, 29, 31, 32};
@@ -1139,10 +1413,6 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
     const int band_hi = std::min(nl - 1, c->host_flags[DevCtx::kBandWord + 1]);
     const int nband = band_hi >= band_lo ? band_hi - band_lo + 1 : 0;
     float *win = static_cast<float *>(c->host_stage);
-    struct OutBlock {
-        int r0, r1;  // rows [r0, r1) of the box
-        int rb;      // row block whose stored count came back with it, or -1
-    };
     OutBlock blk[DevCtx::kOutBlocks];
     int nblk = 0;
     auto copy_back = [&](int r0, int r1, cudaStream_t s) {
@@ -1190,73 +1460,48 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
         }
     }
 
-    // merge into the .geo rows (azimuth_compress.cu:510-537); pixels outside
-    // the box are never replaced, so only the box is read and written
-    std::atomic<int> cuda_err{0};
-    const int per_blk = std::max(1, ntask / std::max(nblk, 1));
-    if (nblk > 0) pool.run(nblk * per_blk, [&](int t) {
-        const int k = t / per_blk, part = t % per_blk;
-        if (cudaEventSynchronize(c->ev_blk[k]) != cudaSuccess) {
-            cuda_err = 1;
-            return;
-        }
-        // a row block came back with every kept tile stored; any other block
-        // waits for the kernel's end and merges only with the error word clear
-        const bool whole = blk[k].rb >= 0 && c->host_rb[2 * K + blk[k].rb] == c->host_rb[blk[k].rb];
-        if (!whole && (cudaEventSynchronize(c->ev_flags) != cudaSuccess || c->host_flags[1])) {
-            cuda_err = 1;
-            return;
-        }
-        const int b0 = blk[k].r0, b1 = blk[k].r1;
-        const int r0 = b0 + (int)((long long)(b1 - b0) * part / per_blk);
-        const int r1 = b0 + (int)((long long)(b1 - b0) * (part + 1) / per_blk);
-        std::vector<float> cur(2 * (size_t)ncols);
-        auto replaced = [](const float *v) { return std::fabs((double)v[0]) > 1.e-18; };
-        for (int r = r0; r < r1; ++r) {
-            // only the span [i0, i1] of replaced pixels is read and written back
-            // (most rows of a burst's box have none: they are left untouched)
-            const float *o2 = win + 2 * (size_t)r * ncols;
-            int i0 = 0;
-            while (i0 < ncols && !replaced(o2 + 2 * i0)) ++i0;
-            if (i0 == ncols) continue;
-            int i1 = ncols - 1;
-            while (!replaced(o2 + 2 * i1)) --i1;
-            const ssize_t want = (ssize_t)(i1 - i0 + 1) * 8;
-            const off_t off = ((off_t)(fl + r) * W + fp_eff + i0) * 8;
-            const ssize_t got = pread(fdout, cur.data(), want, off);
-            if (got < 0) {
-                io_err = 1;
-                return;
-            }
-            if (got < want) std::memset(reinterpret_cast<char *>(cur.data()) + got, 0, want - got);
-            for (int i = i0; i <= i1; ++i) {
-                if (replaced(o2 + 2 * i)) {
-                    cur[2 * (i - i0)] = o2[2 * i];
-                    cur[2 * (i - i0) + 1] = o2[2 * i + 1];
+    DropinTail tail;
+    std::copy(blk, blk + nblk, tail.blk);
+    tail.nblk = nblk;
+    tail.ntask = ntask;
+    tail.ncols = ncols;
+    tail.fl = fl;
+    tail.W = W;
+    tail.fp_eff = fp_eff;
+    tail.fdout = fdout;
+    D->last_h2d = c->last_h2d;
+    D->last_d2h = c->last_d2h;
+    if (o.overlap) {
+        // the caller's buffers are read by the upload only: free once it is
+        // done; the tail merges through a descriptor of its own
+        CKD(cudaStreamSynchronize(c->s_copy));
+        tail.fdout = dup(fdout);
+        tail.overlapped = true;
+        if (tail.fdout >= 0) {
+            // failures of earlier calls' tails only: this call's comes later
+            const int earlier = dropin_take_pending(*D);
+            const std::string earlier_msg = g_err;
+            const int dev = c->dev;
+            dropin_enqueue(*D, si, [D, c, tail, dev] {
+                int r = cudaSetDevice(dev) == cudaSuccess ? dropin_tail(c, tail)
+                                                          : fail(SRG_E_CUDA, "cudaSetDevice failed");
+                close(tail.fdout);
+                if (r) {
+                    std::lock_guard<std::mutex> lk(D->q_mu);
+                    if (!D->pending_rc) {
+                        D->pending_rc = r;
+                        D->pending_err = g_err;
+                    }
                 }
-            }
-            if (pwrite(fdout, cur.data(), want, off) != want) {
-                io_err = 2;
-                return;
-            }
+            });
+            if (earlier) g_err = earlier_msg;
+            return earlier;
         }
-    });
-    CKD(cudaStreamSynchronize(st));
-    // the upload may end after the last chunk that needed it: the caller's
-    // buffer stays in use until then
-    CKD(cudaStreamSynchronize(c->s_copy));
-    CKD(cudaStreamSynchronize(c->s_back));
-    CKD(cudaGetLastError());
-    if (c->host_flags[1]) {  // only row blocks whose every tile was stored were merged
-        const int word = c->host_flags[1];
-        cudaMemsetAsync(static_cast<int *>(c->flags.p) + 1, 0, sizeof(int), st);
-        cudaStreamSynchronize(st);
-        return fail(SRG_E_TIMEOUT, "device error word 0x%x (a bounded device wait gave up)", word);
+        tail.fdout = fdout;  // no descriptor to spare: the tail runs here
+        tail.overlapped = false;
     }
-    if (cuda_err) return fail(SRG_E_CUDA, "copy of the output box failed");
-    if (io_err == 1) return fail(SRG_E_IO, "output read failed (fd %d)", fdout);
-    if (io_err == 2) return fail(SRG_E_IO, "output write failed (fd %d)", fdout);
-    return SRG_OK;
+    rc = dropin_tail(c, tail);
+    return rc ? rc : dropin_take_pending(*D);
 #undef CKD
 }
 

@@ -1,0 +1,178 @@
+"""Overlapped drop-in calls (srg_bp_options.overlap, SRG_DROPIN_OVERLAP): a
+call returns once its range lines are on the device and its merge into the
+.geo finishes behind the caller, in call order.  The .geo must come out
+identical to calls that wait for their merges, the caller's buffers must be
+free when a call returns, the caller may close its .geo descriptor, and a
+failure of a merge must come back from srg_dropin_flush."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import mini_case, rel_err
+from srg_b200 import _lib, api, scene
+
+pytestmark = pytest.mark.gpu
+FP64_REL = 2e-6
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("the CUDA path needs a GPU; none is visible")
+    return torch
+
+
+def three_bursts():
+    """Three bursts over one grid and one DEM whose formed line bands overlap
+    without coinciding (different samples and apertures)."""
+    base = mini_case("slope")
+    bursts = [base]
+    for seed, ap in ((21, 64), (22, 160)):
+        b = scene.mini_fixture(seed=seed, dem_kind="slope", aperture=ap)
+        b.dem = base.dem
+        bursts.append(b)
+    rng = np.random.default_rng(5)
+    init = (rng.standard_normal((base.demlength, base.demwidth)) +
+            1j * rng.standard_normal((base.demlength, base.demwidth))).astype(np.complex64)
+    return base, bursts, init
+
+
+def run_calls(bursts, base, init, form, overlap, spoil=False, close_early=False, repeat=1):
+    """The bursts through srg_azimuth_compress in order onto one .geo file;
+    `spoil`: the caller overwrites each burst's lines with NaN right after the
+    call returns; `close_early`: the .geo descriptor is closed before the
+    flush."""
+    with tempfile.TemporaryDirectory() as td:
+        dem_path, geo_path = os.path.join(td, "e.dem"), os.path.join(td, "s.geo")
+        np.ascontiguousarray(base.dem, np.int16).tofile(dem_path)
+        init.tofile(geo_path)
+        fd_dem, fd_geo = os.open(dem_path, os.O_RDWR), os.open(geo_path, os.O_RDWR)
+        closed = False
+        try:
+            for _ in range(repeat):
+                for b in bursts:
+                    lines = np.ascontiguousarray(b.burst, np.complex64).copy()
+                    api.azimuth_compress_status(b, fd_geo, fd_dem, form=form, burst=lines,
+                                                overlap=overlap)
+                    if spoil:
+                        lines[...] = np.nan
+            if close_early:
+                os.close(fd_geo)
+                closed = True
+            api.dropin_flush()
+        finally:
+            os.close(fd_dem)
+            if not closed:
+                os.close(fd_geo)
+        return np.fromfile(geo_path, np.complex64).reshape(base.demlength, base.demwidth)
+
+
+@pytest.mark.parametrize("form", [_lib.FORM_FP64, _lib.FORM_SPLIT])
+def test_overlapped_calls_merge_like_calls_that_wait(torch_cuda, form):
+    base, bursts, init = three_bursts()
+    want = run_calls(bursts, base, init, form, overlap=0)
+    got = run_calls(bursts, base, init, form, overlap=1)
+    assert (want != init).sum() > 0
+    assert np.array_equal(got, want)
+    # twice over the same file: the second pass's merges see the first's pixels
+    assert np.array_equal(run_calls(bursts, base, init, form, overlap=1, repeat=2),
+                          run_calls(bursts, base, init, form, overlap=0, repeat=2))
+
+
+def test_overlapped_calls_match_the_oracle_entry(torch_cuda):
+    base, bursts, init = three_bursts()
+    O.build()
+    orc = O.Oracle()
+    with tempfile.TemporaryDirectory() as td:
+        dem_path, geo_path = os.path.join(td, "e.dem"), os.path.join(td, "s.geo")
+        np.ascontiguousarray(base.dem, np.int16).tofile(dem_path)
+        init.tofile(geo_path)
+        fd_dem, fd_geo = os.open(dem_path, os.O_RDWR), os.open(geo_path, os.O_RDWR)
+        try:
+            for b in bursts:
+                O.call_33(orc.lib.srg_oracle_azimuth_compress_, b, fd_geo, fd_dem)
+        finally:
+            os.close(fd_dem)
+            os.close(fd_geo)
+        ref = np.fromfile(geo_path, np.complex64).reshape(base.demlength, base.demwidth)
+    got = run_calls(bursts, base, init, _lib.FORM_FP64, overlap=1)
+    assert np.array_equal(got != init, ref != init)
+    assert rel_err(got, ref) < FP64_REL
+
+
+def test_overlapped_call_is_done_with_the_callers_buffers_and_descriptor(torch_cuda):
+    """The caller overwrites each burst's lines as soon as the call returns and
+    closes its .geo descriptor before the flush: the file is the same."""
+    base, bursts, init = three_bursts()
+    want = run_calls(bursts, base, init, _lib.FORM_SPLIT, overlap=0)
+    got = run_calls(bursts, base, init, _lib.FORM_SPLIT, overlap=1, spoil=True,
+                    close_early=True)
+    assert np.array_equal(got, want)
+
+
+def test_overlapped_merge_failure_comes_back_from_flush(torch_cuda):
+    """A .geo descriptor that cannot be written: the overlapped call returns,
+    the flush reports the failed write; a later call on a good descriptor
+    succeeds (the failure is reported once)."""
+    base, bursts, init = three_bursts()
+    b = bursts[0]
+    with tempfile.TemporaryDirectory() as td:
+        dem_path, geo_path = os.path.join(td, "e.dem"), os.path.join(td, "s.geo")
+        np.ascontiguousarray(base.dem, np.int16).tofile(dem_path)
+        init.tofile(geo_path)
+        fd_dem = os.open(dem_path, os.O_RDONLY)
+        fd_ro = os.open(geo_path, os.O_RDONLY)
+        fd_rw = os.open(geo_path, os.O_RDWR)
+        try:
+            api.azimuth_compress_status(b, fd_ro, fd_dem, overlap=1)   # returns before the merge
+            with pytest.raises(_lib.SrgError, match="output write failed"):
+                api.dropin_flush()
+            api.dropin_flush()   # reported once
+            api.azimuth_compress_status(b, fd_rw, fd_dem, overlap=1)
+            api.dropin_flush()
+        finally:
+            for fd in (fd_dem, fd_ro, fd_rw):
+                os.close(fd)
+        got = np.fromfile(geo_path, np.complex64).reshape(base.demlength, base.demwidth)
+    assert (got != init).sum() > 0
+
+
+CHILD = r"""
+import os, sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+sys.path.insert(0, os.path.join(sys.argv[1], "tests"))
+import test_gpu_dropin_overlap as T
+from srg_b200 import _lib, api
+base, bursts, init = T.three_bursts()
+fd_dem = os.open(sys.argv[2], os.O_RDONLY)
+fd_geo = os.open(sys.argv[3], os.O_RDWR)
+for b in bursts:
+    api.azimuth_compress_status(b, fd_geo, fd_dem, form=_lib.FORM_SPLIT, overlap=1)
+os.close(fd_geo)
+print("calls returned", flush=True)
+"""
+
+
+def test_overlapped_calls_finish_at_process_exit(torch_cuda):
+    """A process that makes overlapped calls and exits without a flush: it
+    exits (within the limit) and the .geo holds every merge."""
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    base, bursts, init = three_bursts()
+    want = run_calls(bursts, base, init, _lib.FORM_SPLIT, overlap=0)
+    with tempfile.TemporaryDirectory() as td:
+        dem_path, geo_path = os.path.join(td, "e.dem"), os.path.join(td, "s.geo")
+        np.ascontiguousarray(base.dem, np.int16).tofile(dem_path)
+        init.tofile(geo_path)
+        p = subprocess.run([sys.executable, "-c", CHILD, root, dem_path, geo_path],
+                           capture_output=True, text=True, timeout=300)
+        assert p.returncode == 0, p.stderr[-2000:]
+        assert "calls returned" in p.stdout
+        got = np.fromfile(geo_path, np.complex64).reshape(base.demlength, base.demwidth)
+    assert np.array_equal(got, want)
