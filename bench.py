@@ -170,6 +170,12 @@ def e2e_dropin(torch, wl, steps, form, separate=False, bursts=None, overlap=0):
                 h, d = api.dropin_last_bytes()
                 h2d += h
                 d2h += d
+            if overlap:
+                # overlapped calls take the device's two drop-in contexts in turn: a
+                # second pass gives each context the bursts the first gave the other
+                # (its buffers grow to the largest burst before the timed steps)
+                for call in calls:
+                    call()
             api.dropin_flush()
             torch.cuda.synchronize()
             t0 = time.perf_counter()
