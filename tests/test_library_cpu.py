@@ -116,3 +116,14 @@ def test_dropin_refuses_an_empty_box_and_a_scratch_limit(tmp_path):
         os.close(fd_dem)
         os.close(fd_geo)
     assert np.array_equal(np.fromfile(geo, np.complex64).reshape(init.shape), init)
+
+
+def test_overlap_option_and_flush_without_a_gpu(monkeypatch):
+    """The overlap option defaults off (SRG_DROPIN_OVERLAP unset), its field is
+    where the header puts it, and a flush with no overlapped call made waits
+    for nothing and succeeds on a machine without a GPU."""
+    o = _lib.default_options()
+    assert o.overlap == int(os.environ.get("SRG_DROPIN_OVERLAP", "0") == "1")
+    assert _lib.Options.overlap.offset == _lib.Options.scratch_limit.offset + 8
+    assert _lib.lib().srg_dropin_flush(-1) == _lib.SRG_OK
+    api.dropin_flush()
