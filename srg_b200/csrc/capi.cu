@@ -153,38 +153,44 @@ int dropin_take_pending(DropinDev &d) {
 
 void dropin_flush_all();
 
-// Queues an overlapped call's tail; the worker (started on first use) runs
-// the tails one after the other.
-void dropin_enqueue(DropinDev &d, int slot, std::function<void()> job) {
+// Queues an overlapped call's tail for the device's worker thread (started
+// on first use), which runs the tails one after the other; false, with
+// nothing queued, when the worker cannot be started.
+bool dropin_enqueue(DropinDev &d, int slot, std::function<void()> job) {
     static std::once_flag at_exit;
     std::call_once(at_exit, [] { std::atexit(dropin_flush_all); });
     std::lock_guard<std::mutex> lk(d.q_mu);
+    if (!d.worker) {
+        try {
+            std::thread([&d] {
+                for (;;) {
+                    std::function<void()> f;
+                    {
+                        std::unique_lock<std::mutex> lk2(d.q_mu);
+                        d.q_cv.wait(lk2, [&] { return !d.q.empty(); });
+                        f = std::move(d.q.front());
+                    }
+                    f();  // the entry stays queued while it runs
+                    {
+                        std::lock_guard<std::mutex> g(d.q_mu);
+                        d.q.pop_front();
+                    }
+                    d.q_cv.notify_all();
+                }
+            }).detach();
+        } catch (...) {
+            return false;
+        }
+        d.worker = true;
+    }
     d.busy[slot] = true;
     d.q.push_back([&d, slot, job = std::move(job)] {
         job();
         std::lock_guard<std::mutex> g(d.q_mu);
         d.busy[slot] = false;
     });
-    if (!d.worker) {
-        d.worker = true;
-        std::thread([&d] {
-            for (;;) {
-                std::function<void()> f;
-                {
-                    std::unique_lock<std::mutex> lk2(d.q_mu);
-                    d.q_cv.wait(lk2, [&] { return !d.q.empty(); });
-                    f = std::move(d.q.front());
-                }
-                f();  // the entry stays queued while it runs
-                {
-                    std::lock_guard<std::mutex> g(d.q_mu);
-                    d.q.pop_front();
-                }
-                d.q_cv.notify_all();
-            }
-        }).detach();
-    }
     d.q_cv.notify_all();
+    return true;
 }
 
 void dropin_flush_all() {
@@ -1482,7 +1488,7 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
             const int earlier = dropin_take_pending(*D);
             const std::string earlier_msg = g_err;
             const int dev = c->dev;
-            dropin_enqueue(*D, si, [D, c, tail, dev] {
+            const bool queued = dropin_enqueue(*D, si, [D, c, tail, dev] {
                 int r = cudaSetDevice(dev) == cudaSuccess ? dropin_tail(c, tail)
                                                           : fail(SRG_E_CUDA, "cudaSetDevice failed");
                 close(tail.fdout);
@@ -1494,8 +1500,17 @@ int srg_azimuth_compress(const float *burstdata, const double *satloc, int rawda
                     }
                 }
             });
-            if (earlier) g_err = earlier_msg;
-            return earlier;
+            if (queued) {
+                if (earlier) g_err = earlier_msg;
+                return earlier;
+            }
+            // no worker thread to be had: the tail runs here after all
+            close(tail.fdout);
+            tail.fdout = fdout;
+            tail.overlapped = false;
+            rc = dropin_tail(c, tail);
+            if (!rc && earlier) g_err = earlier_msg;
+            return rc ? rc : earlier;
         }
         tail.fdout = fdout;  // no descriptor to spare: the tail runs here
         tail.overlapped = false;
