@@ -176,3 +176,49 @@ def test_overlapped_calls_finish_at_process_exit(torch_cuda):
         assert "calls returned" in p.stdout
         got = np.fromfile(geo_path, np.complex64).reshape(base.demlength, base.demwidth)
     assert np.array_equal(got, want)
+
+
+def test_overlapped_wait_that_gives_up_comes_back_from_flush(torch_cuda):
+    """An overlapped call whose kernel gives up on rows not in yet (a poll
+    limit far shorter than the pinned upload): the call returns, the flush
+    returns SRG_E_TIMEOUT, and every .geo row is either as it was or exactly
+    the row a complete call writes."""
+    torch = torch_cuda
+    b = scene.config0_point_targets()
+    rng = np.random.default_rng(3)
+    init = (rng.standard_normal((b.demlength, b.demwidth)) +
+            1j * rng.standard_normal((b.demlength, b.demwidth))).astype(np.complex64)
+    pinned = torch.from_numpy(np.ascontiguousarray(b.burst, np.complex64)).pin_memory()
+
+    def run(**options):
+        with tempfile.TemporaryDirectory() as td:
+            dem_path, geo_path = os.path.join(td, "e.dem"), os.path.join(td, "s.geo")
+            np.ascontiguousarray(b.dem, np.int16).tofile(dem_path)
+            init.tofile(geo_path)
+            fd_dem, fd_geo = os.open(dem_path, os.O_RDWR), os.open(geo_path, os.O_RDWR)
+            try:
+                api.azimuth_compress_status(b, fd_geo, fd_dem, burst=pinned.numpy(), overlap=1,
+                                            **options)
+                try:
+                    api.dropin_flush()
+                    rc = _lib.SRG_OK
+                except _lib.SrgError as e:
+                    rc = e.code
+            finally:
+                os.close(fd_dem)
+                os.close(fd_geo)
+            return rc, np.fromfile(geo_path, np.complex64).reshape(init.shape)
+
+    rc, full = run()
+    assert rc == _lib.SRG_OK and (full != init).any()
+    timeouts = 0
+    for _ in range(3):
+        rc, got = run(spin_limit=8)
+        assert rc in (_lib.SRG_OK, _lib.SRG_E_TIMEOUT)
+        timeouts += rc == _lib.SRG_E_TIMEOUT
+        for r in range(b.demlength):
+            assert (np.array_equal(got[r].view(np.uint32), init[r].view(np.uint32)) or
+                    np.array_equal(got[r].view(np.uint32), full[r].view(np.uint32))), r
+    assert timeouts > 0
+    rc, again = run()
+    assert rc == _lib.SRG_OK and np.array_equal(again.view(np.uint32), full.view(np.uint32))
