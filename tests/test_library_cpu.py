@@ -127,3 +127,18 @@ def test_overlap_option_and_flush_without_a_gpu(monkeypatch):
     assert _lib.Options.overlap.offset == _lib.Options.scratch_limit.offset + 8
     assert _lib.lib().srg_dropin_flush(-1) == _lib.SRG_OK
     api.dropin_flush()
+
+
+def test_overlap_environment_switch_sets_the_default():
+    """SRG_DROPIN_OVERLAP=1 in the environment makes overlapped drop-in calls
+    the process-wide default (srg_bp_default_options); other values do not."""
+    import subprocess
+    import sys
+    code = ("import sys; sys.path.insert(0, %r); from srg_b200 import _lib; "
+            "print(_lib.default_options().overlap)" % ROOT)
+    for val, want in (("1", "1"), ("0", "0"), ("yes", "0")):
+        env = dict(os.environ, SRG_DROPIN_OVERLAP=val)
+        p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env,
+                           timeout=120)
+        assert p.returncode == 0, p.stderr[-1000:]
+        assert p.stdout.strip() == want, (val, p.stdout)
