@@ -482,6 +482,75 @@ def profile_shapes(torch, workload: str, shapes, samples: str = "random", seed=N
     torch.cuda.synchronize()
 
 
+def hbm_peak_gbs():
+    """(HBM copy bandwidth in GB/s, where it comes from): the measured figure of
+    MEASURED_PEAKS.json when present, else the pool's earlier measurement."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback (6.65 TB/s, an earlier measurement on this pool)"
+
+
+def range_compression_bench(torch, steps: int, warmup: int):
+    """Range compression of one IW1-sized burst of decoded lines on the device
+    (sentinel/processsub.f90:86-123: each line times the conjugate chirp
+    replica spectrum, 32,768-point FFTs; srg_range_compress_device): 1,500
+    lines of 24,000 complex64 samples, seeded Gaussian samples (the timing does
+    not depend on them), the IW pulse of the tests (64.3 MHz sampling, 52.4 us,
+    0.7792 MHz/us).  Lines resident in HBM; a step compresses the burst once.
+    Algorithmic bytes: every input sample read once and every output sample
+    written once.  CPU baseline: the oracle's numpy restatement (one thread)
+    on 32 lines (parity of the two is tests/test_rangecomp.py's)."""
+    from srg_b200 import api
+    fs = float(np.float32(3.0 / 7.0 * 4.0 * 37.53472224))
+    pulse = dict(samplefreq=fs, startfreq=-20.2, ramprate=0.7792, pulselength=52.4)
+    nlines, nsamps = 1500, 24000
+    g = torch.Generator(device="cuda")
+    g.manual_seed(1005)
+    lines = torch.complex(torch.randn((nlines, nsamps), device="cuda", generator=g),
+                          torch.randn((nlines, nsamps), device="cuda", generator=g))
+    _, npts = api.range_replica(**pulse)
+    nvalid = nsamps - npts
+    out = torch.empty((nlines, nvalid), dtype=torch.complex64, device="cuda")
+    st = torch.cuda.Stream()
+    for _ in range(warmup):
+        api.range_compress(lines, **pulse, out=out, stream=st.cuda_stream, sync=False)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(steps):
+        api.range_compress(lines, **pulse, out=out, stream=st.cuda_stream, sync=False)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    alg_bytes = nlines * (nsamps + nvalid) * 8
+    achieved = alg_bytes / (ms * 1e-3) / 1e9
+    peak, peak_src = hbm_peak_gbs()
+    # the CPU baseline leg: the oracle's restatement on a sample of the lines
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import rangecomp as orc
+    sample = lines[:32].cpu().numpy()
+    t0 = time.perf_counter()
+    orc.range_compress(sample, **pulse)
+    cpu_s = time.perf_counter() - t0
+    line = {
+        "metric": "range-compressed lines/s (IW1 burst, 32,768-point FFTs)", "workload": "rc",
+        "value": nlines / (ms * 1e-3), "unit": "lines/s", "n_gpus": 1, "steps": steps,
+        "warmup": warmup, "ms_per_step": ms, "higher_is_better": True, "dtype": "c64 (f32)",
+        "data": "synthetic, seeded Gaussian decoded lines",
+        "config": {"workload": "range compression of one IW1-sized burst: 1500 lines x 24000 "
+                               "complex64 samples, replica of 3369 points, 32768-point FFTs"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "peak_source": peak_src,
+                     "bytes_per_line": (nsamps + nvalid) * 8},
+        "cpu_baseline": {"value": len(sample) / cpu_s, "unit": "lines/s", "cores": 1,
+                         "kind": "port", "sample": "oracle numpy restatement, 32 lines"},
+    }
+    print(json.dumps(line))
+
+
 # ---------------------------------------------------------------------------
 
 
@@ -491,7 +560,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c4"])
+    ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c4", "rc"],
+                    help="c1-c4: backprojection workloads; rc: range compression of one burst")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--shapes", default=None,
@@ -508,6 +578,10 @@ def main():
         profile_shapes(torch, args.workload, [int(x) for x in args.profile_shapes.split(",")],
                        args.samples)
         print("ok", args.profile_shapes)
+        return
+    if args.workload == "rc":
+        import torch
+        range_compression_bench(torch, max(1, args.steps), max(1, args.warmup))
         return
     pinned = [int(x) for x in args.shapes.split(",")] if args.shapes else None
     rank, world, local = dist_env()
