@@ -217,24 +217,33 @@ def time_plan(torch, plan, steps, warmup, stream, stages=None, label="timed"):
     return sum(e0.elapsed_time(e1) for e0, e1 in ev) / steps
 
 
-def stack_interferograms(torch, wl, s_slcs, d_slcs, stream, steps):
+def stack_interferograms(torch, wl, s_slcs, d_slcs, stream, steps, exchange=None):
     """Crossmul of the stack's sequential pairs (one stack call, timed with
     CUDA events on `stream`), the interferometric phase error of the split
     images against the FP64 images, and of the FP64 interferograms against
-    the injected deformation (4 pi / lambda times the pair's range change)."""
+    the injected deformation (4 pi / lambda times the pair's range change).
+    `exchange` (a stack dealt in blocks over ranks): extends this rank's image
+    list by the next block's first image, inside the timed region."""
     from srg_b200 import api
     sp = stream.cuda_stream
-    outs = api.crossmul_stack(s_slcs, stream=sp)
+    ext = exchange if exchange is not None else (lambda images: list(images))
+    with torch.cuda.stream(stream):
+        pairs = ext(s_slcs)
+    outs = api.crossmul_stack(pairs, stream=sp)
     torch.cuda.synchronize()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(steps)]
     for e0, e1 in ev:
         e0.record(stream)
-        api.crossmul_stack(s_slcs, stream=sp, sync=False, outs=outs)
+        with torch.cuda.stream(stream):
+            pairs = ext(s_slcs)
+        api.crossmul_stack(pairs, stream=sp, sync=False, outs=outs)
         e1.record(stream)
     torch.cuda.synchronize()
     ms = sum(e0.elapsed_time(e1) for e0, e1 in ev) / steps
-    igd, _ = api.crossmul_stack(d_slcs, stream=sp)
+    with torch.cuda.stream(stream):
+        d_pairs = ext(d_slcs)
+    igd, _ = api.crossmul_stack(d_pairs, stream=sp)
     igs = torch.stack(outs[0]).to(torch.complex128)
     igd = torch.stack(igd).to(torch.complex128)
     amp = igd.abs()
@@ -245,7 +254,7 @@ def stack_interferograms(torch, wl, s_slcs, d_slcs, stream, steps):
     want = torch.from_numpy(wl.extra["range_change"]).to(igd.device, torch.float64)
     want = want * (4.0 * np.pi / wl.extra["wvl"] / max(1, n - 1))
     dt = torch.angle(igd * torch.exp(-1j * want)[None]) * 1e3
-    return {"ms_per_stack": ms, "pairs": n - 1, "looks": [1, 1],
+    return {"ms_per_stack": ms, "pairs": len(outs[0]), "looks": [1, 1],
             "ifg_phase_error_vs_fp64": {"ph_rms_mrad": float(torch.sqrt((ph ** 2).mean())),
                                         "ph_max_mrad": float(ph.abs().max()),
                                         "pixels": int(ph.numel())},
@@ -614,11 +623,13 @@ def main():
     build = {"c1": workloads.config1, "c2": workloads.config1, "c3": workloads.config3,
              "c4": workloads.config4}[args.workload]
     # N > 1, the IW scene: one scene partitioned over the ranks (every rank
-    # builds the same scene); other workloads: one replica per rank
+    # builds the same scene); the repeat-pass stack: its acquisitions dealt in
+    # date-order blocks; the one-burst workloads: one replica per rank
     partitioned = world > 1 and args.workload == "c3"
+    stack_blocks = world > 1 and args.workload == "c4"
     wl = build(device=f"cuda:{local}",
                seed={"c1": 1001, "c2": 1001, "c3": 1003, "c4": 1004}[args.workload] +
-               (0 if partitioned else rank))
+               (0 if partitioned or stack_blocks else rank))
     if partitioned:
         from srg_b200 import api, partition
         weights = [api.count_terms([db]) for db in wl.bursts]
@@ -627,9 +638,25 @@ def main():
                                              _lib.FORM_SPLIT)
         own_bursts, terms_rank = wl.plan.mine, int(wl.plan.own_weight())
 
+    exchange = None
+    if stack_blocks:
+        from srg_b200 import api, partition
+        block = partition.block_partition(len(wl.bursts), world)[rank]
+        own_bursts = [wl.bursts[i] for i in block]
+        wl.plan.close()   # the whole-stack plan gives way to this rank's block
+        wl.plan = api.Scene(own_bursts, raster=None, form=_lib.FORM_SPLIT)
+        terms_rank = wl.plan.terms()
+        recv = torch.empty_like(own_bursts[0].out)
+
+        def exchange(images):
+            """This rank's images and, but on the last rank, the next block's
+            first (the pair across the block's end)."""
+            nxt = partition.exchange_boundary(images[0], recv, rank, world, dist)
+            return list(images) + ([nxt] if nxt is not None else [])
+
     stream = torch.cuda.Stream()
     c2 = oversampled_lines(torch, wl, stream) if args.workload == "c2" else None
-    if not partitioned:
+    if not partitioned and not stack_blocks:
         own_bursts, terms_rank = wl.bursts, wl.terms
     fp32_peak = _lib.measure_fma_peak(False)
     fp64_peak = _lib.measure_fma_peak(True)
@@ -654,7 +681,7 @@ def main():
     if wl.raster is not None:
         split_out = wl.raster.clone()
     else:
-        split_out = torch.stack([db.out for db in wl.bursts])
+        split_out = torch.stack([db.out for db in own_bursts])
     if pinned:
         plan.set_form(_lib.FORM_FP64, pinned[1])
         tuned["fp64"] = (plan.shape(), None)
@@ -666,11 +693,11 @@ def main():
     if wl.raster is not None:
         perr = raster_phase_error(torch, split_out, wl.raster) if rank == 0 else None
     else:
-        fp64_out = torch.stack([db.out for db in wl.bursts])
+        fp64_out = torch.stack([db.out for db in own_bursts])
         perr = raster_phase_error(torch, split_out, fp64_out)
         if "range_change" in wl.extra:
             ifg = stack_interferograms(torch, wl, list(split_out), list(fp64_out), stream,
-                                       max(3, args.steps))
+                                       max(3, args.steps), exchange=exchange)
         del fp64_out
     del split_out
     plan.set_form(_lib.FORM_SPLIT, tuned["split"][0])
@@ -714,7 +741,7 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": s_ms, "higher_is_better": True,
-        "scaling": "strong" if partitioned else "weak",
+        "scaling": "strong" if partitioned or stack_blocks else "weak",
         "vs_baseline": None, "dtype": "f32 (split; FP64 orbit/ECEF/reference range)",
         "data": {"c3": "synthetic, seeded: complex Gaussian clutter + forward-projected point targets",
                  "c4": "synthetic, seeded: forward-projected scatterers + point targets, Mogi "

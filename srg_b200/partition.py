@@ -19,6 +19,12 @@ whose merge is azimuth_compress.cu:510-537).  Here:
   (``ordered_merge``), which reproduces the one-rank result bit for bit: a
   pixel ends with the image of the last burst that replaced it, whichever
   rank computed that image.
+
+A repeat-pass stack (acquisitions of one footprint, interferograms of the
+sequential pairs) is dealt in contiguous blocks of the date order instead
+(``block_partition``): each rank forms its block's images and the pairs
+within it, and the pair across a block's end needs one image from the next
+rank (``exchange_boundary``, one point-to-point transfer per boundary).
 """
 from __future__ import annotations
 
@@ -51,6 +57,39 @@ def owners(parts: Sequence[Sequence[int]], n: int) -> List[int]:
     if min(own, default=0) < 0:
         raise ValueError("a burst has no rank")
     return own
+
+
+def block_partition(n: int, nranks: int) -> List[List[int]]:
+    """Indices 0..n-1 in contiguous blocks, one per rank and in order (a
+    repeat-pass stack's date order), sizes differing by at most one (the first
+    n % nranks blocks one longer)."""
+    if nranks < 1:
+        raise ValueError("nranks must be >= 1")
+    q, r = divmod(n, nranks)
+    out, a = [], 0
+    for k in range(nranks):
+        b = a + q + (1 if k < r else 0)
+        out.append(list(range(a, b)))
+        a = b
+    return out
+
+
+def exchange_boundary(first_image, recv_buf, rank: int, world: int, dist, group=None):
+    """The one transfer a stack dealt in contiguous blocks needs for its
+    sequential pairs (k, k+1): every rank but the first sends its first image
+    to the previous rank, and every rank but the last receives the next rank's
+    first image into `recv_buf`, the second image of the pair across the end
+    of its block.  Every rank of a group of two or more takes part.  Returns
+    `recv_buf` on the ranks that receive, else None."""
+    ops = []
+    if rank > 0:
+        ops.append(dist.P2POp(dist.isend, first_image, rank - 1, group=group))
+    if rank < world - 1:
+        ops.append(dist.P2POp(dist.irecv, recv_buf, rank + 1, group=group))
+    if ops:
+        for w in dist.batch_isend_irecv(ops):
+            w.wait()
+    return recv_buf if rank < world - 1 else None
 
 
 def gather_outputs(outs, owner: Sequence[int], rank: int, dist, dst: int = 0, group=None) -> None:

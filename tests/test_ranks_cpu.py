@@ -179,3 +179,83 @@ def test_partitioned_scene_merges_like_one_rank_gloo(world):
                  _images(bursts, range(len(bursts)))).numpy()
     assert np.count_nonzero(ref) > 0
     assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+
+
+def test_block_partition():
+    from srg_b200 import partition
+    assert partition.block_partition(32, 3) == [list(range(0, 11)), list(range(11, 22)),
+                                                list(range(22, 32))]
+    assert partition.block_partition(32, 8) == [list(range(4 * k, 4 * k + 4)) for k in range(8)]
+    assert partition.block_partition(5, 1) == [[0, 1, 2, 3, 4]]
+    for n in range(1, 40):
+        for w in range(1, 9):
+            parts = partition.block_partition(n, w)
+            assert sum(parts, []) == list(range(n))
+            sizes = [len(p) for p in parts]
+            assert max(sizes) - min(sizes) <= 1
+    with pytest.raises(ValueError):
+        partition.block_partition(4, 0)
+
+
+def _pairs(images):
+    """A stand-in for the interferograms of sequential pairs (k, k+1)."""
+    import torch
+    return [torch.conj(images[k]) * images[k + 1] for k in range(len(images) - 1)]
+
+
+def _stack_worker(rank, world, port, n, out):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    from srg_b200 import partition
+    g = torch.Generator().manual_seed(11)
+    every = [torch.complex(torch.randn(6, 5, generator=g), torch.randn(6, 5, generator=g))
+             for _ in range(n)]
+    block = partition.block_partition(n, world)[rank]
+    mine = [every[i].clone() for i in block]
+    recv = torch.empty_like(mine[0])
+    nxt = partition.exchange_boundary(mine[0], recv, rank, world, dist)
+    imgs = mine + ([nxt] if nxt is not None else [])
+    pairs = _pairs(imgs)
+    out[rank] = (block[0], [p.numpy() for p in pairs])
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_stack_blocks_with_boundary_exchange_give_every_pair_gloo(world):
+    """A 7-image stack dealt in date-order blocks over `world` gloo ranks: with
+    the one exchange per block boundary the ranks' sequential pairs are, in
+    order, exactly the one-rank stack's 6 pairs, bit for bit."""
+    import numpy as np
+    import torch
+    import torch.multiprocessing as mp
+    n = 7
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as m:
+        out = m.dict()
+        port = _free_port()
+        procs = [ctx.Process(target=_stack_worker, args=(r, world, port, n, out))
+                 for r in range(world)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(120)
+            assert p.exitcode == 0
+        res = dict(out)
+    got = []
+    for r in range(world):
+        first, pairs = res[r]
+        got += pairs
+    g = torch.Generator().manual_seed(11)
+    every = [torch.complex(torch.randn(6, 5, generator=g), torch.randn(6, 5, generator=g))
+             for _ in range(n)]
+    want = [p.numpy() for p in _pairs(every)]
+    assert len(got) == n - 1
+    for a, b in zip(got, want):
+        assert np.array_equal(a, b)
