@@ -62,8 +62,10 @@ typedef struct srg_bp_options {
                           on the device or by srg_dropin_flush().  The merge
                           into *fdout of a call is complete when the next
                           call without overlap, srg_dropin_flush() or the
-                          process's normal exit returns.  0 (default): every
-                          call returns with its merge done, as the reference.
+                          process's normal exit returns.  The device then
+                          keeps two calls' scratch (two contexts, used in
+                          turn).  0 (default): every call returns with its
+                          merge done, as the reference.
                           The environment variable SRG_DROPIN_OVERLAP=1 sets
                           it in the process-wide defaults. */
 } srg_bp_options;
