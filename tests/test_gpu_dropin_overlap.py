@@ -222,3 +222,26 @@ def test_overlapped_wait_that_gives_up_comes_back_from_flush(torch_cuda):
     assert timeouts > 0
     rc, again = run()
     assert rc == _lib.SRG_OK and np.array_equal(again.view(np.uint32), full.view(np.uint32))
+
+
+def test_overlapped_and_waiting_calls_mixed_keep_call_order(torch_cuda):
+    """Overlapped and waiting calls alternating on one .geo: a waiting call
+    waits for every earlier merge, so the file is the one the calls make
+    when each waits for its own."""
+    base, bursts, init = three_bursts()
+    want = run_calls(bursts * 2, base, init, _lib.FORM_SPLIT, overlap=0)
+    with tempfile.TemporaryDirectory() as td:
+        dem_path, geo_path = os.path.join(td, "e.dem"), os.path.join(td, "s.geo")
+        np.ascontiguousarray(base.dem, np.int16).tofile(dem_path)
+        init.tofile(geo_path)
+        fd_dem, fd_geo = os.open(dem_path, os.O_RDWR), os.open(geo_path, os.O_RDWR)
+        try:
+            for i, b in enumerate(bursts * 2):
+                api.azimuth_compress_status(b, fd_geo, fd_dem, form=_lib.FORM_SPLIT,
+                                            overlap=(i % 3 != 2))
+            api.dropin_flush()
+        finally:
+            os.close(fd_dem)
+            os.close(fd_geo)
+        got = np.fromfile(geo_path, np.complex64).reshape(base.demlength, base.demwidth)
+    assert np.array_equal(got, want)
