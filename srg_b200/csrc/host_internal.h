@@ -36,11 +36,17 @@ struct DevBuf {
             return fail(SRG_E_NOMEM, "cudaMalloc(%zu) failed: %s", want, cudaGetErrorString(e));
         }
         cap = want;
-        // new scratch starts at zero (flag words are read before any kernel writes them)
+        // New scratch starts at zero (flag words are read before any kernel
+        // writes them).  The zeroing runs on the legacy stream, which the
+        // library's non-blocking streams do not wait for: it must be finished
+        // before the buffer is handed out, or a kernel on another stream could
+        // write the buffer first and have it zeroed after (as when another
+        // context's persistent kernel holds every SM and delays the zeroing).
         e = cudaMemset(p, 0, want);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(0);
         if (e != cudaSuccess) {
             cudaGetLastError();
-            return fail(SRG_E_CUDA, "cudaMemset of new scratch failed: %s", cudaGetErrorString(e));
+            return fail(SRG_E_CUDA, "zeroing of new scratch failed: %s", cudaGetErrorString(e));
         }
         return SRG_OK;
     }

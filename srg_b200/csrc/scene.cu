@@ -75,10 +75,11 @@ int alloc(void **p, size_t bytes) {
         *p = nullptr;
         return fail(SRG_E_NOMEM, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
     }
-    // zeroed: the flag words are read before any kernel has written them
-    if (cudaMemset(*p, 0, n) != cudaSuccess) {
+    // zeroed: the flag words are read before any kernel has written them; the
+    // zeroing (legacy stream) is finished before the caller's streams use it
+    if (cudaMemset(*p, 0, n) != cudaSuccess || cudaStreamSynchronize(0) != cudaSuccess) {
         cudaGetLastError();
-        return fail(SRG_E_CUDA, "cudaMemset of plan memory failed");
+        return fail(SRG_E_CUDA, "zeroing of plan memory failed");
     }
     return SRG_OK;
 }
@@ -438,7 +439,8 @@ int srg_scene_sync(srg_scene *s, void *stream) {
     int h[2] = {0, 0};
     SCK(cudaMemcpy(h, s->d_flags, sizeof h, cudaMemcpyDeviceToHost));
     if (h[1]) {
-        cudaMemset(s->d_flags + 1, 0, sizeof(int));
+        cudaMemsetAsync(s->d_flags + 1, 0, sizeof(int), st);
+        cudaStreamSynchronize(st);
         return fail(SRG_E_TIMEOUT, "device error word 0x%x (TMA wait timed out)", h[1]);
     }
     return SRG_OK;

@@ -245,3 +245,61 @@ def test_overlapped_and_waiting_calls_mixed_keep_call_order(torch_cuda):
             os.close(fd_geo)
         got = np.fromfile(geo_path, np.complex64).reshape(base.demlength, base.demwidth)
     assert np.array_equal(got, want)
+
+
+FRESH = r"""
+import json, os, sys, tempfile
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+import torch
+from srg_b200 import _lib, api, workloads
+iw = workloads.config3().bursts
+b0 = iw[0].b
+out = {}
+for ov in (1, 0):   # overlapped first: every context's first call overlapped
+    api.set_default_form(_lib.FORM_SPLIT, overlap=ov)
+    with tempfile.TemporaryDirectory() as td:
+        dem_path, geo_path = os.path.join(td, "e.dem"), os.path.join(td, "s.geo")
+        np.ascontiguousarray(b0.dem, np.int16).tofile(dem_path)
+        with open(geo_path, "wb") as f:
+            f.truncate(b0.demlength * b0.demwidth * 8)
+        fd_dem, fd_geo = os.open(dem_path, os.O_RDWR), os.open(geo_path, os.O_RDWR)
+        hosts = [db.burst.cpu().pin_memory() for db in iw]
+        calls = [api.prepare_azimuth_compress(db.b, fd_geo, fd_dem, burst=h.numpy())
+                 for db, h in zip(iw, hosts)]
+        per = []
+        for c in calls:
+            c()
+            per.append(api.dropin_last_bytes())
+        api.dropin_flush()
+        os.close(fd_dem)
+        os.close(fd_geo)
+        geo = np.fromfile(geo_path, np.complex64)
+    out[ov] = (per, int(np.count_nonzero(geo)), float(np.abs(geo).sum()),
+               geo.view(np.uint32)[::997].tolist())
+api.set_default_form(_lib.FORM_SPLIT, overlap=0)
+print(json.dumps({str(k): v for k, v in out.items()}))
+"""
+
+
+def test_first_overlapped_calls_of_a_process_match_waiting_calls(torch_cuda):
+    """A fresh process whose first drop-in calls are overlapped, on the IW
+    scene's 27 bursts (the kernel of one call holds every SM while the next
+    call sets up its context): every call reports the bytes and the .geo comes
+    out as with waiting calls.  New device scratch is zeroed before it is
+    handed out: when the zeroing was left on the legacy stream, the second
+    call's azimuth centres were zeroed after they were written in about one
+    fresh run in two, and that call formed nothing (the check is as timing
+    dependent as that race was)."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    p = subprocess.run([sys.executable, "-c", FRESH, root], capture_output=True, text=True,
+                       timeout=900)
+    assert p.returncode == 0, p.stderr[-2000:]
+    res = json.loads(p.stdout.strip().splitlines()[-1])
+    ov, wait = res["1"], res["0"]
+    assert ov[0] == wait[0]          # per-call bytes in and out
+    assert ov[1] == wait[1] > 0      # formed pixels in the .geo
+    assert ov[2] == wait[2] and ov[3] == wait[3]
