@@ -178,6 +178,7 @@ def e2e_dropin(torch, wl, steps, form, separate=False, bursts=None, overlap=0):
                     call()
             api.dropin_flush()
             torch.cuda.synchronize()
+            torch.cuda.nvtx.range_push("e2e_overlapped" if overlap else "e2e_waiting")
             t0 = time.perf_counter()
             for _ in range(steps):
                 for call in calls:
@@ -185,6 +186,7 @@ def e2e_dropin(torch, wl, steps, form, separate=False, bursts=None, overlap=0):
                 api.dropin_flush()
             torch.cuda.synchronize()
             dt = (time.perf_counter() - t0) / steps
+            torch.cuda.nvtx.range_pop()
         finally:
             api.dropin_flush()
             api.set_default_form(form, overlap=0)
@@ -581,6 +583,11 @@ def main():
                          "--workload c1 or c3 instead of the benchmark")
     ap.add_argument("--samples", default="random", choices=["random", "forward"],
                     help="profiling driver, c1: random or forward-projected range lines")
+    ap.add_argument("--e2e-only", default=None, choices=["overlapped", "waiting"],
+                    help="only the drop-in end to end on --workload c1, c3 or c4, calls "
+                         "overlapped or waiting (NVTX ranges e2e_overlapped / e2e_waiting); not "
+                         "for ncu: its serialised launches hold the range lines of the gated "
+                         "kernel back")
     args = ap.parse_args()
     if args.profile_shapes is not None:
         import torch
@@ -591,6 +598,18 @@ def main():
     if args.workload == "rc":
         import torch
         range_compression_bench(torch, max(1, args.steps), max(1, args.warmup))
+        return
+    if args.e2e_only is not None:
+        import torch
+        from srg_b200 import _lib, workloads
+        wl = {"c1": workloads.config1, "c3": workloads.config3,
+              "c4": workloads.config4}[args.workload]()
+        dt, h2d, d2h = e2e_dropin(torch, wl, max(1, args.e2e_steps), _lib.FORM_SPLIT,
+                                  separate=args.workload == "c4",
+                                  overlap=1 if args.e2e_only == "overlapped" else 0)
+        print(json.dumps({"e2e_only": args.e2e_only, "workload": args.workload,
+                          "s_per_step": dt, "value": wl.terms / dt / 1e9, "unit": UNIT,
+                          "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}))
         return
     pinned = [int(x) for x in args.shapes.split(",")] if args.shapes else None
     rank, world, local = dist_env()

@@ -308,7 +308,9 @@ int srg_scene_interp(const srg_scene *s);
 int srg_interp_error(const float *lines, long long ld, int nlines, int nsamps, int sample_lines,
                      double *err_linear, double *err_oversampled, void *stream);
 
-/* Select a kernel shape, or a form and shape (-1: that form's default). */
+/* Select a kernel shape, or a form and shape (-1: that form's default).
+ * Blocking: waits for the device to finish the work in flight (the plan's
+ * burst descriptors are rewritten), on any stream. */
 int srg_scene_set_shape(srg_scene *s, int tile_cfg);
 int srg_scene_set_form(srg_scene *s, int form, int tile_cfg);
 /* Kernel shape index in use. */

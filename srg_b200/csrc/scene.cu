@@ -106,8 +106,14 @@ int set_kernel(srg_scene *s, int idx) {
         std::memset(&hm[i], 0, sizeof(CUtensorMap));
         B.tmap = make_tmap(B, ke.shape.window, ke.shape.chunk, &hm[i]) == 0 ? i : -1;
     }
+    // An earlier pass of the plan may still read the descriptors on a caller's
+    // non-blocking stream, which the legacy stream's copies below do not wait
+    // for: wait for the device first.  The copies are from pageable memory and
+    // may still be in flight when cudaMemcpy returns: wait for them too.
+    SCK(cudaDeviceSynchronize());
     SCK(cudaMemcpy(s->d_bursts, s->hb.data(), sizeof(BurstDev) * s->n, cudaMemcpyHostToDevice));
     SCK(cudaMemcpy(s->d_tmaps, hm.data(), sizeof(CUtensorMap) * s->n, cudaMemcpyHostToDevice));
+    SCK(cudaStreamSynchronize(0));
     const size_t need = tile_list_bytes(total);
     if (need > s->tiles_cap) {
         cudaFree(s->d_tiles);
@@ -374,7 +380,8 @@ int srg_scene_create(const srg_burst_desc *bursts, int n, float *scene, int64_t 
     }
     s->total_lines = (int)lines;
     if (cudaMemcpy(s->d_orbit, horb.data(), sizeof(double) * orbit, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(s->d_jobs, jobs.data(), sizeof(CentreJob) * n, cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaMemcpy(s->d_jobs, jobs.data(), sizeof(CentreJob) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaStreamSynchronize(0) != cudaSuccess) {  // (pageable copies may still be in flight)
         cudaGetLastError();
         srg_scene_destroy(s);
         return fail(SRG_E_CUDA, "plan upload failed");
