@@ -68,11 +68,27 @@ typedef struct srg_bp_options {
                           merge done, as the reference.
                           The environment variable SRG_DROPIN_OVERLAP=1 sets
                           it in the process-wide defaults. */
+    int tile_shear;    /* lines per 32 grid columns by which the tiles are
+                          sheared (a tile's column x sits floor(tile_shear x /
+                          32) lines lower), in [-SRG_MAX_TILE_SHEAR,
+                          SRG_MAX_TILE_SHEAR] and offsetting a tile's columns
+                          by fewer lines than it is tall (0: rectangular
+                          tiles); SRG_TILE_SHEAR_AUTO (the default): chosen
+                          per burst from its geometry so that a tile's rows of
+                          pixels follow the lines of constant azimuth centre.
+                          The warp-specialised shapes take it; the
+                          first-generation shapes keep rectangular tiles.
+                          Results depend on it only through the split form's
+                          per-tile closed forms (within its error budget). */
 } srg_bp_options;
+
+#define SRG_TILE_SHEAR_AUTO 1000
+#define SRG_MAX_TILE_SHEAR 8
 
 /* Fill *o with the defaults (split form, tuned tile, current device,
  * centres on the GPU, quiet, default wait limit, range band, no scratch
- * limit, calls not overlapped unless SRG_DROPIN_OVERLAP=1). */
+ * limit, calls not overlapped unless SRG_DROPIN_OVERLAP=1, tile shear from
+ * the geometry). */
 void srg_bp_default_options(srg_bp_options *o);
 
 /* Message of the last failing call on this thread ("" if none). */
@@ -208,6 +224,13 @@ typedef struct srg_burst_desc {
  * enqueueing; srg_sync_check() reports device-side errors. */
 int srg_bp_bursts_device(const srg_burst_desc *bursts, int n,
                          const srg_bp_options *opts, void *stream);
+
+/* Tile shear (lines per 32 columns) and tiles across and down that shape
+ * `tile_cfg` (-1: the split form's default) takes for burst *b under
+ * `tile_shear` (SRG_TILE_SHEAR_AUTO: the geometric choice).  Host only: no
+ * device memory is read, only the descriptor's scalars. */
+int srg_tile_shear(const srg_burst_desc *b, int tile_cfg, int tile_shear, int *shear,
+                   int *tiles_x, int *tiles_y);
 
 /* One burst whose range lines are still being copied to the device, in
  * blocks of pulse rows, by the caller (a pipelined upload; the drop-in entry

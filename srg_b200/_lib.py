@@ -23,6 +23,8 @@ SRG_E_UNSUPPORTED = -6
 
 FORM_FP64 = 0
 FORM_SPLIT = 1
+TILE_SHEAR_AUTO = 1000   # srg_bp_options.tile_shear: chosen from the geometry
+MAX_TILE_SHEAR = 8
 
 _dp = C.POINTER(C.c_double)
 _fp = C.POINTER(C.c_float)
@@ -32,7 +34,8 @@ _ip = C.POINTER(C.c_int)
 class Options(C.Structure):
     _fields_ = [("form", C.c_int), ("tile_cfg", C.c_int), ("device", C.c_int),
                 ("centres_on_host", C.c_int), ("verbose", C.c_int), ("spin_limit", C.c_int),
-                ("full_lines", C.c_int), ("scratch_limit", C.c_longlong), ("overlap", C.c_int)]
+                ("full_lines", C.c_int), ("scratch_limit", C.c_longlong), ("overlap", C.c_int),
+                ("tile_shear", C.c_int)]
 
 
 class BurstDesc(C.Structure):
@@ -122,6 +125,8 @@ _SIGS = {
     "srg_scene_shape": (C.c_int, [C.c_void_p]),
     "srg_scene_destroy": (None, [C.c_void_p]),
     "srg_tile_config_count": (C.c_int, []),
+    "srg_tile_shear": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int),
+                                 C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "srg_tile_config": (C.c_int, [C.c_int, _ip, _ip, _ip, _ip, _ip]),
     "srg_tile_config_name": (C.c_char_p, [C.c_int]),
     "srg_forward_project_device": (C.c_int, [C.POINTER(BurstDesc), C.c_void_p, C.c_int64, C.c_void_p,

@@ -230,14 +230,17 @@ def _stream_ptr(stream) -> Optional[int]:
 
 
 def backproject(bursts: Sequence[DeviceBurst], form: int = FORM_SPLIT, tile_cfg: int = -1,
-                stream=None, sync: bool = True, coefs=None) -> None:
+                stream=None, sync: bool = True, coefs=None, tile_shear: Optional[int] = None) -> None:
     """Backproject device bursts into their `out` tensors (one launch).
     coefs: optional per-burst device tensors of azimuth-centre parabolas
     ([nlines][3] float64, from ``line_centres``); without them the centres are
-    solved on the device first."""
+    solved on the device first.  tile_shear: srg_bp_options.tile_shear (None:
+    chosen from each burst's geometry)."""
     ptrs = [c.data_ptr() for c in coefs] if coefs is not None else [0] * len(bursts)
     arr = (BurstDesc * len(bursts))(*[db.desc(p) for db, p in zip(bursts, ptrs)])
     o = default_options(form, tile_cfg)
+    if tile_shear is not None:
+        o.tile_shear = int(tile_shear)
     st = _stream_ptr(stream)
     check(lib().srg_bp_bursts_device(arr, len(bursts), C.byref(o), C.c_void_p(st)))
     if sync:
@@ -438,11 +441,13 @@ class Scene:
     from a CUDA graph on a non-default stream."""
 
     def __init__(self, bursts: Sequence[DeviceBurst], raster=None, form: int = FORM_SPLIT,
-                 tile_cfg: int = -1):
+                 tile_cfg: int = -1, tile_shear: Optional[int] = None):
         self.bursts = list(bursts)
         self.raster = raster
         self._descs = (BurstDesc * len(self.bursts))(*[db.desc() for db in self.bursts])
         o = default_options(form, tile_cfg)
+        if tile_shear is not None:
+            o.tile_shear = int(tile_shear)
         h = C.c_void_p()
         if raster is not None:
             args = (C.c_void_p(raster.data_ptr()), raster.stride(0), raster.shape[0], raster.shape[1])

@@ -212,7 +212,9 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
     extern __shared__ __align__(128) unsigned char dsm[];
     __shared__ CtlWS ctl;
     __shared__ StageHdr hdr[NS];
-    __shared__ double lat_tab[TY][4], lon_tab[TX][2];  // per-tile line / column factors of the ECEF
+    // per-tile line / column factors of the ECEF (a sheared tile touches
+    // TY + lspan lines, lspan < kMaxShear)
+    __shared__ double lat_tab[TY + kMaxShear][4], lon_tab[TX][2];
     PP *prm = reinterpret_cast<PP *>(dsm);
     float2 *samp0;
     {
@@ -282,8 +284,14 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
         while (b + 1 < nbursts && bursts[b + 1].tile_base <= tile) ++b;
         const BurstDev &B = bursts[b];
         const int ti = tile - B.tile_base;
+        // pixel (x, y) of the tile: column px0 + x, line
+        // ly0 + y + tile_dline(shear, x) - dmax; its line factors are
+        // lat_tab[y + tile_dline(shear, x) - dmax + lspan] (the table starts
+        // at line ly0 - lspan)
+        const int shear = B.shear;
         const int px0 = B.firstpix + (ti % B.tiles_x) * TX;
         const int ly0 = (ti / B.tiles_x) * TY;
+        const int dmax = tile_dmax(shear, TX), lspan = tile_span(shear, TX);
 
         // ---- prologue ----
         // Phase A: consumers solve their pixels' aperture windows; the producer
@@ -298,11 +306,11 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
             for (int m = 0; m < M; ++m) {
                 const int bi = warp + NC * m;
                 const int x = PBX * (bi % BX) + lane % PBX, y = PBY * (bi / BX) + lane / PBX;
-                const int px = px0 + x, line = ly0 + y;
+                const int px = px0 + x, line = ly0 + y + tile_dline(shear, x) - dmax;
                 X[m][0] = X[m][1] = X[m][2] = 0.0;
                 azs[m] = aze[m] = 0;
                 hgt[m] = 0;
-                if (px <= B.lastpix_eff && line < B.nlines) {
+                if (px <= B.lastpix_eff && line >= 0 && line < B.nlines) {
                     hgt[m] = B.dem[(long long)line * B.dem_ld + px];
                     pixel_window(B, pixel_azoff(B, B.coef + 3 * line, px), azs[m], aze[m]);
                     if (aze[m] > azs[m]) {
@@ -324,23 +332,26 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                 atomicMin(&ctl.aze_min, emin);
             }
         } else {
-            for (int r = lane; r < TY + TX; r += 32) {
-                if (r < TY) {
-                    const LineTrig L = line_trig(B, ly0 + r);
+            for (int r = lane; r < TY + lspan + TX; r += 32) {
+                if (r < TY + lspan) {
+                    const LineTrig L = line_trig(B, ly0 - lspan + r);
                     lat_tab[r][0] = L.slat;
                     lat_tab[r][1] = L.clat;
                     lat_tab[r][2] = L.re;
                     lat_tab[r][3] = L.rez;
                 } else {
-                    col_trig(B, px0 + r - TY, lon_tab[r - TY][0], lon_tab[r - TY][1]);
+                    col_trig(B, px0 + r - TY - lspan, lon_tab[r - TY - lspan][0],
+                             lon_tab[r - TY - lspan][1]);
                 }
             }
             __syncwarp();
             if (lane == 0) {
-                // tile-centre pixel (inside the tile, so its factors are in the tables)
+                // tile-centre pixel, inside the burst (its factors are in the
+                // tables; the clamp only guards the index)
                 const int cx = min(max(px0 + TX / 2, B.firstpix), B.lastpix_eff);
-                const int cy = min(ly0 + TY / 2, B.nlines - 1);
-                const int ty = cy - ly0, tx = cx - px0;
+                const int tx = cx - px0;
+                const int cy = min(max(ly0 + TY / 2 + tile_dline(shear, tx) - dmax, 0), B.nlines - 1);
+                const int ty = min(max(cy - ly0 + lspan, 0), TY + lspan - 1);
                 pixel_ecef_from(lat_tab[ty][0], lat_tab[ty][1], lat_tab[ty][2], lat_tab[ty][3],
                                 lon_tab[tx][0], lon_tab[tx][1],
                                 (double)B.dem[(long long)cy * B.dem_ld + cx], ctl.xc[0], ctl.xc[1],
@@ -355,8 +366,8 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                 for (int m = 0; m < M; ++m) {
                     const int bi = warp + NC * m;
                     const int x = PBX * (bi % BX) + lane % PBX, y = PBY * (bi / BX) + lane / PBX;
-                    const int px = px0 + x, line = ly0 + y;
-                    if (px <= B.lastpix_eff && line < B.nlines)
+                    const int px = px0 + x, line = ly0 + y + tile_dline(shear, x) - dmax;
+                    if (px <= B.lastpix_eff && line >= 0 && line < B.nlines)
                         B.out[(long long)line * B.out_ld + (px - B.out_pix0)] = make_float2(0.f, 0.f);
                 }
             } else if (lane == 0) {
@@ -376,7 +387,8 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                 if (aze[m] > azs[m]) {
                     const int bi = warp + NC * m;
                     const int x = PBX * (bi % BX) + lane % PBX, y = PBY * (bi / BX) + lane / PBX;
-                    pixel_ecef_from(lat_tab[y][0], lat_tab[y][1], lat_tab[y][2], lat_tab[y][3],
+                    const int ty = y + tile_dline(shear, x) - dmax + lspan;  // the pixel's table line
+                    pixel_ecef_from(lat_tab[ty][0], lat_tab[ty][1], lat_tab[ty][2], lat_tab[ty][3],
                                     lon_tab[x][0], lon_tab[x][1], (double)hgt[m], X[m][0], X[m][1],
                                     X[m][2]);
                 }
@@ -969,8 +981,9 @@ bp_ws(const BurstDev *__restrict__ bursts, int nbursts, int total_tiles,
                 for (int m = 0; m < M; ++m) {
                     const int bi = warp + NC * m;
                     const int x = PBX * (bi % BX) + lane % PBX, y = PBY * (bi / BX) + lane / PBX;
-                    const int px = px0 + x, line = ly0 + y;
-                    if (px <= B.lastpix_eff && line < B.nlines) {
+                    const int px = px0 + x,
+                              line = ly0 + y + tile_dline(B.shear, x) - tile_dmax(B.shear, TX);
+                    if (px <= B.lastpix_eff && line >= 0 && line < B.nlines) {
                         float2 o = make_float2(0.f, 0.f);
                         const int n = aze[m] - azs[m];
                         if (n > 0) {

@@ -74,7 +74,8 @@ int env_overlap() {
     }();
     return v;
 }
-srg_bp_options g_default_opts = {SRG_FORM_SPLIT, -1, -1, 0, 0, 0, 0, 0, env_overlap()};
+srg_bp_options g_default_opts = {SRG_FORM_SPLIT, -1, -1, 0, 0, 0, 0, 0, env_overlap(),
+                                 SRG_TILE_SHEAR_AUTO};
 std::mutex g_opts_mu;
 
 DevCtx g_ctx[64];
@@ -450,6 +451,50 @@ int validate_desc(const srg_burst_desc &d) {
     return SRG_OK;
 }
 
+// Azimuth-centre and range slopes of a burst per grid line and per column,
+// at the grid's centre at height 0 on the WGS-84 ellipsoid: a ground step dx
+// moves a point's time of closest approach by about (v . dx) / |v|^2
+// (mid-burst velocity v), and its range by about e . dx (e the unit vector
+// from the mid-burst position).  Zero without a velocity, position and PRF (a
+// caller that passes its own azimuth centres need not give them).
+static void centre_slopes(const srg_burst_desc &d, BurstDev &B) {
+    B.slope_line = B.slope_col = B.rbin_line = B.rbin_col = 0.0;
+    const double *v = d.vel_mid, *s = d.xyz_mid;
+    const double vv = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    if (!(vv > 0.0) || !std::isfinite(vv) || !(d.prf > 0.0) || !std::isfinite(d.prf) ||
+        !(d.dmrg > 0.0))
+        return;
+    auto ecef = [](double lat_deg, double lon_deg, double x[3]) {
+        const double a = 6378137.0, e2 = 0.0066943799901499996, r = M_PI / 180.0;
+        const double sl = std::sin(lat_deg * r), cl = std::cos(lat_deg * r);
+        const double n = a / std::sqrt(1.0 - e2 * sl * sl);
+        x[0] = n * cl * std::cos(lon_deg * r);
+        x[1] = n * cl * std::sin(lon_deg * r);
+        x[2] = n * (1.0 - e2) * sl;
+    };
+    const double lat = d.firstlat + (d.firstline + 0.5 * d.nlines) * d.deltalat;
+    const double lon = d.firstlon + 0.5 * (d.firstpix + d.lastpix) * d.deltalon;
+    double p0[3], pl[3], pc[3];
+    ecef(lat, lon, p0);
+    ecef(lat + d.deltalat, lon, pl);
+    ecef(lat, lon + d.deltalon, pc);
+    auto dot = [](const double *a, const double *p, const double *q) {
+        return a[0] * (p[0] - q[0]) + a[1] * (p[1] - q[1]) + a[2] * (p[2] - q[2]);
+    };
+    const double k = d.prf / vv;
+    const double r = std::sqrt((p0[0] - s[0]) * (p0[0] - s[0]) + (p0[1] - s[1]) * (p0[1] - s[1]) +
+                               (p0[2] - s[2]) * (p0[2] - s[2]));
+    const double e[3] = {(p0[0] - s[0]) / r, (p0[1] - s[1]) / r, (p0[2] - s[2]) / r};
+    const double sl = k * dot(v, pl, p0), sc = k * dot(v, pc, p0);
+    const double rl = dot(e, pl, p0) / d.dmrg, rc = dot(e, pc, p0) / d.dmrg;
+    if (std::isfinite(sl) && std::isfinite(sc) && std::isfinite(rl) && std::isfinite(rc)) {
+        B.slope_line = sl;
+        B.slope_col = sc;
+        B.rbin_line = rl;
+        B.rbin_col = rc;
+    }
+}
+
 BurstDev make_burst_dev(const srg_burst_desc &d, const double *coef) {
     BurstDev B{};
     B.burst = reinterpret_cast<const float2 *>(d.burst);
@@ -491,7 +536,50 @@ BurstDev make_burst_dev(const srg_burst_desc &d, const double *coef) {
     B.K_lo = (float)(B.K - (double)B.K_hi);
     B.K_f = B.K_hi;
     B.inv_dmrg_f = (float)B.inv_dmrg;
+    centre_slopes(d, B);
     return B;
+}
+
+int set_tiles(BurstDev &B, const KernelEntry &ke, int shear) {
+    static_assert(kMaxShear == SRG_MAX_TILE_SHEAR, "shear limit");
+    const int tx = ke.shape.tx, ty = ke.shape.ty;
+    if (shear != SRG_TILE_SHEAR_AUTO &&
+        (shear < -kMaxShear || shear > kMaxShear || tile_span(shear, tx) >= ty))
+        return fail(SRG_E_ARG, "tile_shear %d: outside [-%d, %d] or a line offset of %d over a "
+                    "tile of %d x %d", shear, kMaxShear, kMaxShear, tile_span(shear, tx), tx, ty);
+    const int nx = B.lastpix_eff - B.firstpix + 1;
+    int best = 0;
+    if (ke.shears && shear != SRG_TILE_SHEAR_AUTO) {
+        best = shear;
+    } else if (ke.shears && nx > 0 && B.nlines > 0) {
+        // A tile's pixels span aperture + spread pulses, the spread of their
+        // azimuth centres; its tile rows need span more lines.  A shear of s
+        // lines per 32 columns turns the per-column slopes by s / 32 of the
+        // per-line ones.  Shears that widen a tile's range-bin window by more
+        // than kShearBins are passed over (the staged window is fixed).
+        constexpr double kShearBins = 8.0;
+        auto slots = [&](int s) {
+            const double spread = std::fabs(B.slope_col + s / 32.0 * B.slope_line) * (tx - 1) +
+                                  std::fabs(B.slope_line) * (ty - 1);
+            return (B.aperture + spread) * (double)(B.nlines + tile_span(s, tx));
+        };
+        auto bins = [&](int s) { return std::fabs(B.rbin_col + s / 32.0 * B.rbin_line) * (tx - 1); };
+        double least = slots(0);
+        for (int m = 1; m <= kMaxShear; ++m) {
+            for (const int s : {-m, m}) {
+                if (tile_span(s, tx) >= ty || bins(s) > bins(0) + kShearBins) continue;
+                const double v = slots(s);
+                if (v < least * (1.0 - 1e-9)) {
+                    least = v;
+                    best = s;
+                }
+            }
+        }
+    }
+    B.shear = best;
+    B.tiles_x = nx > 0 ? (nx + tx - 1) / tx : 0;
+    B.tiles_y = B.nlines > 0 ? (B.nlines + tile_span(best, tx) + ty - 1) / ty : 0;
+    return SRG_OK;
 }
 
 int make_tmap(const BurstDev &B, int box_x, int box_y, CUtensorMap *out) {
@@ -680,9 +768,9 @@ int run_bursts(DevCtx &c, const srg_burst_desc *descs, int n, const srg_bp_optio
         }
         BurstDev B = make_burst_dev(d, coef);
         if (o.spin_limit > 0) B.spin = (unsigned)o.spin_limit;
-        const int nx = B.lastpix_eff - B.firstpix + 1;
-        B.tiles_x = nx > 0 ? (nx + TX - 1) / TX : 0;
-        B.tiles_y = (B.nlines + TY - 1) / TY;
+        // row blocks copied back while the sum runs count whole tile rows of
+        // rectangular tiles
+        if ((rc = set_tiles(B, *ke, gated && gate->rb ? 0 : o.tile_shear))) return rc;
         B.tile_base = total;
         total += B.tiles_x * B.tiles_y;
         max_burst_tiles = std::max(max_burst_tiles, B.tiles_x * B.tiles_y);
@@ -763,6 +851,7 @@ void srg_bp_default_options(srg_bp_options *o) {
     o->full_lines = 0;
     o->scratch_limit = 0;
     o->overlap = env_overlap();
+    o->tile_shear = SRG_TILE_SHEAR_AUTO;
 }
 
 const char *srg_last_error(void) { return g_err.c_str(); }
@@ -774,6 +863,20 @@ void srg_set_default_options(const srg_bp_options *o) {
 }
 
 int srg_tile_config_count(void) { return kNumKernels; }
+
+int srg_tile_shear(const srg_burst_desc *b, int tile_cfg, int tile_shear, int *shear,
+                   int *tiles_x, int *tiles_y) {
+    if (!b || !shear || !tiles_x || !tiles_y) return fail(SRG_E_ARG, "null argument");
+    const KernelEntry *ke = tile_cfg < 0 ? pick_kernel(SRG_FORM_SPLIT, -1)
+                            : tile_cfg < kNumKernels ? &kKernels[tile_cfg] : nullptr;
+    if (!ke) return fail(SRG_E_ARG, "shape index %d", tile_cfg);
+    BurstDev B = make_burst_dev(*b, nullptr);
+    if (const int rc = set_tiles(B, *ke, tile_shear)) return rc;
+    *shear = B.shear;
+    *tiles_x = B.tiles_x;
+    *tiles_y = B.tiles_y;
+    return SRG_OK;
+}
 
 const char *srg_tile_config_name(int idx) {
     if (idx < 0 || idx >= kNumKernels) return "";

@@ -31,6 +31,12 @@ struct BurstDev {
     int out_pix0;
     int aperture, ap2;        // ap2 = aperture / 2 (integer division, as the reference)
     int tiles_x, tiles_y, tile_base;
+    // Lines per 32 columns by which the tiles are sheared (0: rectangular
+    // tiles); see tile_dline.
+    int shear;
+    // Azimuth-centre slopes (pulses) and range slopes (bins) per grid line
+    // and per column: host estimates from the geometry that choose the shear
+    double slope_line, slope_col, rbin_line, rbin_col;
     int tmap;                 // index of this burst's TMA descriptor, -1 = none
     unsigned spin;            // polls of a bounded device-side wait (the launch's first burst's)
     // The lines held in device memory: logical range bins [bin0, bin0 + nbins)
@@ -57,6 +63,28 @@ struct BurstDev {
     int *rb_count, *rb_expect, *rb_done, *rb_order;
     int rb_tile_rows, rb_seq;
 };
+
+// Largest tile shear, in lines per 32 columns.
+constexpr int kMaxShear = 8;
+
+// Tile geometry.  Tile ti of a burst (tiles_x per tile row) covers columns
+// px0 + [0, tx), px0 = firstpix + (ti % tiles_x) * tx, and on its column
+// px0 + x the lines ly0 + y + tile_dline(shear, x) - tile_dmax(shear, tx),
+// y in [0, ty), with ly0 = (ti / tiles_x) * ty.  On every column the tile
+// rows partition the lines; with the shear a tile's rows of pixels follow
+// the lines of constant azimuth centre across the columns, so its pixels
+// share more of their apertures.  Tile row r touches the lines
+// [r ty - span, r ty + ty), span = tile_span(shear, tx) < ty.
+__host__ __device__ __forceinline__ int tile_dline(int shear, int x) {
+    const int v = shear * x;
+    return v >= 0 ? v / 32 : -((31 - v) / 32);  // floor(shear * x / 32)
+}
+__host__ __device__ __forceinline__ int tile_dmax(int shear, int tx) {
+    return shear > 0 ? tile_dline(shear, tx - 1) : 0;
+}
+__host__ __device__ __forceinline__ int tile_span(int shear, int tx) {
+    return shear > 0 ? tile_dline(shear, tx - 1) : -tile_dline(shear, tx - 1);
+}
 
 // Grid lines run against the pulses (the azimuth centre of the last formed
 // line precedes the first's): a burst's tiles are then taken from the last

@@ -115,6 +115,12 @@ int kernel_index(const KernelEntry *e);
 void ensure_attrs(DevCtx &c, int idx);
 int validate_desc(const srg_burst_desc &d);
 BurstDev make_burst_dev(const srg_burst_desc &d, const double *coef);
+// B.shear, B.tiles_x and B.tiles_y for the tiles of kernel `ke`.  shear:
+// srg_bp_options::tile_shear; SRG_TILE_SHEAR_AUTO takes the shear that, by
+// B's azimuth-centre slopes, leaves the fewest pixel-pulse slots per tile
+// row.  Kernels with rectangular tiles get 0.  SRG_E_ARG for a shear out of
+// range.
+int set_tiles(BurstDev &B, const KernelEntry &ke, int shear);
 // 0 and *out filled when a TMA descriptor can describe the burst, else -1.
 int make_tmap(const BurstDev &B, int box_x, int box_y, CUtensorMap *out);
 double ref_pi();

@@ -243,7 +243,11 @@ __global__ void __launch_bounds__(256) merge_scene_kernel(const BurstDev *__rest
                 const int ll = l - B.firstline;
                 if (ll < 0 || ll >= B.nlines || c < B.firstpix || c > B.lastpix_eff) continue;
                 if (tmask) {
-                    const int ti = (ll >> ty_log2) * B.tiles_x + ((c - B.firstpix) >> tx_log2);
+                    // the tile of (ll, c): its column block, then the tile
+                    // row from the line less the column's line offset
+                    const int xc = c - B.firstpix, x = xc & ((1 << tx_log2) - 1);
+                    const int lr = ll - tile_dline(B.shear, x) + tile_dmax(B.shear, 1 << tx_log2);
+                    const int ti = (lr >> ty_log2) * B.tiles_x + (xc >> tx_log2);
                     if (!tmask[B.tile_base + ti]) continue;
                 }
                 const float2 v = B.out[(long long)ll * B.out_ld + (c - B.out_pix0)];
@@ -353,13 +357,25 @@ __global__ void __launch_bounds__(256) tile_mask_kernel(const BurstDev *__restri
     const int lane = threadIdx.x & 31;
     const int ti = blockIdx.x * 8 + (threadIdx.x >> 5);
     if (ti >= B.tiles_x * B.tiles_y) return;
-    const int px0 = B.firstpix + (ti % B.tiles_x) * tx;
+    const int col0 = B.firstpix + (ti % B.tiles_x) * tx;
     const int ly0 = (ti / B.tiles_x) * ty;
-    const int px1 = min(px0 + tx - 1, B.lastpix_eff);
-    const int nl = min(ty, B.nlines - ly0);
+    const int dmax = tile_dmax(B.shear, tx), span = tile_span(B.shear, tx);
+    // lane j < ty + span: the tile's columns [px0, px1] on line ly0 - span + j
+    // (one interval: the line offset is monotone in the column), clipped to
+    // the burst's
+    const int line = ly0 - span + lane;
+    int xa = tx, xb = -1;
+    for (int x = 0; x < tx; ++x) {
+        const int y = line - ly0 - tile_dline(B.shear, x) + dmax;
+        if (y >= 0 && y < ty) {
+            xa = min(xa, x);
+            xb = x;
+        }
+    }
+    const int px0 = col0 + xa, px1 = min(col0 + xb, B.lastpix_eff);
     bool keep = false;
-    if (lane < nl) {
-        const double *c = B.coef + 3 * (ly0 + lane);
+    if (lane < ty + span && line >= 0 && line < B.nlines && px0 <= px1) {
+        const double *c = B.coef + 3 * line;
         const float den = (float)(B.lastpix - B.firstpix);
         const double a0 = dsub(dmul((double)__fdiv_rn((float)(px0 - B.firstpix), den), 2.0), 1.0);
         const double a1 = dsub(dmul((double)__fdiv_rn((float)(px1 - B.firstpix), den), 2.0), 1.0);
@@ -378,9 +394,10 @@ __global__ void __launch_bounds__(256) tile_mask_kernel(const BurstDev *__restri
     }
     keep = __any_sync(0xffffffffu, keep);
     if (B.rb_order && ti == 0 && lane == 0) *B.rb_order = lines_against_pulses(B) ? 1 : 0;
-    if (!keep && lane < tx && px0 + lane <= px1) {
-        for (int y = 0; y < nl; ++y)
-            B.out[(long long)(ly0 + y) * B.out_ld + (px0 + lane - B.out_pix0)] = make_float2(0.f, 0.f);
+    if (!keep && lane < tx && col0 + lane <= B.lastpix_eff) {
+        const int l0 = ly0 + tile_dline(B.shear, lane) - dmax;
+        for (int y = max(0, -l0); y < ty && l0 + y < B.nlines; ++y)
+            B.out[(long long)(l0 + y) * B.out_ld + (col0 + lane - B.out_pix0)] = make_float2(0.f, 0.f);
     }
     if (lane == 0) {
         const int t = B.tile_base + ti;
@@ -388,8 +405,8 @@ __global__ void __launch_bounds__(256) tile_mask_kernel(const BurstDev *__restri
         if (keep) {
             atomicAdd(seg_count + (t >> kTileSegShift), 1);
             if (band) {
-                atomicMin(band, ly0);
-                atomicMax(band + 1, ly0 + nl - 1);
+                atomicMin(band, max(ly0 - span, 0));
+                atomicMax(band + 1, min(ly0 + ty - 1, B.nlines - 1));
             }
             if (B.rb_expect) atomicAdd(B.rb_expect + (ti / B.tiles_x) / B.rb_tile_rows, 1);
         }
@@ -495,12 +512,12 @@ cudaError_t launch_fma_peak(int fp64, int blocks, int iters, void *sink, cudaStr
 #define SRG_ENTRY(F, TXv, TYv, NTv, CKv, WBv)                                                   \
     {F, {TXv, TYv, NTv, CKv, WBv}, params_bytes<F, CKv>() + 1024 + CKv * WBv * 8,               \
      (const void *)bp_tiles<F, TXv, TYv, NTv, CKv>,                                             \
-     "bp_tiles<" #F "," #TXv "x" #TYv ",threads " #NTv ",chunk " #CKv ",window " #WBv ">"},
+     "bp_tiles<" #F "," #TXv "x" #TYv ",threads " #NTv ",chunk " #CKv ",window " #WBv ">", 0},
 #define SRG_WS_ENTRY(F, TXv, TYv, NCv, CKv, NSv, WBv, MBv)                                      \
     {F, {TXv, TYv, (NCv + 1) * 32, CKv, WBv}, ws_smem_bytes<F, CKv, NSv>(WBv),                  \
      (const void *)bp_ws<F, TXv, TYv, NCv, CKv, NSv, WBv, MBv>,                                 \
      "bp_ws<" #F "," #TXv "x" #TYv ",consumer warps " #NCv ",chunk " #CKv ",stages " #NSv       \
-     ",window " #WBv ",min blocks " #MBv ">"},
+     ",window " #WBv ",min blocks " #MBv ">", 1},
 
 // The first shape of a form is its default: the fastest measured on the
 // B200 (warp-specialised for the split form, first generation for FP64).
@@ -514,7 +531,7 @@ const int kNumKernels = sizeof(kKernels) / sizeof(kKernels[0]);
     {F, {TXv, TYv, (NCv + 1) * 32, CKv, WBv}, ws_smem_bytes<F, CKv, NSv>(WBv),                  \
      (const void *)bp_ws<F, TXv, TYv, NCv, CKv, NSv, WBv, MBv, true>,                           \
      "bp_ws<" #F "," #TXv "x" #TYv ",consumer warps " #NCv ",chunk " #CKv ",stages " #NSv       \
-     ",window " #WBv ",min blocks " #MBv ",gated>"},
+     ",window " #WBv ",min blocks " #MBv ",gated>", 1},
 const KernelEntry kGatedKernels[] = {SRG_WS_GATED_ENTRY(FORM_SPLIT, 32, 8, 4, 31, 2, 128, 3)};
 const int kNumGatedKernels = sizeof(kGatedKernels) / sizeof(kGatedKernels[0]);
 

@@ -27,6 +27,7 @@ struct KernelEntry {
     int smem;          // dynamic shared memory bytes
     const void *fn;
     const char *name;  // template and shape, for reports
+    int shears;        // 1: the kernel takes sheared tiles (BurstDev::shear)
 };
 
 extern const KernelEntry kKernels[];

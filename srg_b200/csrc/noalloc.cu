@@ -128,9 +128,7 @@ extern "C" int srg_bp_burst_device_noalloc(const srg_burst_desc *b, const srg_bp
     }
     BurstDev B = make_burst_dev(*b, coef);
     if (o.spin_limit > 0) B.spin = (unsigned)o.spin_limit;
-    const int nx = B.lastpix_eff - B.firstpix + 1;
-    B.tiles_x = nx > 0 ? (nx + ke->shape.tx - 1) / ke->shape.tx : 0;
-    B.tiles_y = (B.nlines + ke->shape.ty - 1) / ke->shape.ty;
+    if ((rc = set_tiles(B, *ke, o.tile_shear))) return rc;
     B.tile_base = 0;
     const int total = B.tiles_x * B.tiles_y;
     CUtensorMap tm;

@@ -97,9 +97,7 @@ int set_kernel(srg_scene *s, int idx) {
     int total = 0, max_burst_tiles = 0;
     for (int i = 0; i < s->n; ++i) {
         BurstDev &B = s->hb[i];
-        const int nx = B.lastpix_eff - B.firstpix + 1;
-        B.tiles_x = nx > 0 ? (nx + ke.shape.tx - 1) / ke.shape.tx : 0;
-        B.tiles_y = (B.nlines + ke.shape.ty - 1) / ke.shape.ty;
+        if (const int e = set_tiles(B, ke, s->opts.tile_shear)) return e;
         B.tile_base = total;
         total += B.tiles_x * B.tiles_y;
         max_burst_tiles = std::max(max_burst_tiles, B.tiles_x * B.tiles_y);

@@ -14,6 +14,15 @@ pytestmark = pytest.mark.gpu
 NAMES = [c[0] for c in MINI_CASES]
 SPLIT_CFGS = [c[0] for c in _lib.tile_configs() if c[1] == _lib.FORM_SPLIT]
 FP64_CFGS = [c[0] for c in _lib.tile_configs() if c[1] == _lib.FORM_FP64]
+# the warp-specialised FP64 shapes (they take sheared tiles)
+WS_FP64_CFGS = [c for c in FP64_CFGS if _lib.tile_config_name(c).startswith("bp_ws")]
+SHAPES = {c[0]: c for c in _lib.tile_configs()}
+
+
+def shear_fits(cfg, shear):
+    """A shear offsets a tile's columns by fewer lines than it is tall."""
+    tx, ty = SHAPES[cfg][2], SHAPES[cfg][3]
+    return abs((shear * (tx - 1)) // 32) < ty
 
 # Tolerances.  FP64 form vs the oracle's GPU form: identical bins, weights and
 # phases up to the last ulp of sin/cos and of the FP64 accumulation order, so
@@ -228,19 +237,22 @@ def test_config0_point_targets(torch_cuda, orc):
         assert abs(np.angle(spl[li, pix])) < 0.1
 
 
+@pytest.mark.parametrize("shear", [None, -3, 4])
 @pytest.mark.parametrize("form", [_lib.FORM_FP64, _lib.FORM_SPLIT])
-def test_tiles_without_formed_pixels(torch_cuda, orc, form):
+def test_tiles_without_formed_pixels(torch_cuda, orc, form, shear):
     """A grid reaching far past the lines the pulses see: most tiles hold no
     formed pixel and stay out of the kernel's work list.  Their pixels still
     come out zero (the output starts filled with 7+7j) and the formed pixels
-    match the oracle."""
+    match the oracle; with sheared tiles too (forced on the warp-specialised
+    shapes, whose dropped tiles are zeroed line by line along the shear)."""
     b = scene.mini_fixture(seed=31, length=400, width=96)
     ref = oracle_gpu_form(orc, b)["out"]
     rows = np.abs(ref).sum(axis=1) > 0
     assert 0 < rows.sum() < 0.5 * len(rows)          # mostly unformed lines
     db = api.to_device(b)
     db.out.fill_(complex(7.0, 7.0))
-    api.backproject([db], form=form)
+    cfg = WS_FP64_CFGS[0] if (shear is not None and form == _lib.FORM_FP64) else -1
+    api.backproject([db], form=form, tile_cfg=cfg, tile_shear=shear)
     out = db.out.cpu().numpy()
     assert not np.any(out == np.complex64(7 + 7j))
     assert np.array_equal(out != 0, ref != 0)
@@ -249,6 +261,45 @@ def test_tiles_without_formed_pixels(torch_cuda, orc, form):
     else:
         e = phase_amp_errors(out, ref)
         assert e["ph_rms"] < SPLIT_PH_RMS_MRAD and e["amp_rms"] < SPLIT_AMP_RMS, e
+
+
+@pytest.mark.parametrize("shear", [-7, -3, 4])
+@pytest.mark.parametrize("name", NAMES)
+def test_sheared_tiles_match_oracle(torch_cuda, orc, name, shear):
+    """Tiles sheared by `shear` columns per grid line (forced: the mini grids
+    are too narrow for the geometric choice to take a shear).  The FP64 form
+    on the warp-specialised shapes gives every pixel the same terms in the
+    same pulse order as rectangular tiles, so the outputs agree with those and
+    with the oracle to FP32 rounding; the split form stays within its budget.
+    Every pixel of the burst's columns is written (the output starts filled
+    with 7+7j), and no other."""
+    b = mini_case(name)
+    ref = oracle_gpu_form(orc, b)["out"]
+    db = api.to_device(b)
+    cols = slice(db.firstpix - db.out_pix0, min(db.lastpix, b.demwidth - 1) - db.out_pix0 + 1)
+    for cfg in [c for c in WS_FP64_CFGS if shear_fits(c, shear)]:
+        outs = []
+        for s in (0, shear):
+            db.out.fill_(complex(7.0, 7.0))
+            api.backproject([db], form=_lib.FORM_FP64, tile_cfg=cfg, tile_shear=s)
+            outs.append(db.out.cpu().numpy())
+        rect, sheared = outs
+        unset = sheared == np.complex64(7 + 7j)
+        assert np.array_equal(unset, rect == np.complex64(7 + 7j))
+        assert not np.any(unset[:, cols])
+        rect, sheared = np.where(unset, 0, rect), np.where(unset, 0, sheared)
+        assert np.array_equal(sheared != 0, ref != 0)
+        assert rel_err(sheared, ref) < FP64_REL
+        assert rel_err(sheared, rect) < FP64_REL
+    db.out.fill_(complex(7.0, 7.0))
+    api.backproject([db], form=_lib.FORM_SPLIT, tile_shear=shear)
+    out = db.out.cpu().numpy()
+    assert np.array_equal(out == np.complex64(7 + 7j), unset)
+    out = np.where(unset, 0, out)
+    assert np.array_equal(out != 0, ref != 0)
+    e = phase_amp_errors(out, ref)
+    assert e["ph_rms"] < SPLIT_PH_RMS_MRAD and e["ph_max"] < SPLIT_PH_MAX_MRAD, e
+    assert e["amp_rms"] < SPLIT_AMP_RMS, e
 
 
 def test_dropin_sequential_bursts_merge_like_the_oracle(torch_cuda, orc):

@@ -31,19 +31,29 @@ def mini():
     return grid, bursts, geo, terms
 
 
-def build(torch, grid, bursts, form):
+def build(torch, grid, bursts, form, tile_cfg=-1, tile_shear=None):
     dem = torch.from_numpy(grid.dem).cuda()
     dbs = [api.to_device(b, dem_tensor=dem, narrow_out=True) for b in bursts]
     raster = torch.zeros((grid.length, grid.width), dtype=torch.complex64, device="cuda")
-    return dbs, raster, api.Scene(dbs, raster=raster, form=form)
+    return dbs, raster, api.Scene(dbs, raster=raster, form=form, tile_cfg=tile_cfg,
+                                  tile_shear=tile_shear)
 
 
+WS_FP64 = [c[0] for c in _lib.tile_configs()
+           if c[1] == _lib.FORM_FP64 and _lib.tile_config_name(c[0]).startswith("bp_ws")]
+
+
+@pytest.mark.parametrize("shear", [None, -3])
 @pytest.mark.parametrize("form", [_lib.FORM_FP64, _lib.FORM_SPLIT])
-def test_scene_plan_matches_sequential_merge(torch_cuda, mini, form):
+def test_scene_plan_matches_sequential_merge(torch_cuda, mini, form, shear):
+    """The plan's passes (graph replays and direct launches) against the
+    oracle's bursts merged one after the other; with sheared tiles the merge
+    reads the work-list mask along the shear."""
     torch = torch_cuda
     grid, bursts, geo, terms = mini
     assert geo.any()
-    dbs, raster, sc = build(torch, grid, bursts, form)
+    cfg = WS_FP64[0] if (shear is not None and form == _lib.FORM_FP64) else -1
+    dbs, raster, sc = build(torch, grid, bursts, form, cfg, shear)
     assert sc.terms() == terms
     st = torch.cuda.Stream()
     for rep in range(3):          # first pass captures the graph, then replays

@@ -1,5 +1,6 @@
 """The C ABI library without a GPU: it loads, exports every entry point that
 include/srg_bp.h declares, and reports its kernel shapes.  No compute call."""
+import ctypes as C
 import os
 import re
 
@@ -142,3 +143,57 @@ def test_overlap_environment_switch_sets_the_default():
                            timeout=120)
         assert p.returncode == 0, p.stderr[-1000:]
         assert p.stdout.strip() == want, (val, p.stdout)
+
+
+def _host_desc(b):
+    """A descriptor with the burst's scalars only (no device memory): enough
+    for srg_tile_shear, which reads nothing else."""
+    fl, ll, fp, lp = api.limits(b)
+    d = _lib.BurstDesc()
+    d.P, d.S, d.demwidth = b.rawdatalines, b.samples, b.demwidth
+    d.firstline, d.nlines, d.firstpix, d.lastpix = fl, ll - fl + 1, fp, lp
+    d.aperture = b.aperture
+    d.firstlat, d.deltalat, d.firstlon, d.deltalon = b.firstlat, b.deltalat, b.firstlon, b.deltalon
+    d.rngstart, d.rngend, d.dmrg, d.wvl = b.rngstart, b.rngend, b.dmrg, b.wvl
+    for i in range(3):
+        d.xyz_mid[i] = float(b.xyz_mid[i])
+        d.vel_mid[i] = float(b.vel_mid[i])
+    d.prf = b.prf
+    return d
+
+
+def _shear(d, cfg=-1, forced=_lib.TILE_SHEAR_AUTO):
+    s, tx, ty = C.c_int(), C.c_int(), C.c_int()
+    rc = _lib.lib().srg_tile_shear(C.byref(d), cfg, forced, C.byref(s), C.byref(tx), C.byref(ty))
+    return rc, s.value, tx.value, ty.value
+
+
+def test_tile_shear_follows_the_azimuth_centres():
+    """On the IW scene the azimuth centre moves ~2.43 pulses per grid line
+    and ~0.56 per column, the range ~0.6-1.0 bins per line and ~2.5-3.0 per
+    column.  The default 32 x 8 tiles shear by -7 lines per 32 columns: each
+    tile's rows of pixels then follow the lines of constant centre (measured
+    with the oracle's windows: 3.6 % fewer pixel-pulse slots, 7.6 % fewer
+    chunks) and widen its range window by ~4 bins; a column then needs
+    ceil((nlines + 7) / 8) tiles.  First-generation shapes keep rectangular
+    tiles; a forced shear is taken as given and one out of range, or one that
+    offsets a tile's columns by its height or more, is refused."""
+    _, bursts = scene.iw_scene(seed=1003)
+    first_gen = [c[0] for c in _lib.tile_configs() if "bp_tiles" in _lib.tile_config_name(c[0])]
+    assert first_gen
+    for b in bursts[:3]:
+        d = _host_desc(b)
+        nx = min(d.lastpix, d.demwidth - 1) - d.firstpix + 1
+        rc, s, tx, ty = _shear(d)
+        assert rc == _lib.SRG_OK and s == -7, (rc, s)
+        assert tx == -(-nx // 32) and ty == -(-(d.nlines + 7) // 8)
+        assert all(_shear(d, cfg)[1] == 0 for cfg in first_gen)
+        assert _shear(d, -1, 3)[:2] == (_lib.SRG_OK, 3)
+        assert _shear(d, -1, 0)[1:] == (0, -(-nx // 32), -(-d.nlines // 8))
+        assert _shear(d, -1, 9)[0] == _lib.SRG_E_ARG
+        assert _shear(d, -1, 8)[0] == _lib.SRG_OK     # offset floor(8 * 31 / 32) = 7 < 8
+    # without a velocity (a caller passing its own centres) the tiles stay rectangular
+    d = _host_desc(bursts[0])
+    for i in range(3):
+        d.vel_mid[i] = 0.0
+    assert _shear(d)[1] == 0
