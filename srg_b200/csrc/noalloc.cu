@@ -39,7 +39,7 @@ static_assert(kScratchBytes == SRG_NOALLOC_SCRATCH_BYTES, "header and layout dis
 static_assert(sizeof(BurstDev) <= kOffTmap - kOffBurst, "BurstDev outgrew its slot");
 static_assert(kOffTmap % 64 == 0 && kOffCoef % 8 == 0, "alignment");
 
-__device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 std::mutex g_addr_mu;
 void *g_addr[64] = {};
