@@ -456,19 +456,22 @@ def reference_cpu(workload: str, steps: int, warmup: int):
 # profiling driver
 
 
-def profile_shapes(torch, workload: str, shapes, samples: str = "random", seed=None):
+def profile_shapes(torch, workload: str, shapes, samples: str = "random", seed=None,
+                   tile_shear=None):
     """A fixed workload and a list of kernel shapes: one warm-up launch, then
     one measured launch per shape, nothing else on the GPU (the command line
     of the committed ncu summaries).  c1: one IW1-sized burst (random or
     forward-projected samples); c3: the 27-burst IW scene, azimuth centres
     and backprojection stages of its scene plan.  Under ncu, select the
     backprojection kernels by name (regex:bp_) and skip the warm-up launches
-    with -s <number of shapes>."""
+    with -s <number of shapes>.  tile_shear: srg_bp_options.tile_shear (None:
+    the default, rectangular tiles)."""
     from srg_b200 import _lib, api, scene, workloads
     cfgs = _lib.tile_configs()
     if workload == "c3":
         wl = workloads.config3(seed=1003 if seed is None else seed)
-        plan = wl.plan
+        plan = wl.plan if tile_shear is None else api.Scene(wl.bursts, raster=None,
+                                                             tile_shear=tile_shear)
         for rep in range(2):  # warm-up, then measured
             for s in shapes:
                 plan.set_form(cfgs[s][1], s)
@@ -489,7 +492,8 @@ def profile_shapes(torch, workload: str, shapes, samples: str = "random", seed=N
         coef = api.line_centres(db)
     for rep in range(2):  # warm-up, then measured
         for s in shapes:
-            api.backproject([db], form=cfgs[s][1], tile_cfg=s, coefs=[coef])
+            api.backproject([db], form=cfgs[s][1], tile_cfg=s, coefs=[coef],
+                            tile_shear=tile_shear)
     torch.cuda.synchronize()
 
 
@@ -581,6 +585,9 @@ def main():
     ap.add_argument("--profile-shapes", default=None,
                     help="comma-separated kernel shape indices: run the profiling driver on "
                          "--workload c1 or c3 instead of the benchmark")
+    ap.add_argument("--tile-shear", default=None,
+                    help="with --profile-shapes: tile shear, lines per 32 columns, or 'auto' "
+                         "(the geometric choice); default rectangular tiles")
     ap.add_argument("--samples", default="random", choices=["random", "forward"],
                     help="profiling driver, c1: random or forward-projected range lines")
     ap.add_argument("--e2e-only", default=None, choices=["overlapped", "waiting"],
@@ -591,8 +598,11 @@ def main():
     args = ap.parse_args()
     if args.profile_shapes is not None:
         import torch
+        from srg_b200 import _lib
+        shear = (None if args.tile_shear is None else _lib.TILE_SHEAR_AUTO
+                 if args.tile_shear == "auto" else int(args.tile_shear))
         profile_shapes(torch, args.workload, [int(x) for x in args.profile_shapes.split(",")],
-                       args.samples)
+                       args.samples, tile_shear=shear)
         print("ok", args.profile_shapes)
         return
     if args.workload == "rc":
@@ -690,6 +700,7 @@ def main():
         tuned["split"] = (plan.shape(), None)
     else:
         tuned["split"] = plan.tune(iters=2)
+    split_shears = sorted(set(plan.tile_shears()))
     with ClockSampler(local) as clk:
         if world > 1:
             dist.barrier()
@@ -771,6 +782,7 @@ def main():
         "workload_detail": wl.description,
         "terms_per_step": terms_all,
         "kernel_shapes": {k: _lib.tile_config_name(v[0]) for k, v in tuned.items()},
+        "tile_shear_split": split_shears,
         "fp64_form": {"value": fp64_value, "ms_per_step": d_ms, "kernel_ms": d_kern,
                       "split_over_fp64": value / fp64_value},
         "phase_error_vs_fp64": perr,

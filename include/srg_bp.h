@@ -72,11 +72,15 @@ typedef struct srg_bp_options {
                           sheared (a tile's column x sits floor(tile_shear x /
                           32) lines lower), in [-SRG_MAX_TILE_SHEAR,
                           SRG_MAX_TILE_SHEAR] and offsetting a tile's columns
-                          by fewer lines than it is tall (0: rectangular
-                          tiles); SRG_TILE_SHEAR_AUTO (the default): chosen
-                          per burst from its geometry so that a tile's rows of
+                          by fewer lines than it is tall; 0 (the default):
+                          rectangular tiles; SRG_TILE_SHEAR_AUTO: chosen per
+                          burst from its geometry so that a tile's rows of
                           pixels follow the lines of constant azimuth centre.
-                          The warp-specialised shapes take it; the
+                          That pays on gentle terrain (fewer pulses per tile)
+                          and costs over strong relief (a tile's range window
+                          outgrows the staged one), so the scene plan's tuner
+                          times both (srg_scene_autotune).  The
+                          warp-specialised shapes take it; the
                           first-generation shapes keep rectangular tiles.
                           Results depend on it only through the split form's
                           per-tile closed forms (within its error budget). */
@@ -87,8 +91,8 @@ typedef struct srg_bp_options {
 
 /* Fill *o with the defaults (split form, tuned tile, current device,
  * centres on the GPU, quiet, default wait limit, range band, no scratch
- * limit, calls not overlapped unless SRG_DROPIN_OVERLAP=1, tile shear from
- * the geometry). */
+ * limit, calls not overlapped unless SRG_DROPIN_OVERLAP=1, rectangular
+ * tiles). */
 void srg_bp_default_options(srg_bp_options *o);
 
 /* Message of the last failing call on this thread ("" if none). */
@@ -281,7 +285,9 @@ int srg_scene_sync(srg_scene *s, void *stream);
 int srg_scene_terms(srg_scene *s, int64_t *terms);
 /* Autotuner: time every compiled kernel shape of the plan's form on this
  * scene (`iters` timed launches each) and keep the fastest, or take the
- * cached best shape of a scene of the same shape (srg_scene_autotune). */
+ * cached best shape of a scene of the same shape (srg_scene_autotune); with
+ * rectangular and with geometrically sheared tiles (srg_bp_options.
+ * tile_shear), whichever is faster on this scene (timed on every call). */
 int srg_scene_tune(srg_scene *s, int iters, int *best_cfg, double *best_ms);
 /* Autotuner with the range interpolation in its search.  With
  * interp_budget > 0 it first estimates, from a sample of every burst's lines,
@@ -308,9 +314,15 @@ typedef struct srg_tune_request {
 typedef struct srg_tune_result {
     int tile_cfg;          /* shape in use */
     int interp;            /* SRG_INTERP_* in use */
-    int from_cache;        /* 1: the shape came from the cache (nothing timed) */
-    int pad;
-    double ms;             /* mean backprojection time of the shape (-1: cached) */
+    int from_cache;        /* 1: the shape came from the cache (no shape timed) */
+    int tile_shear;        /* tile shear in use: 0 (rectangular tiles) or
+                              SRG_TILE_SHEAR_AUTO (the geometric shear), timed
+                              against each other on every call: which pays
+                              depends on the terrain, which the cache does not
+                              key on */
+    double ms;             /* mean backprojection time of the choice (-1:
+                              nothing timed: a cached shape and no burst that
+                              the geometric shear would shear) */
     double err_linear, err_oversampled; /* estimated RMS phase error (rad) of
                               each interpolation (-1: not estimated) */
 } srg_tune_result;
@@ -338,6 +350,8 @@ int srg_scene_set_shape(srg_scene *s, int tile_cfg);
 int srg_scene_set_form(srg_scene *s, int form, int tile_cfg);
 /* Kernel shape index in use. */
 int srg_scene_shape(const srg_scene *s);
+/* Tile shear (lines per 32 columns) in use for burst `burst` of the plan. */
+int srg_scene_tile_shear(const srg_scene *s, int burst, int *shear);
 void srg_scene_destroy(srg_scene *s);
 
 /* Exact count of executed terms (pixel, pulse pairs inside the aperture

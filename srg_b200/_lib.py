@@ -74,7 +74,7 @@ class TuneRequest(C.Structure):
 
 class TuneResult(C.Structure):
     _fields_ = [("tile_cfg", C.c_int), ("interp", C.c_int), ("from_cache", C.c_int),
-                ("pad", C.c_int), ("ms", C.c_double), ("err_linear", C.c_double),
+                ("tile_shear", C.c_int), ("ms", C.c_double), ("err_linear", C.c_double),
                 ("err_oversampled", C.c_double)]
 
 
@@ -123,6 +123,7 @@ _SIGS = {
     "srg_scene_set_shape": (C.c_int, [C.c_void_p, C.c_int]),
     "srg_scene_set_form": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "srg_scene_shape": (C.c_int, [C.c_void_p]),
+    "srg_scene_tile_shear": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
     "srg_scene_destroy": (None, [C.c_void_p]),
     "srg_tile_config_count": (C.c_int, []),
     "srg_tile_shear": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int),

@@ -483,7 +483,7 @@ class Scene:
         q = _lib.TuneRequest(iters, int(bool(use_cache)), float(interp_budget))
         r = _lib.TuneResult()
         check(lib().srg_scene_autotune(self.handle, C.byref(q), C.byref(r)))
-        return {k: getattr(r, k) for k, _ in r._fields_ if k != "pad"}
+        return {k: getattr(r, k) for k, _ in r._fields_}
 
     def set_interp(self, interp: int) -> None:
         check(lib().srg_scene_set_interp(self.handle, interp))
@@ -493,6 +493,15 @@ class Scene:
 
     def set_form(self, form: int, tile_cfg: int = -1) -> None:
         check(lib().srg_scene_set_form(self.handle, form, tile_cfg))
+
+    def tile_shears(self) -> list:
+        """Tile shear (lines per 32 columns) in use for each burst."""
+        out = []
+        for i in range(len(self.bursts)):
+            v = C.c_int()
+            check(lib().srg_scene_tile_shear(self.handle, i, C.byref(v)))
+            out.append(int(v.value))
+        return out
 
     def shape(self) -> int:
         return int(lib().srg_scene_shape(self.handle))

@@ -74,8 +74,7 @@ int env_overlap() {
     }();
     return v;
 }
-srg_bp_options g_default_opts = {SRG_FORM_SPLIT, -1, -1, 0, 0, 0, 0, 0, env_overlap(),
-                                 SRG_TILE_SHEAR_AUTO};
+srg_bp_options g_default_opts = {SRG_FORM_SPLIT, -1, -1, 0, 0, 0, 0, 0, env_overlap(), 0};
 std::mutex g_opts_mu;
 
 DevCtx g_ctx[64];
@@ -851,7 +850,7 @@ void srg_bp_default_options(srg_bp_options *o) {
     o->full_lines = 0;
     o->scratch_limit = 0;
     o->overlap = env_overlap();
-    o->tile_shear = SRG_TILE_SHEAR_AUTO;
+    o->tile_shear = 0;
 }
 
 const char *srg_last_error(void) { return g_err.c_str(); }

@@ -349,6 +349,10 @@ __device__ __forceinline__ double azoff_fit(const double *c, double arg) {
     return dadd(dadd(dmul(dmul(c[0], arg), arg), dmul(c[1], arg)), c[2]);
 }
 
+// floor(a / b) and ceil(a / b) for b > 0 (integer division truncates)
+__device__ __forceinline__ int floor_div(int a, int b) { return a >= 0 ? a / b : -((b - 1 - a) / b); }
+__device__ __forceinline__ int ceil_div(int a, int b) { return -floor_div(-a, b); }
+
 __global__ void __launch_bounds__(256) tile_mask_kernel(const BurstDev *__restrict__ bursts, int tx,
                                                         int ty, unsigned char *__restrict__ mask,
                                                         int *__restrict__ seg_count,
@@ -360,18 +364,25 @@ __global__ void __launch_bounds__(256) tile_mask_kernel(const BurstDev *__restri
     const int col0 = B.firstpix + (ti % B.tiles_x) * tx;
     const int ly0 = (ti / B.tiles_x) * ty;
     const int dmax = tile_dmax(B.shear, tx), span = tile_span(B.shear, tx);
-    // lane j < ty + span: the tile's columns [px0, px1] on line ly0 - span + j
-    // (one interval: the line offset is monotone in the column), clipped to
-    // the burst's
+    // lane j < ty + span: the tile's columns [px0, px1] on line ly0 - span + j,
+    // clipped to the burst's: the x in [0, tx) whose line offset
+    // d(x) = floor(shear x / 32) puts the line among the tile's rows,
+    // lo <= d(x) <= hi (one interval: d is monotone in x)
     const int line = ly0 - span + lane;
-    int xa = tx, xb = -1;
-    for (int x = 0; x < tx; ++x) {
-        const int y = line - ly0 - tile_dline(B.shear, x) + dmax;
-        if (y >= 0 && y < ty) {
-            xa = min(xa, x);
-            xb = x;
-        }
+    const int lo = line - ly0 + dmax - ty + 1, hi = line - ly0 + dmax, sh = B.shear;
+    int xa, xb;
+    if (sh == 0) {
+        xa = lo <= 0 && hi >= 0 ? 0 : tx;
+        xb = tx - 1;
+    } else if (sh > 0) {  // 32 lo <= sh x < 32 (hi + 1)
+        xa = ceil_div(32 * lo, sh);
+        xb = ceil_div(32 * (hi + 1), sh) - 1;
+    } else {              // 32 lo <= sh x < 32 (hi + 1), sh < 0
+        xa = floor_div(-32 * (hi + 1), -sh) + 1;
+        xb = floor_div(-32 * lo, -sh);
     }
+    xa = max(xa, 0);
+    xb = min(xb, tx - 1);
     const int px0 = col0 + xa, px1 = min(col0 + xb, B.lastpix_eff);
     bool keep = false;
     if (lane < ty + span && line >= 0 && line < B.nlines && px0 <= px1) {

@@ -506,47 +506,66 @@ int srg_scene_autotune(srg_scene *s, const srg_tune_request *req, srg_tune_resul
         }
     }
     r.interp = s->interp;
+    // The shape: every compiled shape of the form is timed, unless the cache
+    // holds the best shape of a scene of the same sizes.  The tile shear
+    // (rectangular tiles or the geometric shear) is timed on every call: it
+    // pays or costs by the terrain (a tile's range window grows with the
+    // relief it covers), which the cache key does not see.
     const std::string key = rc == SRG_OK ? tune_key(s) : std::string();
     const int cached = rc == SRG_OK && q.use_cache ? tune_lookup(key) : -1;
-    if (cached >= 0 && cached < kNumKernels && kKernels[cached].form == s->opts.form) {
-        rc = set_kernel(s, cached);
-        if (rc == SRG_OK) {
-            s->opts.tile_cfg = cached;
-            r.tile_cfg = cached;
-            r.from_cache = 1;
-        }
-        cudaStreamDestroy(st);
-        if (res) *res = r;
-        return rc;
-    }
+    const bool from_cache =
+        cached >= 0 && cached < kNumKernels && kKernels[cached].form == s->opts.form;
+    const int shear0 = s->opts.tile_shear;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    if (rc == SRG_OK) rc = enqueue_centres(s, st);
-    if (rc == SRG_OK) rc = enqueue_oversample(s, st);
-    if (rc == SRG_OK && cudaStreamSynchronize(st) != cudaSuccess)
-        rc = fail(SRG_E_CUDA, "azimuth centres failed: %s", cudaGetErrorString(cudaGetLastError()));
-    int best = -1;
+    bool centres_done = false;
+    int best = -1, best_shear = 0;
     float best_t = 1e30f;
     for (int idx = 0; idx < kNumKernels && rc == SRG_OK; ++idx) {
-        if (kKernels[idx].form != s->opts.form) continue;
-        if ((rc = set_kernel(s, idx))) break;
-        if ((rc = enqueue_backprojection(s, st))) break;  // warm-up
-        float tot = 0.f;
-        for (int it = 0; it < q.iters && rc == SRG_OK; ++it) {
-            cudaEventRecord(e0, st);
-            rc = enqueue_backprojection(s, st);
-            cudaEventRecord(e1, st);
-            cudaEventSynchronize(e1);
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            tot += ms;
+        if (from_cache ? idx != cached : kKernels[idx].form != s->opts.form) continue;
+        // shear candidates: rectangular tiles, and the geometric shear where
+        // it shears a burst
+        bool geo = false;
+        for (int i = 0; i < s->n && kKernels[idx].shears && !geo; ++i) {
+            BurstDev probe = s->hb[i];
+            geo = set_tiles(probe, kKernels[idx], SRG_TILE_SHEAR_AUTO) == SRG_OK && probe.shear != 0;
         }
-        if (rc) break;
-        const float t = tot / q.iters;
-        if (t < best_t) {
-            best_t = t;
+        if (from_cache && !geo) {  // nothing to time
             best = idx;
+            break;
+        }
+        for (const int shear : {0, SRG_TILE_SHEAR_AUTO}) {
+            if (shear != 0 && !geo) continue;
+            s->opts.tile_shear = shear;
+            if ((rc = set_kernel(s, idx))) break;
+            if (!centres_done) {
+                if ((rc = enqueue_centres(s, st)) || (rc = enqueue_oversample(s, st))) break;
+                if (cudaStreamSynchronize(st) != cudaSuccess) {
+                    rc = fail(SRG_E_CUDA, "azimuth centres failed: %s",
+                              cudaGetErrorString(cudaGetLastError()));
+                    break;
+                }
+                centres_done = true;
+            }
+            if ((rc = enqueue_backprojection(s, st))) break;  // warm-up
+            float tot = 0.f;
+            for (int it = 0; it < q.iters && rc == SRG_OK; ++it) {
+                cudaEventRecord(e0, st);
+                rc = enqueue_backprojection(s, st);
+                cudaEventRecord(e1, st);
+                cudaEventSynchronize(e1);
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                tot += ms;
+            }
+            if (rc) break;
+            const float t = tot / q.iters;
+            if (t < best_t) {
+                best_t = t;
+                best = idx;
+                best_shear = shear;
+            }
         }
     }
     if (rc == SRG_OK && cudaStreamSynchronize(st) != cudaSuccess)
@@ -554,14 +573,20 @@ int srg_scene_autotune(srg_scene *s, const srg_tune_request *req, srg_tune_resul
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaStreamDestroy(st);
-    if (rc) return rc;
-    if (best < 0) return fail(SRG_E_UNSUPPORTED, "no kernel shape of form %d", s->opts.form);
+    if (rc || best < 0) {
+        s->opts.tile_shear = shear0;
+        if (rc) return rc;
+        return fail(SRG_E_UNSUPPORTED, "no kernel shape of form %d", s->opts.form);
+    }
+    s->opts.tile_shear = best_shear;
     rc = set_kernel(s, best);
     if (rc) return rc;
     s->opts.tile_cfg = best;
-    tune_record(key, best);
+    if (!from_cache) tune_record(key, best);
     r.tile_cfg = best;
-    r.ms = best_t;
+    r.tile_shear = best_shear;
+    r.from_cache = from_cache ? 1 : 0;
+    r.ms = best_t < 1e30f ? best_t : -1.0;
     if (res) *res = r;
     return SRG_OK;
 }
@@ -603,6 +628,12 @@ int srg_scene_set_form(srg_scene *s, int form, int tile_cfg) {
 }
 
 int srg_scene_shape(const srg_scene *s) { return s ? s->kernel : -1; }
+
+int srg_scene_tile_shear(const srg_scene *s, int burst, int *shear) {
+    if (!s || !shear || burst < 0 || burst >= s->n) return fail(SRG_E_ARG, "bad arguments");
+    *shear = s->hb[burst].shear;
+    return SRG_OK;
+}
 
 void srg_scene_destroy(srg_scene *s) {
     if (!s) return;

@@ -181,3 +181,6 @@ class PartitionedScene:
 
     def shape(self) -> int:
         return self.plan.shape() if self.plan is not None else -1
+
+    def tile_shears(self) -> list:
+        return self.plan.tile_shears() if self.plan is not None else []

@@ -56,10 +56,16 @@ def cases():
     return out
 
 
-def run(db, form, cfg):
+def run(db, form, cfg, tile_shear=None):
     db.out.fill_(complex(7.0, 7.0))
-    api.backproject([db], form=form, tile_cfg=cfg)
+    api.backproject([db], form=form, tile_cfg=cfg, tile_shear=tile_shear)
     return db.out.cpu().numpy()
+
+
+# the warp-specialised 32 x 8 shape of each form (they take sheared tiles)
+WS_32x8 = {form: next(c[0] for c in _lib.tile_configs() if c[1] == form and c[2:4] == (32, 8)
+                      and _lib.tile_config_name(c[0]).startswith("bp_ws"))
+           for form in (_lib.FORM_FP64, _lib.FORM_SPLIT)}
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -84,6 +90,35 @@ def test_split_form_full_size(cases, name, cfg):
     db, ref, _ = cases[name]
     got = run(db, _lib.FORM_SPLIT, cfg)
     assert np.array_equal(got != 0, ref != 0)
+    e = phase_amp_errors(got, ref)
+    assert e["ph_rms"] < SPLIT_PH_RMS_MRAD, e
+    assert e["ph_max"] < SPLIT_PH_MAX_MRAD, e
+    assert e["amp_rms"] < SPLIT_AMP_RMS, e
+    h = phase_amp_errors(got, ref, floor_frac=0.5)
+    assert h["ph_max"] < SPLIT_PH_MAX_HALF_RMS_MRAD, h
+
+
+@pytest.mark.parametrize("form", [_lib.FORM_FP64, _lib.FORM_SPLIT])
+@pytest.mark.parametrize("name", CASES)
+def test_geometric_shear_full_size(cases, name, form):
+    """Sheared tiles at full size: the geometric shear (tile_shear =
+    SRG_TILE_SHEAR_AUTO, -7 lines per 32 columns on these IW geometries) on
+    the warp-specialised 32 x 8 shape of each form, against the oracle with
+    the same bounds as rectangular tiles."""
+    import ctypes as C
+    db, ref, _ = cases[name]
+    cfg = WS_32x8[form]
+    sh, tx, ty = C.c_int(), C.c_int(), C.c_int()
+    d = db.desc()
+    assert _lib.lib().srg_tile_shear(C.byref(d), cfg, _lib.TILE_SHEAR_AUTO, C.byref(sh),
+                                     C.byref(tx), C.byref(ty)) == _lib.SRG_OK
+    if name != "c2":          # (c2's half-spaced bins can make the range guard keep 0)
+        assert sh.value != 0
+    got = run(db, form, cfg, tile_shear=_lib.TILE_SHEAR_AUTO)
+    assert np.array_equal(got != 0, ref != 0)
+    if form == _lib.FORM_FP64:
+        assert rel_err(got, ref) < FP64_REL
+        return
     e = phase_amp_errors(got, ref)
     assert e["ph_rms"] < SPLIT_PH_RMS_MRAD, e
     assert e["ph_max"] < SPLIT_PH_MAX_MRAD, e

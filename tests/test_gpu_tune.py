@@ -2,6 +2,7 @@
 2x-oversampled ones) chosen against a phase-error budget from the lines'
 own spectrum, the kernel shape timed or taken from the results cache, and
 the cache carried to a later process through SRG_TUNE_CACHE."""
+import ctypes as C
 import json
 import os
 import subprocess
@@ -74,11 +75,21 @@ def test_autotune_interpolation_budget_and_cache(torch_cuda):
     dbs, sc = _mini_plan(torch)
     r = sc.autotune(interp_budget=10.0, iters=1, use_cache=False)   # anything goes: linear
     assert r["interp"] == _lib.INTERP_LINEAR and r["from_cache"] == 0 and r["ms"] > 0
+    assert r["tile_shear"] in (0, _lib.TILE_SHEAR_AUTO)
     assert r["err_linear"] > r["err_oversampled"] > 0
     # a second plan of the same shape takes the cached shape without timing
+    # shapes; it times the shear only where the geometric one shears a burst
     dbs2, sc2 = _mini_plan(torch)
     r2 = sc2.autotune(iters=1)
-    assert r2["from_cache"] == 1 and r2["tile_cfg"] == r["tile_cfg"] and r2["ms"] == -1
+    assert r2["from_cache"] == 1 and r2["tile_cfg"] == r["tile_cfg"]
+    geo = False
+    for db in dbs2:
+        sh, tx, ty = C.c_int(), C.c_int(), C.c_int()
+        d = db.desc()
+        assert _lib.lib().srg_tile_shear(C.byref(d), r["tile_cfg"], _lib.TILE_SHEAR_AUTO,
+                                         C.byref(sh), C.byref(tx), C.byref(ty)) == _lib.SRG_OK
+        geo |= sh.value != 0
+    assert (r2["ms"] == -1) == (not geo)
     # a budget below the linear error: oversampled lines, made by the plan in
     # every pass; the images equal a plan's on lines oversampled beforehand
     r3 = sc.autotune(interp_budget=0.5 * r["err_linear"], iters=1, use_cache=False)
@@ -88,7 +99,8 @@ def test_autotune_interpolation_budget_and_cache(torch_cuda):
     sc.sync(st.cuda_stream)
     got = [db.out.clone() for db in dbs]
     over = [api.oversample2(db) for db in dbs2]
-    ref_plan = api.Scene(over, raster=None, form=_lib.FORM_SPLIT, tile_cfg=r3["tile_cfg"])
+    ref_plan = api.Scene(over, raster=None, form=_lib.FORM_SPLIT, tile_cfg=r3["tile_cfg"],
+                         tile_shear=r3["tile_shear"])
     ref_plan.run(st.cuda_stream)
     ref_plan.sync(st.cuda_stream)
     for g, db in zip(got, over):
