@@ -10,10 +10,14 @@
 // go through in blocks: one kernel pads a block, cuFFT transforms it, one
 // kernel multiplies, cuFFT transforms back, one kernel writes the valid
 // samples.  FFTs by cuFFT (the reference uses FFTW in single precision).
+// Pulses of up to 4,096 samples (Sentinel-1 IW: ~3,370) take the fused
+// overlap-save kernel instead (rc_os_kernel below), same samples.
 #include <cuda_runtime.h>
 #include <cufft.h>
 
+#include <climits>
 #include <cmath>
+#include <complex>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -74,12 +78,192 @@ __global__ void rc_out_kernel(const float2 *__restrict__ buf, int l0, int nlines
     }
 }
 
+// ---------------------------------------------------------------------------
+// Fused matched filter by overlap-save.  The samples the reference keeps,
+// y[n] = 32768 sum_{j < npts} conj(r[j]) x[n + j] for n < nvalid, are a
+// linear correlation (the 32,768-point circular one never wraps into them),
+// so 8,192-point transforms give them exactly up to rounding: a segment of
+// 8,192 samples from s0 (zeros past the line) yields y[s0 .. s0 + L),
+// L = 8192 - npts + 1.  One CTA per (line, segment) loads its samples once,
+// transforms them in shared memory, multiplies by the filter
+// H = (32768 / 8192) conj(DFT_8192(r)), transforms back (a forward transform
+// of the conjugate, conjugated) and writes its L outputs once: the lines
+// cross HBM once each way, where the cuFFT path below takes five passes over
+// 32,768-point rows.  Transforms: Stockham autosort passes of radix 16, 16,
+// 16 and 2 (16 values per thread per pass), each DFT in registers, the
+// padded shared layout i + i / 16 keeping the 16-strided accesses off common
+// banks, twiddles exp(-2 pi i m / 8192) from two small tables
+// (whi[m / 64] wlo[m % 64]).  Pulses of more than 4,096 samples take the
+// cuFFT path.
+constexpr int kOsM = 8192;                       // segment transform
+constexpr int kOsMaxPts = kOsM / 2;              // longest pulse the segments take
+constexpr int kOsBuf = kOsM + (kOsM >> 4);       // padded segment (float2)
+constexpr int kOsTw = 128 + 64;                  // whi, wlo
+constexpr int kOsSmem = (kOsBuf + kOsTw) * (int)sizeof(float2);
+
+// exp(-2 pi i q / 16), q = 0..7
+__constant__ float2 kW16[8] = {{1.000000000f, 0.000000000f},   {0.923879533f, -0.382683432f},
+                               {0.707106781f, -0.707106781f},  {0.382683432f, -0.923879533f},
+                               {0.000000000f, -1.000000000f},  {-0.382683432f, -0.923879533f},
+                               {-0.707106781f, -0.707106781f}, {-0.923879533f, -0.382683432f}};
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+__device__ __forceinline__ int os_pad(int i) { return i + (i >> 4); }
+template <int R>
+__device__ __forceinline__ constexpr int brev(int i) {
+    int o = 0;
+    for (int b = 1, t = R >> 1; b < R; b <<= 1, t >>= 1)
+        if (i & b) o |= t;
+    return o;
+}
+// exp(-2 pi i m / 8192), 0 <= m < 8192
+__device__ __forceinline__ float2 os_tw(int m, const float2 *whi, const float2 *wlo) {
+    return cmul(whi[m >> 6], wlo[m & 63]);
+}
+
+// R-point DFT in registers (R = 8 or 16), in place: input X in natural
+// order, output DFT(X)[r] in v[brev<R>(r)] (radix-2 decimation in time on
+// the bit-reversed view a[p] = v[brev<R>(p)], so no permutation moves data;
+// the butterflies of half-size h take exp(-2 pi i q / (2h)) = kW16[8 q / h]).
+template <int R>
+__device__ __forceinline__ void dft(float2 (&v)[R]) {
+#pragma unroll
+    for (int h = 1; h < R; h <<= 1) {
+#pragma unroll
+        for (int i = 0; i < R; i += 2 * h) {
+#pragma unroll
+            for (int q = 0; q < h; ++q) {
+                float2 &lo = v[brev<R>(i + q)], &hi = v[brev<R>(i + q + h)];
+                const float2 b = q == 0 ? hi : cmul(hi, kW16[q * (8 / h)]);
+                hi = csub(lo, b);
+                lo = cadd(lo, b);
+            }
+        }
+    }
+}
+
+// One radix-R Stockham pass over the segment in shared memory, one work item
+// per thread (8192 / R threads): item j reads v[r] = x[j + r 8192 / R],
+// scales v[r] by exp(-2 pi i r k / (R Ns)), k = j mod Ns, takes the R-point
+// DFT and writes y[(j - k) R + k + r Ns].
+template <int R>
+__device__ __forceinline__ void os_pass(float2 *buf, int Ns, const float2 *whi, const float2 *wlo) {
+    constexpr int J = kOsM / R;
+    const int j = threadIdx.x, k = j & (Ns - 1);
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = buf[os_pad(j + r * J)];
+    __syncthreads();
+    if (Ns > 1) {
+        const int step = k * (kOsM / (R * Ns));
+#pragma unroll
+        for (int r = 1; r < R; ++r) v[r] = cmul(v[r], os_tw(r * step, whi, wlo));
+    }
+    dft<R>(v);
+    const int base = (j - k) * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) buf[os_pad(base + r * Ns)] = v[brev<R>(r)];
+    __syncthreads();
+}
+
+// The segment's forward transform after its first pass: radix-R passes up to
+// Ns = 4096 (the first pass, Ns = 1, is the caller's).
+template <int R>
+__device__ __forceinline__ void os_middle(float2 *buf, const float2 *whi, const float2 *wlo) {
+#pragma unroll
+    for (int Ns = R; Ns < kOsM / 2; Ns *= R) os_pass<R>(buf, Ns, whi, wlo);
+}
+
+template <int R>
+__global__ void __launch_bounds__(kOsM / R, 1)
+rc_os_kernel(const float2 *__restrict__ in, long long ld_in, int nsamps, int nvalid, int L,
+             int nseg, const float2 *__restrict__ H, const float2 *__restrict__ tw,
+             float2 *__restrict__ out, long long ld_out) {
+    constexpr int T = kOsM / R;  // threads
+    static_assert(R == 8 || R == 16, "radix");
+    extern __shared__ float2 os_sm[];
+    float2 *buf = os_sm, *whi = os_sm + kOsBuf, *wlo = whi + 128;
+    const int line = blockIdx.x / nseg, s0 = (blockIdx.x - line * nseg) * L;
+    const float2 *x = in + (long long)line * ld_in;
+    const int t = threadIdx.x;
+    if (t < kOsTw) whi[t] = tw[t];
+    // forward transform, pass 1 (Ns = 1) straight from the line
+    {
+        float2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int i = s0 + t + r * T;
+            v[r] = i < nsamps ? __ldg(x + i) : make_float2(0.f, 0.f);
+        }
+        dft<R>(v);
+#pragma unroll
+        for (int r = 0; r < R; ++r) buf[os_pad(t * R + r)] = v[brev<R>(r)];
+    }
+    __syncthreads();
+    os_middle<R>(buf, whi, wlo);
+    // last pass (radix 2, Ns = 4096): each item touches only its own pair, so
+    // the filter and the conjugation of the inverse go in place
+#pragma unroll
+    for (int it = 0; it < kOsM / 2 / T; ++it) {
+        const int j = t + it * T;
+        const float2 a = buf[os_pad(j)], b = cmul(buf[os_pad(j + kOsM / 2)], os_tw(j, whi, wlo));
+        buf[os_pad(j)] = cconj(cmul(cadd(a, b), __ldg(H + j)));
+        buf[os_pad(j + kOsM / 2)] = cconj(cmul(csub(a, b), __ldg(H + j + kOsM / 2)));
+    }
+    __syncthreads();
+    // inverse: forward transform of the conjugate
+    os_pass<R>(buf, 1, whi, wlo);
+    os_middle<R>(buf, whi, wlo);
+    float2 *y = out + (long long)line * ld_out + s0;
+    const int nout = min(L, nvalid - s0);
+#pragma unroll
+    for (int it = 0; it < kOsM / 2 / T; ++it) {
+        const int j = t + it * T;
+        const float2 a = buf[os_pad(j)], b = cmul(buf[os_pad(j + kOsM / 2)], os_tw(j, whi, wlo));
+        if (j < nout) y[j] = cconj(cadd(a, b));
+        if (j + kOsM / 2 < nout) y[j + kOsM / 2] = cconj(csub(a, b));
+    }
+}
+constexpr int kOsRadix = 16;  // radix of the passes (8: 1,024 threads, 16: 512)
+
+// Forward DFT (sign -1, unnormalised) of a power-of-two length, in FP64 on
+// the host: iterative radix-2 decimation in time.
+void host_fft(std::vector<std::complex<double>> &a) {
+    const int n = (int)a.size();
+    for (int i = 1, j = 0; i < n; ++i) {
+        int bit = n >> 1;
+        for (; j & bit; bit >>= 1) j ^= bit;
+        j ^= bit;
+        if (i < j) std::swap(a[i], a[j]);
+    }
+    const double pi = 4.0 * std::atan2(1.0, 1.0);
+    for (int len = 2; len <= n; len <<= 1) {
+        for (int k = 0; k < len / 2; ++k) {
+            const std::complex<double> w = std::polar(1.0, -2.0 * pi * k / len);
+            for (int i = 0; i < n; i += len) {
+                const std::complex<double> u = a[i + k], v = a[i + k + len / 2] * w;
+                a[i + k] = u + v;
+                a[i + k + len / 2] = u - v;
+            }
+        }
+    }
+}
+
 struct RcCtx {
     std::mutex mu;
     cufftHandle plan_blk = 0, plan_one = 0;
     bool have_plans = false;
     DevBuf buf, ref;
     float key[4] = {NAN, NAN, NAN, NAN};  // replica parameters of `ref`
+    // overlap-save path: filter spectrum, twiddle tables, their parameters
+    DevBuf os_h, os_tw;
+    bool os_ready = false;
+    float os_key[4] = {NAN, NAN, NAN, NAN};
 };
 RcCtx g_rc[64];
 
@@ -127,6 +311,51 @@ int srg_range_compress_device(const float *lines, long long ld_in, int nlines, i
     RcCtx &x = g_rc[dev];
     std::lock_guard<std::mutex> g(x.mu);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (npts <= kOsMaxPts) {
+        // fused overlap-save kernel (see rc_os_kernel)
+        if ((rc = x.os_h.ensure(sizeof(float2) * kOsM)) || (rc = x.os_tw.ensure(sizeof(float2) * kOsTw)))
+            return rc;
+        const double pi = 4.0 * std::atan2(1.0, 1.0);
+        if (!x.os_ready) {
+            std::vector<float2> tw(kOsTw);
+            for (int h = 0; h < 128; ++h)
+                tw[h] = make_float2((float)std::cos(2.0 * pi * h * 64 / kOsM),
+                                    (float)-std::sin(2.0 * pi * h * 64 / kOsM));
+            for (int l = 0; l < 64; ++l)
+                tw[128 + l] = make_float2((float)std::cos(2.0 * pi * l / kOsM),
+                                          (float)-std::sin(2.0 * pi * l / kOsM));
+            CKR(cudaFuncSetAttribute(rc_os_kernel<kOsRadix>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     kOsSmem));
+            CKR(cudaMemcpyAsync(x.os_tw.p, tw.data(), sizeof(float2) * kOsTw, cudaMemcpyHostToDevice, st));
+            CKR(cudaStreamSynchronize(st));  // `tw` is pageable host memory that goes out of scope
+            x.os_ready = true;
+        }
+        const float key[4] = {samplefreq, startfreq, ramprate, pulselength};
+        if (std::memcmp(key, x.os_key, sizeof key) != 0) {
+            // H = (32768 / 8192) conj(DFT_8192(replica)), in FP64 from the
+            // replica's complex64 samples
+            std::vector<std::complex<double>> a(kOsM);
+            for (int j = 0; j < npts; ++j) a[j] = std::complex<double>(rep[2 * j], rep[2 * j + 1]);
+            host_fft(a);
+            std::vector<float2> h(kOsM);
+            const double scale = (double)kRangeFFT / kOsM;
+            for (int k = 0; k < kOsM; ++k)
+                h[k] = make_float2((float)(scale * a[k].real()), (float)(-scale * a[k].imag()));
+            CKR(cudaMemcpyAsync(x.os_h.p, h.data(), sizeof(float2) * kOsM, cudaMemcpyHostToDevice, st));
+            CKR(cudaStreamSynchronize(st));  // `h` is pageable host memory that goes out of scope
+            std::memcpy(x.os_key, key, sizeof key);
+        }
+        const int L = kOsM - npts + 1;
+        const int nseg = (nvalid + L - 1) / L;
+        if ((long long)nlines * nseg > INT_MAX) return fail(SRG_E_ARG, "too many lines: %d", nlines);
+        rc_os_kernel<kOsRadix><<<nlines * nseg, kOsM / kOsRadix, kOsSmem, st>>>(
+            reinterpret_cast<const float2 *>(lines), ld_in, nsamps, nvalid, L, nseg,
+            static_cast<const float2 *>(x.os_h.p), static_cast<const float2 *>(x.os_tw.p),
+            reinterpret_cast<float2 *>(out), ld_out);
+        CKR(cudaGetLastError());
+        if (nvalid_out) *nvalid_out = nvalid;
+        return SRG_OK;
+    }
     if (!x.have_plans) {
         CKFR(cufftPlan1d(&x.plan_blk, kRangeFFT, CUFFT_C2C, kBlock));
         CKFR(cufftPlan1d(&x.plan_one, kRangeFFT, CUFFT_C2C, 1));

@@ -46,9 +46,9 @@ def torch_cuda():
     return torch
 
 
-def _lines(rng, nlines, nsamps, ntargets=5):
+def _lines(rng, nlines, nsamps, ntargets=5, pulse=PULSE):
     x = (rng.standard_normal((nlines, nsamps)) + 1j * rng.standard_normal((nlines, nsamps))).astype(np.complex64)
-    rep, npts = orc.replica(**PULSE)
+    rep, npts = orc.replica(**pulse)
     for l in range(nlines):
         for d in rng.integers(0, nsamps - npts, ntargets):
             x[l, d:d + npts] += 10.0 * rep[:npts] * npts
@@ -75,6 +75,34 @@ def test_gpu_range_compress_matches_oracle(torch_cuda, nlines, nsamps, pad_in, p
     assert err < 2e-5, err
     if pad_out:
         assert torch.count_nonzero(tout[:, nvalid:]).item() == 0
+
+
+@gpu
+@pytest.mark.parametrize("pulselength", [PULSE["pulselength"], 80.0])
+def test_gpu_range_compress_both_paths(torch_cuda, pulselength):
+    """Pulses of up to 4,096 samples take the fused overlap-save kernel (8,192-
+    point segments), longer ones the cuFFT path (32,768-point rows); both
+    match the oracle at every kept sample, lines with targets near both ends
+    included (the lines of the test above, plus one target per line at an
+    edge or a segment boundary)."""
+    torch = torch_cuda
+    from srg_b200 import api
+    pulse = dict(PULSE, pulselength=pulselength)
+    rep, npts = orc.replica(**pulse)
+    assert (npts <= 4096) == (pulselength == PULSE["pulselength"])
+    rng = np.random.default_rng(npts)
+    nlines, nsamps = 9, 21000
+    x = _lines(rng, nlines, nsamps, pulse=pulse)
+    for l, d in enumerate([0, 1, nsamps - npts, nsamps - npts - 1, 4821, 4822, 9000, 13000, 17000]):
+        d = min(d, nsamps - npts)
+        x[l, d:d + npts] += 10.0 * rep[:npts] * npts
+    want = orc.range_compress(x, **pulse)
+    tin = torch.from_numpy(x).cuda()
+    tout = torch.zeros((nlines, want.shape[1]), dtype=torch.complex64, device="cuda")
+    api.range_compress(tin, nsamps=nsamps, out=tout, **pulse)
+    got = tout.cpu().numpy()
+    err = np.abs(got.astype(np.complex128) - want).max() / np.sqrt(np.mean(np.abs(want) ** 2))
+    assert err < 2e-5, err
 
 
 @gpu
