@@ -84,21 +84,28 @@ __global__ void rc_out_kernel(const float2 *__restrict__ buf, int l0, int nlines
 // linear correlation (the 32,768-point circular one never wraps into them),
 // so 8,192-point transforms give them exactly up to rounding: a segment of
 // 8,192 samples from s0 (zeros past the line) yields y[s0 .. s0 + L),
-// L = 8192 - npts + 1.  One CTA per (line, segment) loads its samples once,
-// transforms them in shared memory, multiplies by the filter
+// L = 8192 - npts + 1.  A CTA (one per SM, persistent) takes (line,
+// segment) items in turn: it loads the segment's samples once, transforms
+// them in shared memory, multiplies by the filter
 // H = (32768 / 8192) conj(DFT_8192(r)), transforms back (a forward transform
 // of the conjugate, conjugated) and writes its L outputs once: the lines
 // cross HBM once each way, where the cuFFT path below takes five passes over
 // 32,768-point rows.  Transforms: Stockham autosort passes of radix 16, 16,
 // 16 and 2 (16 values per thread per pass), each DFT in registers, the
 // padded shared layout i + i / 16 keeping the 16-strided accesses off common
-// banks, twiddles exp(-2 pi i m / 8192) from two small tables
-// (whi[m / 64] wlo[m % 64]).  Pulses of more than 4,096 samples take the
-// cuFFT path.
+// banks, the twiddles of each pass from its own table in shared memory
+// (exactly rounded, laid out so that a warp reads consecutive entries),
+// loaded once per CTA.  Pulses of more than 4,096 samples take the cuFFT
+// path.
 constexpr int kOsM = 8192;                       // segment transform
 constexpr int kOsMaxPts = kOsM / 2;              // longest pulse the segments take
 constexpr int kOsBuf = kOsM + (kOsM >> 4);       // padded segment (float2)
-constexpr int kOsTw = 128 + 64;                  // whi, wlo
+constexpr int kOsThreads = kOsM / 16;            // one radix-16 work item per thread
+// twiddles exp(-2 pi i r k / (16 Ns)) of the passes Ns = 16 and 256 at
+// [(r - 1) Ns + k] (r = 1..15, k < Ns: consecutive k, conflict-free), then
+// exp(-2 pi i k / 8192), k < 4096, of the last radix-2 pass
+constexpr int kOsTw16 = 0, kOsTw256 = 15 * 16, kOsTw2 = kOsTw256 + 15 * 256;
+constexpr int kOsTw = kOsTw2 + kOsM / 2;
 constexpr int kOsSmem = (kOsBuf + kOsTw) * (int)sizeof(float2);
 
 // exp(-2 pi i q / 16), q = 0..7
@@ -121,12 +128,7 @@ __device__ __forceinline__ constexpr int brev(int i) {
         if (i & b) o |= t;
     return o;
 }
-// exp(-2 pi i m / 8192), 0 <= m < 8192
-__device__ __forceinline__ float2 os_tw(int m, const float2 *whi, const float2 *wlo) {
-    return cmul(whi[m >> 6], wlo[m & 63]);
-}
-
-// R-point DFT in registers (R = 8 or 16), in place: input X in natural
+// R-point DFT in registers (R <= 16), in place: input X in natural
 // order, output DFT(X)[r] in v[brev<R>(r)] (radix-2 decimation in time on
 // the bit-reversed view a[p] = v[brev<R>(p)], so no permutation moves data;
 // the butterflies of half-size h take exp(-2 pi i q / (2h)) = kW16[8 q / h]).
@@ -147,89 +149,81 @@ __device__ __forceinline__ void dft(float2 (&v)[R]) {
     }
 }
 
-// One radix-R Stockham pass over the segment in shared memory, one work item
-// per thread (8192 / R threads): item j reads v[r] = x[j + r 8192 / R],
-// scales v[r] by exp(-2 pi i r k / (R Ns)), k = j mod Ns, takes the R-point
-// DFT and writes y[(j - k) R + k + r Ns].
-template <int R>
-__device__ __forceinline__ void os_pass(float2 *buf, int Ns, const float2 *whi, const float2 *wlo) {
-    constexpr int J = kOsM / R;
+// One radix-16 Stockham pass over the segment in shared memory, one work
+// item per thread: item j reads v[r] = x[j + 512 r], scales v[r] by
+// exp(-2 pi i r k / (16 Ns)) = tw[(r - 1) Ns + k], k = j mod Ns, takes the
+// 16-point DFT and writes y[(j - k) 16 + k + r Ns].
+__device__ __forceinline__ void os_pass(float2 *buf, int Ns, const float2 *tw) {
     const int j = threadIdx.x, k = j & (Ns - 1);
-    float2 v[R];
+    float2 v[16];
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = buf[os_pad(j + r * J)];
+    for (int r = 0; r < 16; ++r) v[r] = buf[os_pad(j + r * kOsThreads)];
     __syncthreads();
     if (Ns > 1) {
-        const int step = k * (kOsM / (R * Ns));
 #pragma unroll
-        for (int r = 1; r < R; ++r) v[r] = cmul(v[r], os_tw(r * step, whi, wlo));
+        for (int r = 1; r < 16; ++r) v[r] = cmul(v[r], tw[(r - 1) * Ns + k]);
     }
-    dft<R>(v);
-    const int base = (j - k) * R + k;
+    dft<16>(v);
+    const int base = (j - k) * 16 + k;
 #pragma unroll
-    for (int r = 0; r < R; ++r) buf[os_pad(base + r * Ns)] = v[brev<R>(r)];
+    for (int r = 0; r < 16; ++r) buf[os_pad(base + r * Ns)] = v[brev<16>(r)];
     __syncthreads();
 }
 
-// The segment's forward transform after its first pass: radix-R passes up to
-// Ns = 4096 (the first pass, Ns = 1, is the caller's).
-template <int R>
-__device__ __forceinline__ void os_middle(float2 *buf, const float2 *whi, const float2 *wlo) {
-#pragma unroll
-    for (int Ns = R; Ns < kOsM / 2; Ns *= R) os_pass<R>(buf, Ns, whi, wlo);
-}
-
-template <int R>
-__global__ void __launch_bounds__(kOsM / R, 1)
+// Persistent: each CTA takes segments (line, s0) in turn, after loading the
+// twiddle tables once.
+__global__ void __launch_bounds__(kOsThreads, 1)
 rc_os_kernel(const float2 *__restrict__ in, long long ld_in, int nsamps, int nvalid, int L,
-             int nseg, const float2 *__restrict__ H, const float2 *__restrict__ tw,
+             int nseg, int nitems, const float2 *__restrict__ H, const float2 *__restrict__ twg,
              float2 *__restrict__ out, long long ld_out) {
-    constexpr int T = kOsM / R;  // threads
-    static_assert(R == 8 || R == 16, "radix");
     extern __shared__ float2 os_sm[];
-    float2 *buf = os_sm, *whi = os_sm + kOsBuf, *wlo = whi + 128;
-    const int line = blockIdx.x / nseg, s0 = (blockIdx.x - line * nseg) * L;
-    const float2 *x = in + (long long)line * ld_in;
+    float2 *buf = os_sm, *tw = os_sm + kOsBuf;
     const int t = threadIdx.x;
-    if (t < kOsTw) whi[t] = tw[t];
-    // forward transform, pass 1 (Ns = 1) straight from the line
-    {
-        float2 v[R];
+    for (int i = t; i < kOsTw; i += kOsThreads) tw[i] = __ldg(twg + i);
+    for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+        const int line = item / nseg, s0 = (item - line * nseg) * L;
+        const float2 *x = in + (long long)line * ld_in;
+        // forward transform, pass 1 (Ns = 1) straight from the line
+        {
+            float2 v[16];
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const int i = s0 + t + r * T;
-            v[r] = i < nsamps ? __ldg(x + i) : make_float2(0.f, 0.f);
+            for (int r = 0; r < 16; ++r) {
+                const int i = s0 + t + r * kOsThreads;
+                v[r] = i < nsamps ? __ldg(x + i) : make_float2(0.f, 0.f);
+            }
+            dft<16>(v);
+#pragma unroll
+            for (int r = 0; r < 16; ++r) buf[os_pad(t * 16 + r)] = v[brev<16>(r)];
         }
-        dft<R>(v);
+        __syncthreads();  // (the first time also the tables)
+        os_pass(buf, 16, tw + kOsTw16);
+        os_pass(buf, 256, tw + kOsTw256);
+        // last pass (radix 2, Ns = 4096): each item touches only its own pair,
+        // so the filter and the conjugation of the inverse go in place
 #pragma unroll
-        for (int r = 0; r < R; ++r) buf[os_pad(t * R + r)] = v[brev<R>(r)];
-    }
-    __syncthreads();
-    os_middle<R>(buf, whi, wlo);
-    // last pass (radix 2, Ns = 4096): each item touches only its own pair, so
-    // the filter and the conjugation of the inverse go in place
+        for (int it = 0; it < kOsM / 2 / kOsThreads; ++it) {
+            const int j = t + it * kOsThreads;
+            const float2 a = buf[os_pad(j)], b = cmul(buf[os_pad(j + kOsM / 2)], tw[kOsTw2 + j]);
+            buf[os_pad(j)] = cconj(cmul(cadd(a, b), __ldg(H + j)));
+            buf[os_pad(j + kOsM / 2)] = cconj(cmul(csub(a, b), __ldg(H + j + kOsM / 2)));
+        }
+        __syncthreads();
+        // inverse: forward transform of the conjugate
+        os_pass(buf, 1, nullptr);
+        os_pass(buf, 16, tw + kOsTw16);
+        os_pass(buf, 256, tw + kOsTw256);
+        float2 *y = out + (long long)line * ld_out + s0;
+        const int nout = min(L, nvalid - s0);
 #pragma unroll
-    for (int it = 0; it < kOsM / 2 / T; ++it) {
-        const int j = t + it * T;
-        const float2 a = buf[os_pad(j)], b = cmul(buf[os_pad(j + kOsM / 2)], os_tw(j, whi, wlo));
-        buf[os_pad(j)] = cconj(cmul(cadd(a, b), __ldg(H + j)));
-        buf[os_pad(j + kOsM / 2)] = cconj(cmul(csub(a, b), __ldg(H + j + kOsM / 2)));
-    }
-    __syncthreads();
-    // inverse: forward transform of the conjugate
-    os_pass<R>(buf, 1, whi, wlo);
-    os_middle<R>(buf, whi, wlo);
-    float2 *y = out + (long long)line * ld_out + s0;
-    const int nout = min(L, nvalid - s0);
-#pragma unroll
-    for (int it = 0; it < kOsM / 2 / T; ++it) {
-        const int j = t + it * T;
-        const float2 a = buf[os_pad(j)], b = cmul(buf[os_pad(j + kOsM / 2)], os_tw(j, whi, wlo));
-        if (j < nout) y[j] = cconj(cadd(a, b));
-        if (j + kOsM / 2 < nout) y[j + kOsM / 2] = cconj(csub(a, b));
+        for (int it = 0; it < kOsM / 2 / kOsThreads; ++it) {
+            const int j = t + it * kOsThreads;
+            const float2 a = buf[os_pad(j)], b = cmul(buf[os_pad(j + kOsM / 2)], tw[kOsTw2 + j]);
+            if (j < nout) y[j] = cconj(cadd(a, b));
+            if (j + kOsM / 2 < nout) y[j + kOsM / 2] = cconj(csub(a, b));
+        }
+        __syncthreads();  // the segment's reads are done before the next one's writes
     }
 }
-constexpr int kOsRadix = 16;  // radix of the passes (8: 1,024 threads, 16: 512)
 
 // Forward DFT (sign -1, unnormalised) of a power-of-two length, in FP64 on
 // the host: iterative radix-2 decimation in time.
@@ -263,6 +257,7 @@ struct RcCtx {
     // overlap-save path: filter spectrum, twiddle tables, their parameters
     DevBuf os_h, os_tw;
     bool os_ready = false;
+    int sms = 0;
     float os_key[4] = {NAN, NAN, NAN, NAN};
 };
 RcCtx g_rc[64];
@@ -318,14 +313,16 @@ int srg_range_compress_device(const float *lines, long long ld_in, int nlines, i
         const double pi = 4.0 * std::atan2(1.0, 1.0);
         if (!x.os_ready) {
             std::vector<float2> tw(kOsTw);
-            for (int h = 0; h < 128; ++h)
-                tw[h] = make_float2((float)std::cos(2.0 * pi * h * 64 / kOsM),
-                                    (float)-std::sin(2.0 * pi * h * 64 / kOsM));
-            for (int l = 0; l < 64; ++l)
-                tw[128 + l] = make_float2((float)std::cos(2.0 * pi * l / kOsM),
-                                          (float)-std::sin(2.0 * pi * l / kOsM));
-            CKR(cudaFuncSetAttribute(rc_os_kernel<kOsRadix>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     kOsSmem));
+            auto w = [&](double num, double den) {
+                return make_float2((float)std::cos(2.0 * pi * num / den), (float)-std::sin(2.0 * pi * num / den));
+            };
+            for (int Ns : {16, 256})
+                for (int r = 1; r < 16; ++r)
+                    for (int k = 0; k < Ns; ++k)
+                        tw[(Ns == 16 ? kOsTw16 : kOsTw256) + (r - 1) * Ns + k] = w((double)r * k, 16.0 * Ns);
+            for (int k = 0; k < kOsM / 2; ++k) tw[kOsTw2 + k] = w(k, kOsM);
+            CKR(cudaFuncSetAttribute(rc_os_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kOsSmem));
+            CKR(cudaDeviceGetAttribute(&x.sms, cudaDevAttrMultiProcessorCount, dev));
             CKR(cudaMemcpyAsync(x.os_tw.p, tw.data(), sizeof(float2) * kOsTw, cudaMemcpyHostToDevice, st));
             CKR(cudaStreamSynchronize(st));  // `tw` is pageable host memory that goes out of scope
             x.os_ready = true;
@@ -348,8 +345,9 @@ int srg_range_compress_device(const float *lines, long long ld_in, int nlines, i
         const int L = kOsM - npts + 1;
         const int nseg = (nvalid + L - 1) / L;
         if ((long long)nlines * nseg > INT_MAX) return fail(SRG_E_ARG, "too many lines: %d", nlines);
-        rc_os_kernel<kOsRadix><<<nlines * nseg, kOsM / kOsRadix, kOsSmem, st>>>(
-            reinterpret_cast<const float2 *>(lines), ld_in, nsamps, nvalid, L, nseg,
+        const int nitems = nlines * nseg;
+        rc_os_kernel<<<std::min(nitems, x.sms), kOsThreads, kOsSmem, st>>>(
+            reinterpret_cast<const float2 *>(lines), ld_in, nsamps, nvalid, L, nseg, nitems,
             static_cast<const float2 *>(x.os_h.p), static_cast<const float2 *>(x.os_tw.p),
             reinterpret_cast<float2 *>(out), ld_out);
         CKR(cudaGetLastError());
