@@ -3,9 +3,10 @@
 // Follows int/crossmul.f90:95-185 line for line in what it computes; the
 // layout is the GPU's: every output line of every pair is independent, so the
 // images are transformed whole (one batched FFT per image and direction,
-// cuFFT) and one fused kernel forms the cross products, the two-sample
-// reclaim, the looks down and across, the square-rooted amplitudes and the
-// zero-input mask.  Per image:
+// cuFFT; for lines of 2,049-4,096 samples one fused shared-memory kernel per
+// line instead, upsample4096_kernel) and one fused kernel forms the cross
+// products, the two-sample reclaim, the looks down and across, the
+// square-rooted amplitudes and the zero-input mask.  Per image:
 //   1. in * scale, zero-padded from na to nnn = the first 2^i >= na (i >= 1)
 //      (crossmul.f90:69-73, 128-135);
 //   2. forward FFT of nnn points (FFTW sign -1, unnormalised);
@@ -27,6 +28,7 @@
 
 #include "../../include/srg_bp.h"
 #include "host_internal.h"
+#include "smem_fft.cuh"
 
 using namespace srg;
 using namespace srg::detail;
@@ -137,6 +139,76 @@ __global__ void crossmul_looks_kernel(const float2 *__restrict__ up1, const floa
     }
 }
 
+// Steps 1-4 for one image when nnn = 4096 (lines of 2,049-4,096 samples),
+// fused per line in shared memory: in * scale padded to 4,096, the forward
+// transform, the spread into 8,192 bins and the inverse transform (the
+// forward transform of the conjugate, conjugated; unnormalised), written
+// once as the line's 8,192 upsampled samples: the image crosses HBM once
+// each way where the cuFFT path takes five passes over padded rows.
+// Persistent: one CTA of smem_fft::kThreads per SM takes lines in turn,
+// after loading the twiddle tables once.
+constexpr int kXmSmem = (smem_fft::kBuf + smem_fft::kTw) * (int)sizeof(float2);
+
+__global__ void __launch_bounds__(smem_fft::kThreads, 1)
+upsample4096_kernel(const float2 *__restrict__ in, long long ld, int na, int nl, float scale,
+                    const float2 *__restrict__ twg, float2 *__restrict__ up) {
+    using namespace smem_fft;
+    constexpr int N = 4096, N2 = 8192, T = kThreads;
+    extern __shared__ float2 xm_sm[];
+    float2 *buf = xm_sm, *tw = xm_sm + kBuf;
+    const int t = threadIdx.x;
+    for (int i = t; i < kTw; i += T) tw[i] = __ldg(twg + i);
+    for (int l = blockIdx.x; l < nl; l += gridDim.x) {
+        const float2 *x = in + (long long)l * ld;
+        // forward 4,096-point transform, pass 1 (Ns = 1) from the line
+        if (t < N / 16) {
+            float2 v[16];
+#pragma unroll
+            for (int r = 0; r < 16; ++r) {
+                const int i = t + r * (N / 16);
+                float2 a = make_float2(0.f, 0.f);
+                if (i < na) {
+                    a = __ldg(x + i);
+                    a = make_float2(a.x * scale, a.y * scale);
+                }
+                v[r] = a;
+            }
+            dft<16>(v);
+#pragma unroll
+            for (int r = 0; r < 16; ++r) buf[pad(t * 16 + r)] = v[brev<16>(r)];
+        }
+        __syncthreads();  // (the first time also the tables)
+        pass16<N>(buf, 16, tw + kTw16);
+        pass16<N>(buf, 256, tw + kTw256);
+        // spread, conjugated: Y[m] = conj X[m] (m < 2048), 0 (2048 <= m < 6144),
+        // conj X[m - 4096] (m >= 6144)
+        float2 hi[N / 2 / T];
+#pragma unroll
+        for (int q = 0; q < N / 2 / T; ++q) hi[q] = buf[pad(N / 2 + t + q * T)];
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < N / 2 / T; ++q) buf[pad(t + q * T)] = cconj(buf[pad(t + q * T)]);
+#pragma unroll
+        for (int q = 0; q < N / T; ++q) buf[pad(N / 2 + t + q * T)] = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int q = 0; q < N / 2 / T; ++q) buf[pad(N2 - N / 2 + t + q * T)] = cconj(hi[q]);
+        __syncthreads();
+        // 8,192-point forward transform of the conjugate
+        pass16<N2>(buf, 1, nullptr);
+        pass16<N2>(buf, 16, tw + kTw16);
+        pass16<N2>(buf, 256, tw + kTw256);
+        float2 *u = up + (long long)l * N2;
+#pragma unroll
+        for (int it = 0; it < N2 / 2 / T; ++it) {
+            const int j = t + it * T;
+            const float2 a = buf[pad(j)], b = cmul(buf[pad(j + N2 / 2)], tw[kTw2 + j]);
+            u[j] = cconj(cadd(a, b));
+            u[j + N2 / 2] = cconj(csub(a, b));
+        }
+        __syncthreads();  // the line's reads are done before the next one's writes
+    }
+}
+
 struct Plan {
     int n = 0, batch = 0;
     cufftHandle h = 0;
@@ -147,6 +219,9 @@ struct XmCtx {
     std::mutex mu;
     Plan fwd, inv;
     DevBuf pad, upA, upB;
+    DevBuf tw;          // twiddle tables of the fused upsampling (smem_fft)
+    bool fused_ready = false;
+    int sms = 0;
 };
 XmCtx g_xm[64];
 
@@ -169,6 +244,12 @@ int grid_for(long long n) {
 // upsampled lines of one image into `up` (nl x 2nnn)
 int upsample(XmCtx &x, const float2 *in, long long ld, int na, int nnn, int nl, float scale,
              float2 *up, cudaStream_t st) {
+    if (nnn == 4096) {
+        upsample4096_kernel<<<std::min(nl, x.sms), smem_fft::kThreads, kXmSmem, st>>>(
+            in, ld, na, nl, scale, static_cast<const float2 *>(x.tw.p), up);
+        CKC(cudaGetLastError());
+        return SRG_OK;
+    }
     float2 *pad = static_cast<float2 *>(x.pad.p);
     pad_scale_kernel<<<grid_for((long long)nl * nnn), 256, 0, st>>>(in, ld, na, nnn, nl, scale, pad);
     CKC(cudaGetLastError());
@@ -218,11 +299,24 @@ int run_stack(const float *const *slcs, int n, long long ld, int na, int nlines,
     const int nnn = fft_length(na);
     const int nout_lines = nlines / looksdn, nout_cols = na / looksac;
     const int nl = nout_lines * looksdn;
-    if ((rc = plan_for(x.fwd, nnn, nl)) || (rc = plan_for(x.inv, 2 * nnn, nl))) return rc;
-    const size_t up_bytes = (size_t)nl * 2 * nnn * sizeof(float2);
-    if ((rc = x.pad.ensure((size_t)nl * nnn * sizeof(float2))) || (rc = x.upA.ensure(up_bytes)) ||
-        (rc = x.upB.ensure(up_bytes)))
+    if (nnn == 4096) {  // the fused upsampling (upsample4096_kernel)
+        if (!x.fused_ready) {
+            if ((rc = x.tw.ensure(sizeof(float2) * smem_fft::kTw))) return rc;
+            const std::vector<float2> tw = smem_fft::twiddle_tables();
+            CKC(cudaFuncSetAttribute(upsample4096_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     kXmSmem));
+            CKC(cudaDeviceGetAttribute(&x.sms, cudaDevAttrMultiProcessorCount, dev));
+            CKC(cudaMemcpyAsync(x.tw.p, tw.data(), sizeof(float2) * smem_fft::kTw,
+                                cudaMemcpyHostToDevice, st));
+            CKC(cudaStreamSynchronize(st));  // `tw` is pageable host memory that goes out of scope
+            x.fused_ready = true;
+        }
+    } else if ((rc = plan_for(x.fwd, nnn, nl)) || (rc = plan_for(x.inv, 2 * nnn, nl)) ||
+               (rc = x.pad.ensure((size_t)nl * nnn * sizeof(float2)))) {
         return rc;
+    }
+    const size_t up_bytes = (size_t)nl * 2 * nnn * sizeof(float2);
+    if ((rc = x.upA.ensure(up_bytes)) || (rc = x.upB.ensure(up_bytes))) return rc;
     float2 *cur = static_cast<float2 *>(x.upA.p), *nxt = static_cast<float2 *>(x.upB.p);
     if ((rc = upsample(x, reinterpret_cast<const float2 *>(slcs[0]), ld, na, nnn, nl, scale, cur, st)))
         return rc;

@@ -24,6 +24,7 @@
 
 #include "../../include/srg_bp.h"
 #include "host_internal.h"
+#include "smem_fft.cuh"
 
 using namespace srg;
 using namespace srg::detail;
@@ -99,75 +100,20 @@ __global__ void rc_out_kernel(const float2 *__restrict__ buf, int l0, int nlines
 // path.
 constexpr int kOsM = 8192;                       // segment transform
 constexpr int kOsMaxPts = kOsM / 2;              // longest pulse the segments take
-constexpr int kOsBuf = kOsM + (kOsM >> 4);       // padded segment (float2)
-constexpr int kOsThreads = kOsM / 16;            // one radix-16 work item per thread
-// twiddles exp(-2 pi i r k / (16 Ns)) of the passes Ns = 16 and 256 at
-// [(r - 1) Ns + k] (r = 1..15, k < Ns: consecutive k, conflict-free), then
-// exp(-2 pi i k / 8192), k < 4096, of the last radix-2 pass
-constexpr int kOsTw16 = 0, kOsTw256 = 15 * 16, kOsTw2 = kOsTw256 + 15 * 256;
-constexpr int kOsTw = kOsTw2 + kOsM / 2;
+constexpr int kOsBuf = smem_fft::kBuf;          // padded segment (float2)
+constexpr int kOsThreads = smem_fft::kThreads;   // one radix-16 work item per thread
+constexpr int kOsTw16 = smem_fft::kTw16, kOsTw256 = smem_fft::kTw256, kOsTw2 = smem_fft::kTw2;
+constexpr int kOsTw = smem_fft::kTw;
 constexpr int kOsSmem = (kOsBuf + kOsTw) * (int)sizeof(float2);
-
-// exp(-2 pi i q / 16), q = 0..7
-__constant__ float2 kW16[8] = {{1.000000000f, 0.000000000f},   {0.923879533f, -0.382683432f},
-                               {0.707106781f, -0.707106781f},  {0.382683432f, -0.923879533f},
-                               {0.000000000f, -1.000000000f},  {-0.382683432f, -0.923879533f},
-                               {-0.707106781f, -0.707106781f}, {-0.923879533f, -0.382683432f}};
-
-__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
-}
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
-__device__ __forceinline__ int os_pad(int i) { return i + (i >> 4); }
-template <int R>
-__device__ __forceinline__ constexpr int brev(int i) {
-    int o = 0;
-    for (int b = 1, t = R >> 1; b < R; b <<= 1, t >>= 1)
-        if (i & b) o |= t;
-    return o;
-}
-// R-point DFT in registers (R <= 16), in place: input X in natural
-// order, output DFT(X)[r] in v[brev<R>(r)] (radix-2 decimation in time on
-// the bit-reversed view a[p] = v[brev<R>(p)], so no permutation moves data;
-// the butterflies of half-size h take exp(-2 pi i q / (2h)) = kW16[8 q / h]).
-template <int R>
-__device__ __forceinline__ void dft(float2 (&v)[R]) {
-#pragma unroll
-    for (int h = 1; h < R; h <<= 1) {
-#pragma unroll
-        for (int i = 0; i < R; i += 2 * h) {
-#pragma unroll
-            for (int q = 0; q < h; ++q) {
-                float2 &lo = v[brev<R>(i + q)], &hi = v[brev<R>(i + q + h)];
-                const float2 b = q == 0 ? hi : cmul(hi, kW16[q * (8 / h)]);
-                hi = csub(lo, b);
-                lo = cadd(lo, b);
-            }
-        }
-    }
-}
-
-// One radix-16 Stockham pass over the segment in shared memory, one work
-// item per thread: item j reads v[r] = x[j + 512 r], scales v[r] by
-// exp(-2 pi i r k / (16 Ns)) = tw[(r - 1) Ns + k], k = j mod Ns, takes the
-// 16-point DFT and writes y[(j - k) 16 + k + r Ns].
+using smem_fft::brev;
+using smem_fft::cadd;
+using smem_fft::cconj;
+using smem_fft::cmul;
+using smem_fft::csub;
+using smem_fft::dft;
+__device__ __forceinline__ int os_pad(int i) { return smem_fft::pad(i); }
 __device__ __forceinline__ void os_pass(float2 *buf, int Ns, const float2 *tw) {
-    const int j = threadIdx.x, k = j & (Ns - 1);
-    float2 v[16];
-#pragma unroll
-    for (int r = 0; r < 16; ++r) v[r] = buf[os_pad(j + r * kOsThreads)];
-    __syncthreads();
-    if (Ns > 1) {
-#pragma unroll
-        for (int r = 1; r < 16; ++r) v[r] = cmul(v[r], tw[(r - 1) * Ns + k]);
-    }
-    dft<16>(v);
-    const int base = (j - k) * 16 + k;
-#pragma unroll
-    for (int r = 0; r < 16; ++r) buf[os_pad(base + r * Ns)] = v[brev<16>(r)];
-    __syncthreads();
+    smem_fft::pass16<kOsM>(buf, Ns, tw);
 }
 
 // Persistent: each CTA takes segments (line, s0) in turn, after loading the
@@ -312,15 +258,7 @@ int srg_range_compress_device(const float *lines, long long ld_in, int nlines, i
             return rc;
         const double pi = 4.0 * std::atan2(1.0, 1.0);
         if (!x.os_ready) {
-            std::vector<float2> tw(kOsTw);
-            auto w = [&](double num, double den) {
-                return make_float2((float)std::cos(2.0 * pi * num / den), (float)-std::sin(2.0 * pi * num / den));
-            };
-            for (int Ns : {16, 256})
-                for (int r = 1; r < 16; ++r)
-                    for (int k = 0; k < Ns; ++k)
-                        tw[(Ns == 16 ? kOsTw16 : kOsTw256) + (r - 1) * Ns + k] = w((double)r * k, 16.0 * Ns);
-            for (int k = 0; k < kOsM / 2; ++k) tw[kOsTw2 + k] = w(k, kOsM);
+            const std::vector<float2> tw = smem_fft::twiddle_tables();
             CKR(cudaFuncSetAttribute(rc_os_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kOsSmem));
             CKR(cudaDeviceGetAttribute(&x.sms, cudaDevAttrMultiProcessorCount, dev));
             CKR(cudaMemcpyAsync(x.os_tw.p, tw.data(), sizeof(float2) * kOsTw, cudaMemcpyHostToDevice, st));

@@ -93,7 +93,9 @@ def _close(got, want, tol=2e-5):
 @gpu
 @pytest.mark.parametrize("na,nd,lac,ldn,scale,mask", [
     (300, 40, 2, 3, 0.5, True), (64, 16, 1, 1, 1.0, False), (257, 9, 4, 2, 2.0, True),
-    (1000, 6, 5, 1, 1.0, True)])
+    (1000, 6, 5, 1, 1.0, True),
+    # lines of 2,049-4,096 samples: the fused shared-memory upsampling
+    (2500, 12, 4, 2, 0.5, True), (4096, 5, 1, 1, 1.0, False), (2049, 4, 3, 1, 2.0, True)])
 def test_gpu_crossmul_matches_oracle(torch_cuda, na, nd, lac, ldn, scale, mask):
     torch = torch_cuda
     from srg_b200 import api
@@ -126,11 +128,12 @@ def test_gpu_crossmul_row_stride_and_valid_lines(torch_cuda):
 
 
 @gpu
-def test_gpu_crossmul_stack_equals_pairs(torch_cuda):
+@pytest.mark.parametrize("na", [200, 2600])
+def test_gpu_crossmul_stack_equals_pairs(torch_cuda, na):
     torch = torch_cuda
     from srg_b200 import api
     rng = np.random.default_rng(8)
-    imgs = [torch.from_numpy(_img(rng, 24, 200)).cuda() for _ in range(5)]
+    imgs = [torch.from_numpy(_img(rng, 24, na)).cuda() for _ in range(5)]
     igs, ams = api.crossmul_stack(imgs, looksac=2, looksdn=4, scale=0.25)
     for k in range(4):
         ig, am = api.crossmul(imgs[k], imgs[k + 1], looksac=2, looksdn=4, scale=0.25)
