@@ -149,63 +149,150 @@ __global__ void crossmul_looks_kernel(const float2 *__restrict__ up1, const floa
 // after loading the twiddle tables once.
 constexpr int kXmSmem = (smem_fft::kBuf + smem_fft::kTw) * (int)sizeof(float2);
 
+// One line of one image, steps 1-4 with nnn = 4096: the 8,192 upsampled
+// samples (unnormalised) left in buf (padded layout, natural order).  All
+// kThreads threads call it; tw holds the twiddle tables.
+__device__ __forceinline__ void upsample_line(const float2 *__restrict__ x, int na, float scale,
+                                              float2 *buf, const float2 *tw) {
+    using namespace smem_fft;
+    constexpr int N = 4096, N2 = 8192, T = kThreads;
+    const int t = threadIdx.x;
+    // forward 4,096-point transform, pass 1 (Ns = 1) from the line
+    if (t < N / 16) {
+        float2 v[16];
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+            const int i = t + r * (N / 16);
+            float2 a = make_float2(0.f, 0.f);
+            if (i < na) {
+                a = __ldg(x + i);
+                a = make_float2(a.x * scale, a.y * scale);
+            }
+            v[r] = a;
+        }
+        dft<16>(v);
+#pragma unroll
+        for (int r = 0; r < 16; ++r) buf[pad(t * 16 + r)] = v[brev<16>(r)];
+    }
+    __syncthreads();
+    pass16<N>(buf, 16, tw + kTw16);
+    pass16<N>(buf, 256, tw + kTw256);
+    // spread, conjugated: Y[m] = conj X[m] (m < 2048), 0 (2048 <= m < 6144),
+    // conj X[m - 4096] (m >= 6144)
+    float2 hi[N / 2 / T];
+#pragma unroll
+    for (int q = 0; q < N / 2 / T; ++q) hi[q] = buf[pad(N / 2 + t + q * T)];
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < N / 2 / T; ++q) buf[pad(t + q * T)] = cconj(buf[pad(t + q * T)]);
+#pragma unroll
+    for (int q = 0; q < N / T; ++q) buf[pad(N / 2 + t + q * T)] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int q = 0; q < N / 2 / T; ++q) buf[pad(N2 - N / 2 + t + q * T)] = cconj(hi[q]);
+    __syncthreads();
+    // 8,192-point forward transform of the conjugate; its last (radix-2) pass
+    // touches only each item's own pair, so it goes in place
+    pass16<N2>(buf, 1, nullptr);
+    pass16<N2>(buf, 16, tw + kTw16);
+    pass16<N2>(buf, 256, tw + kTw256);
+#pragma unroll
+    for (int it = 0; it < N2 / 2 / T; ++it) {
+        const int j = t + it * T;
+        const float2 a = buf[pad(j)], b = cmul(buf[pad(j + N2 / 2)], tw[kTw2 + j]);
+        buf[pad(j)] = cconj(cadd(a, b));
+        buf[pad(j + N2 / 2)] = cconj(csub(a, b));
+    }
+    __syncthreads();
+}
+
 __global__ void __launch_bounds__(smem_fft::kThreads, 1)
 upsample4096_kernel(const float2 *__restrict__ in, long long ld, int na, int nl, float scale,
                     const float2 *__restrict__ twg, float2 *__restrict__ up) {
     using namespace smem_fft;
-    constexpr int N = 4096, N2 = 8192, T = kThreads;
     extern __shared__ float2 xm_sm[];
     float2 *buf = xm_sm, *tw = xm_sm + kBuf;
     const int t = threadIdx.x;
-    for (int i = t; i < kTw; i += T) tw[i] = __ldg(twg + i);
+    for (int i = t; i < kTw; i += kThreads) tw[i] = __ldg(twg + i);
+    __syncthreads();
     for (int l = blockIdx.x; l < nl; l += gridDim.x) {
-        const float2 *x = in + (long long)l * ld;
-        // forward 4,096-point transform, pass 1 (Ns = 1) from the line
-        if (t < N / 16) {
-            float2 v[16];
-#pragma unroll
-            for (int r = 0; r < 16; ++r) {
-                const int i = t + r * (N / 16);
-                float2 a = make_float2(0.f, 0.f);
-                if (i < na) {
-                    a = __ldg(x + i);
-                    a = make_float2(a.x * scale, a.y * scale);
-                }
-                v[r] = a;
-            }
-            dft<16>(v);
-#pragma unroll
-            for (int r = 0; r < 16; ++r) buf[pad(t * 16 + r)] = v[brev<16>(r)];
-        }
-        __syncthreads();  // (the first time also the tables)
-        pass16<N>(buf, 16, tw + kTw16);
-        pass16<N>(buf, 256, tw + kTw256);
-        // spread, conjugated: Y[m] = conj X[m] (m < 2048), 0 (2048 <= m < 6144),
-        // conj X[m - 4096] (m >= 6144)
-        float2 hi[N / 2 / T];
-#pragma unroll
-        for (int q = 0; q < N / 2 / T; ++q) hi[q] = buf[pad(N / 2 + t + q * T)];
-        __syncthreads();
-#pragma unroll
-        for (int q = 0; q < N / 2 / T; ++q) buf[pad(t + q * T)] = cconj(buf[pad(t + q * T)]);
-#pragma unroll
-        for (int q = 0; q < N / T; ++q) buf[pad(N / 2 + t + q * T)] = make_float2(0.f, 0.f);
-#pragma unroll
-        for (int q = 0; q < N / 2 / T; ++q) buf[pad(N2 - N / 2 + t + q * T)] = cconj(hi[q]);
-        __syncthreads();
-        // 8,192-point forward transform of the conjugate
-        pass16<N2>(buf, 1, nullptr);
-        pass16<N2>(buf, 16, tw + kTw16);
-        pass16<N2>(buf, 256, tw + kTw256);
-        float2 *u = up + (long long)l * N2;
-#pragma unroll
-        for (int it = 0; it < N2 / 2 / T; ++it) {
-            const int j = t + it * T;
-            const float2 a = buf[pad(j)], b = cmul(buf[pad(j + N2 / 2)], tw[kTw2 + j]);
-            u[j] = cconj(cadd(a, b));
-            u[j + N2 / 2] = cconj(csub(a, b));
-        }
+        upsample_line(in + (long long)l * ld, na, scale, buf, tw);
+        float2 *u = up + (long long)l * 8192;
+        for (int j = t; j < 8192; j += kThreads) u[j] = buf[pad(j)];
         __syncthreads();  // the line's reads are done before the next one's writes
+    }
+}
+
+// The whole stack with looks of one line down and nnn = 4096, fused: per grid
+// line, image k's upsampled line is made in one shared buffer while image
+// k - 1's is still in the other, and the pair's interferogram and amplitude
+// samples of that line are formed from the two (the sums of
+// crossmul_looks_kernel with looksdn = 1, in its order): the images are read
+// once and no upsampled image goes through HBM.  Persistent over lines.
+constexpr int kXmStackSmem = (2 * smem_fft::kBuf + smem_fft::kTw) * (int)sizeof(float2);
+
+__global__ void __launch_bounds__(smem_fft::kThreads, 1)
+crossmul_stack4096_kernel(const float2 *const *__restrict__ imgs, int n, long long ld, int na,
+                          int nlines, int nout_cols, int looksac, float scale, int mask,
+                          const float2 *__restrict__ twg, float2 *const *__restrict__ igrams,
+                          float2 *const *__restrict__ amps) {
+    using namespace smem_fft;
+    extern __shared__ float2 xm_sm[];
+    float2 *tw = xm_sm + 2 * kBuf;
+    const int t = threadIdx.x;
+    for (int i = t; i < kTw; i += kThreads) tw[i] = __ldg(twg + i);
+    __syncthreads();
+    const float inv = 1.f / 4096.f;  // a power of two: same as the reference's division
+    for (int l = blockIdx.x; l < nlines; l += gridDim.x) {
+        for (int k = 0; k < n; ++k) {
+            float2 *cur = xm_sm + (k & 1) * kBuf;
+            upsample_line(imgs[k] + (long long)l * ld, na, scale, cur, tw);
+            if (k == 0) continue;
+            const float2 *up1 = xm_sm + ((k - 1) & 1) * kBuf, *up2 = cur;
+            const float2 *in1 = imgs[k - 1] + (long long)l * ld, *in2 = imgs[k] + (long long)l * ld;
+            for (int j = t; j < nout_cols; j += kThreads) {
+                float2 ig = make_float2(0.f, 0.f), am = make_float2(0.f, 0.f);
+                float2 m1 = make_float2(0.f, 0.f), m2 = make_float2(0.f, 0.f);
+                for (int q = 0; q < looksac; ++q) {
+                    const int c = j * looksac + q;
+                    float2 gd = make_float2(0.f, 0.f), ad = make_float2(0.f, 0.f);
+                    float2 s1 = make_float2(0.f, 0.f), s2 = make_float2(0.f, 0.f);
+                    float2 a0 = up1[pad(2 * c)], a1 = up1[pad(2 * c + 1)];
+                    float2 b0 = up2[pad(2 * c)], b1 = up2[pad(2 * c + 1)];
+                    a0 = make_float2(a0.x * inv * 0.5f, a0.y * inv * 0.5f);
+                    a1 = make_float2(a1.x * inv * 0.5f, a1.y * inv * 0.5f);
+                    b0 = make_float2(b0.x * inv * 0.5f, b0.y * inv * 0.5f);
+                    b1 = make_float2(b1.x * inv * 0.5f, b1.y * inv * 0.5f);
+                    const float2 g0 = cmul_conj(a0, b0), g1 = cmul_conj(a1, b1);
+                    gd.x += g0.x + g1.x;
+                    gd.y += g0.y + g1.y;
+                    ad.x += (a0.x * a0.x + a0.y * a0.y) + (a1.x * a1.x + a1.y * a1.y);
+                    ad.y += (b0.x * b0.x + b0.y * b0.y) + (b1.x * b1.x + b1.y * b1.y);
+                    if (mask) {
+                        const float2 x1 = __ldg(in1 + c), x2 = __ldg(in2 + c);
+                        s1.x += x1.x;
+                        s1.y += x1.y;
+                        s2.x += x2.x;
+                        s2.y += x2.y;
+                    }
+                    ig.x += gd.x;
+                    ig.y += gd.y;
+                    am.x += ad.x;
+                    am.y += ad.y;
+                    m1.x += s1.x;
+                    m1.y += s1.y;
+                    m2.x += s2.x;
+                    m2.y += s2.y;
+                }
+                am = make_float2(sqrtf(am.x), sqrtf(am.y));
+                if (mask && (hypotf(m1.x, m1.y) <= 1.e-6f || hypotf(m2.x, m2.y) <= 1.e-6f)) {
+                    ig = make_float2(0.f, 0.f);
+                    am = make_float2(0.f, 0.f);
+                }
+                igrams[k - 1][(long long)l * nout_cols + j] = ig;
+                amps[k - 1][(long long)l * nout_cols + j] = am;
+            }
+            __syncthreads();  // the pair's reads are done before the next image overwrites up1
+        }
     }
 }
 
@@ -219,7 +306,8 @@ struct XmCtx {
     std::mutex mu;
     Plan fwd, inv;
     DevBuf pad, upA, upB;
-    DevBuf tw;          // twiddle tables of the fused upsampling (smem_fft)
+    DevBuf tw;          // twiddle tables of the fused kernels (smem_fft)
+    DevBuf ptrs;        // image and output pointers of the fused stack kernel
     bool fused_ready = false;
     int sms = 0;
 };
@@ -299,17 +387,39 @@ int run_stack(const float *const *slcs, int n, long long ld, int na, int nlines,
     const int nnn = fft_length(na);
     const int nout_lines = nlines / looksdn, nout_cols = na / looksac;
     const int nl = nout_lines * looksdn;
-    if (nnn == 4096) {  // the fused upsampling (upsample4096_kernel)
+    if (nnn == 4096) {  // the fused kernels (upsample4096_kernel, crossmul_stack4096_kernel)
         if (!x.fused_ready) {
             if ((rc = x.tw.ensure(sizeof(float2) * smem_fft::kTw))) return rc;
             const std::vector<float2> tw = smem_fft::twiddle_tables();
             CKC(cudaFuncSetAttribute(upsample4096_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      kXmSmem));
+            CKC(cudaFuncSetAttribute(crossmul_stack4096_kernel,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, kXmStackSmem));
             CKC(cudaDeviceGetAttribute(&x.sms, cudaDevAttrMultiProcessorCount, dev));
             CKC(cudaMemcpyAsync(x.tw.p, tw.data(), sizeof(float2) * smem_fft::kTw,
                                 cudaMemcpyHostToDevice, st));
             CKC(cudaStreamSynchronize(st));  // `tw` is pageable host memory that goes out of scope
             x.fused_ready = true;
+        }
+        if (looksdn == 1) {  // the whole stack in one launch
+            std::vector<const void *> ptrs(3 * (size_t)n);
+            for (int k = 0; k < n; ++k) ptrs[k] = slcs[k];
+            for (int k = 0; k + 1 < n; ++k) {
+                ptrs[n + k] = igrams[k];
+                ptrs[2 * n + k] = amps[k];
+            }
+            // (a copy from pageable memory is staged before the call returns)
+            if ((rc = x.ptrs.ensure(sizeof(void *) * ptrs.size()))) return rc;
+            CKC(cudaMemcpyAsync(x.ptrs.p, ptrs.data(), sizeof(void *) * ptrs.size(),
+                                cudaMemcpyHostToDevice, st));
+            void **vp = static_cast<void **>(x.ptrs.p);
+            crossmul_stack4096_kernel<<<std::min(nout_lines, x.sms), smem_fft::kThreads,
+                                        kXmStackSmem, st>>>(
+                reinterpret_cast<const float2 *const *>(vp), n, ld, na, nout_lines, nout_cols,
+                looksac, scale, mask, static_cast<const float2 *>(x.tw.p),
+                reinterpret_cast<float2 *const *>(vp + n), reinterpret_cast<float2 *const *>(vp + 2 * n));
+            CKC(cudaGetLastError());
+            return SRG_OK;
         }
     } else if ((rc = plan_for(x.fwd, nnn, nl)) || (rc = plan_for(x.inv, 2 * nnn, nl)) ||
                (rc = x.pad.ensure((size_t)nl * nnn * sizeof(float2)))) {

@@ -128,16 +128,25 @@ def test_gpu_crossmul_row_stride_and_valid_lines(torch_cuda):
 
 
 @gpu
-@pytest.mark.parametrize("na", [200, 2600])
-def test_gpu_crossmul_stack_equals_pairs(torch_cuda, na):
+@pytest.mark.parametrize("na,ldn", [(200, 4), (2600, 4), (2600, 1)])
+def test_gpu_crossmul_stack_equals_pairs(torch_cuda, na, ldn):
+    """A stack's pairs equal the pairs formed one by one (na 2,600 with looks
+    of one line down: the fused stack kernel; also against the oracle)."""
     torch = torch_cuda
     from srg_b200 import api
     rng = np.random.default_rng(8)
-    imgs = [torch.from_numpy(_img(rng, 24, na)).cuda() for _ in range(5)]
-    igs, ams = api.crossmul_stack(imgs, looksac=2, looksdn=4, scale=0.25)
+    hosts = [_img(rng, 24, na) for _ in range(5)]
+    hosts[2][:, 500:520] = 0                       # an empty window for the mask
+    imgs = [torch.from_numpy(h).cuda() for h in hosts]
+    igs, ams = api.crossmul_stack(imgs, looksac=2, looksdn=ldn, scale=0.25, mask=True)
     for k in range(4):
-        ig, am = api.crossmul(imgs[k], imgs[k + 1], looksac=2, looksdn=4, scale=0.25)
+        ig, am = api.crossmul(imgs[k], imgs[k + 1], looksac=2, looksdn=ldn, scale=0.25, mask=True)
         assert torch.equal(ig, igs[k]) and torch.equal(am, ams[k])
+        if na > 2048:
+            want_ig, want_am = ox.crossmul(hosts[k], hosts[k + 1], looksac=2, looksdn=ldn,
+                                           scale=0.25, mask=True)
+            _close(igs[k].cpu().numpy(), want_ig)
+            _close(ams[k].cpu().numpy(), want_am)
 
 
 @gpu
