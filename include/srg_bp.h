@@ -452,8 +452,13 @@ int srg_forward_project_device(const srg_burst_desc *b, const float *refl,
  * its look window| <= 1e-6 in either image (the reference's default 'y').
  * Inputs: [nlines][ld] complex64 (device); nlines plays the reference's
  * <valid_lines>.  Outputs: [nlines/looksdn][na/looksac] complex64 (device).
- * Enqueued on `stream`; FFTs by cuFFT (the reference uses FFTW in single
- * precision, so results agree to FP32 rounding, not bit for bit). */
+ * Enqueued on `stream`.  FFTs in FP32 (the reference uses FFTW in single
+ * precision, so results agree to FP32 rounding, not bit for bit): for lines
+ * of 2,049-4,096 samples (nnn = 4,096) kernels of the library's own that
+ * transform each line in shared memory (and, with looksdn = 1, form the
+ * pairs there too), otherwise cuFFT.  The device's scratch (upsampled
+ * images, twiddle tables, pointer arrays) is shared by every call on it:
+ * calls on the same device whose GPU work overlaps (other streams) race. */
 int srg_crossmul_device(const float *slc1, const float *slc2, long long ld, int na, int nlines,
                         int looksac, int looksdn, float scale, int mask, float *igram,
                         float *amp, void *stream);
@@ -479,8 +484,11 @@ int srg_range_replica(float samplefreq, float startfreq, float ramprate, float p
  * replica's 32,768-point spectrum, inverse FFT (unnormalised, as FFTW's), and
  * write the first nvalid = nsamps - npts samples of each line to `out`
  * ([nlines][ld_out] complex64, device; *nvalid_out receives nvalid).
- * Enqueued on `stream`; FFTs by cuFFT (the reference uses FFTW in single
- * precision: results agree to FP32 rounding, not bit for bit). */
+ * Enqueued on `stream`.  Pulses of up to 4,096 samples: one fused kernel
+ * forms those samples by overlap-save (8,192-point transforms in shared
+ * memory; the same samples, the 32,768-point correlation never wrapping into
+ * them); longer pulses: cuFFT.  FP32 throughout (the reference uses FFTW in
+ * single precision: results agree to FP32 rounding, not bit for bit). */
 int srg_range_compress_device(const float *lines, long long ld_in, int nlines, int nsamps,
                               float samplefreq, float startfreq, float ramprate,
                               float pulselength, float *out, long long ld_out, int *nvalid_out,
