@@ -149,13 +149,27 @@ __global__ void crossmul_looks_kernel(const float2 *__restrict__ up1, const floa
 // after loading the twiddle tables once.
 constexpr int kXmSmem = (smem_fft::kBuf + smem_fft::kTw) * (int)sizeof(float2);
 
-// One line of one image, steps 1-4 with nnn = 4096: the 8,192 upsampled
-// samples (unnormalised) left in buf (padded layout, natural order).  All
-// kThreads threads call it; tw holds the twiddle tables.
+// One line of one image, steps 1-4 with nnn = 4096.  With the spectrum X
+// spread as step 3 does, the unnormalised 8,192-point inverse u has
+// u[2n] = 4096 x_s[n] (x_s = in * scale padded to 4096: the forward and
+// inverse 4,096-point transforms cancel) and u[2n + 1] = the 4,096-point
+// inverse of X[k] s_k exp(i pi k / 4096), s_k = 1 for k < 2048 and -1 for the
+// bins moved to the top.  So the odd samples come from two 4,096-point
+// transforms (the inverse as the forward transform of the conjugate) and
+// the even ones straight from the input (even_sample): u[2n + 1] is left in
+// buf[pad(n)], n < 4096.  All kThreads threads call it; tw holds the
+// twiddle tables.
+__device__ __forceinline__ float2 even_sample(const float2 *__restrict__ x, int n, int na,
+                                              float scale) {
+    if (n >= na) return make_float2(0.f, 0.f);
+    const float2 a = __ldg(x + n);
+    return make_float2(a.x * scale * 4096.f, a.y * scale * 4096.f);
+}
+
 __device__ __forceinline__ void upsample_line(const float2 *__restrict__ x, int na, float scale,
                                               float2 *buf, const float2 *tw) {
     using namespace smem_fft;
-    constexpr int N = 4096, N2 = 8192, T = kThreads;
+    constexpr int N = 4096, T = kThreads;
     const int t = threadIdx.x;
     // forward 4,096-point transform, pass 1 (Ns = 1) from the line
     if (t < N / 16) {
@@ -177,31 +191,20 @@ __device__ __forceinline__ void upsample_line(const float2 *__restrict__ x, int 
     __syncthreads();
     pass16<N>(buf, 16, tw + kTw16);
     pass16<N>(buf, 256, tw + kTw256);
-    // spread, conjugated: Y[m] = conj X[m] (m < 2048), 0 (2048 <= m < 6144),
-    // conj X[m - 4096] (m >= 6144)
-    float2 hi[N / 2 / T];
+    // conj(X[k] s_k exp(i pi k / 4096)) = s_k conj(X[k]) exp(-2 pi i k / 8192),
+    // each item its own entry
 #pragma unroll
-    for (int q = 0; q < N / 2 / T; ++q) hi[q] = buf[pad(N / 2 + t + q * T)];
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < N / 2 / T; ++q) buf[pad(t + q * T)] = cconj(buf[pad(t + q * T)]);
-#pragma unroll
-    for (int q = 0; q < N / T; ++q) buf[pad(N / 2 + t + q * T)] = make_float2(0.f, 0.f);
-#pragma unroll
-    for (int q = 0; q < N / 2 / T; ++q) buf[pad(N2 - N / 2 + t + q * T)] = cconj(hi[q]);
-    __syncthreads();
-    // 8,192-point forward transform of the conjugate; its last (radix-2) pass
-    // touches only each item's own pair, so it goes in place
-    pass16<N2>(buf, 1, nullptr);
-    pass16<N2>(buf, 16, tw + kTw16);
-    pass16<N2>(buf, 256, tw + kTw256);
-#pragma unroll
-    for (int it = 0; it < N2 / 2 / T; ++it) {
-        const int j = t + it * T;
-        const float2 a = buf[pad(j)], b = cmul(buf[pad(j + N2 / 2)], tw[kTw2 + j]);
-        buf[pad(j)] = cconj(cadd(a, b));
-        buf[pad(j + N2 / 2)] = cconj(csub(a, b));
+    for (int q = 0; q < N / T; ++q) {
+        const int k = t + q * T;
+        const float2 z = cmul(cconj(buf[pad(k)]), tw[kTw2 + k]);
+        buf[pad(k)] = k < N / 2 ? z : make_float2(-z.x, -z.y);
     }
+    __syncthreads();
+    pass16<N>(buf, 1, nullptr);
+    pass16<N>(buf, 16, tw + kTw16);
+    pass16<N>(buf, 256, tw + kTw256);
+#pragma unroll
+    for (int q = 0; q < N / T; ++q) buf[pad(t + q * T)] = cconj(buf[pad(t + q * T)]);
     __syncthreads();
 }
 
@@ -215,9 +218,13 @@ upsample4096_kernel(const float2 *__restrict__ in, long long ld, int na, int nl,
     for (int i = t; i < kTw; i += kThreads) tw[i] = __ldg(twg + i);
     __syncthreads();
     for (int l = blockIdx.x; l < nl; l += gridDim.x) {
-        upsample_line(in + (long long)l * ld, na, scale, buf, tw);
-        float2 *u = up + (long long)l * 8192;
-        for (int j = t; j < 8192; j += kThreads) u[j] = buf[pad(j)];
+        const float2 *x = in + (long long)l * ld;
+        upsample_line(x, na, scale, buf, tw);
+        float4 *u = reinterpret_cast<float4 *>(up + (long long)l * 8192);  // (u[2n], u[2n + 1])
+        for (int j = t; j < 4096; j += kThreads) {
+            const float2 e = even_sample(x, j, na, scale), o = buf[pad(j)];
+            u[j] = make_float4(e.x, e.y, o.x, o.y);
+        }
         __syncthreads();  // the line's reads are done before the next one's writes
     }
 }
@@ -256,8 +263,8 @@ crossmul_stack4096_kernel(const float2 *const *__restrict__ imgs, int n, long lo
                     const int c = j * looksac + q;
                     float2 gd = make_float2(0.f, 0.f), ad = make_float2(0.f, 0.f);
                     float2 s1 = make_float2(0.f, 0.f), s2 = make_float2(0.f, 0.f);
-                    float2 a0 = up1[pad(2 * c)], a1 = up1[pad(2 * c + 1)];
-                    float2 b0 = up2[pad(2 * c)], b1 = up2[pad(2 * c + 1)];
+                    float2 a0 = even_sample(in1, c, na, scale), a1 = up1[pad(c)];
+                    float2 b0 = even_sample(in2, c, na, scale), b1 = up2[pad(c)];
                     a0 = make_float2(a0.x * inv * 0.5f, a0.y * inv * 0.5f);
                     a1 = make_float2(a1.x * inv * 0.5f, a1.y * inv * 0.5f);
                     b0 = make_float2(b0.x * inv * 0.5f, b0.y * inv * 0.5f);

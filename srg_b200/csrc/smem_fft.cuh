@@ -100,10 +100,11 @@ __device__ __forceinline__ void pass16(float2 *buf, int Ns, const float2 *tw) {
     const int j = threadIdx.x, k = j & (Ns - 1);
     const bool item = every || j < J;
     float2 v[16];
-    if (item) {
+    // (threads without an item load too, from a valid index, and discard: the
+    // register array is then set on every path and stays in registers)
+    const int jl = every ? j : (j & (J - 1));
 #pragma unroll
-        for (int r = 0; r < 16; ++r) v[r] = buf[pad(j + r * J)];
-    }
+    for (int r = 0; r < 16; ++r) v[r] = buf[pad(jl + r * J)];
     __syncthreads();
     if (item) {
         if (Ns > 1) {
