@@ -229,13 +229,134 @@ upsample4096_kernel(const float2 *__restrict__ in, long long ld, int na, int nl,
     }
 }
 
+// One radix-16 pass of a 4,096-point transform per half-CTA, each half on its
+// own buffer (threads t < 256: buf of the first half, t >= 256: of the
+// second); otherwise as smem_fft::pass16.  Every thread calls it.
+__device__ __forceinline__ void pass16_halves(float2 *buf, int Ns, const float2 *tw) {
+    using namespace smem_fft;
+    constexpr int J = 256;
+    const int j = threadIdx.x & (J - 1), k = j & (Ns - 1);
+    float2 v[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = buf[pad(j + r * J)];
+    __syncthreads();
+    if (Ns > 1) {
+#pragma unroll
+        for (int r = 1; r < 16; ++r) v[r] = cmul(v[r], tw[(r - 1) * Ns + k]);
+    }
+    dft<16>(v);
+    const int base = (j - k) * 16 + k;
+#pragma unroll
+    for (int r = 0; r < 16; ++r) buf[pad(base + r * Ns)] = v[brev<16>(r)];
+    __syncthreads();
+}
+
+// upsample_line for two lines at once, one per half-CTA: x0 into b0 (threads
+// t < 256), x1 into b1 (t >= 256; x1 null: that half transforms zeros).
+__device__ __forceinline__ void upsample_two(const float2 *__restrict__ x0,
+                                             const float2 *__restrict__ x1, int na, float scale,
+                                             float2 *b0, float2 *b1, const float2 *tw) {
+    using namespace smem_fft;
+    constexpr int N = 4096, J = 256;
+    const int t = threadIdx.x, jt = t & (J - 1);
+    const float2 *x = t < J ? x0 : x1;
+    float2 *buf = t < J ? b0 : b1;
+    {
+        float2 v[16];
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+            const int i = jt + r * J;
+            float2 a = make_float2(0.f, 0.f);
+            if (x && i < na) {
+                a = __ldg(x + i);
+                a = make_float2(a.x * scale, a.y * scale);
+            }
+            v[r] = a;
+        }
+        dft<16>(v);
+#pragma unroll
+        for (int r = 0; r < 16; ++r) buf[pad(jt * 16 + r)] = v[brev<16>(r)];
+    }
+    __syncthreads();
+    pass16_halves(buf, 16, tw + kTw16);
+    pass16_halves(buf, 256, tw + kTw256);
+#pragma unroll
+    for (int q = 0; q < N / J; ++q) {
+        const int k = jt + q * J;
+        const float2 z = cmul(cconj(buf[pad(k)]), tw[kTw2 + k]);
+        buf[pad(k)] = k < N / 2 ? z : make_float2(-z.x, -z.y);
+    }
+    __syncthreads();
+    pass16_halves(buf, 1, nullptr);
+    pass16_halves(buf, 16, tw + kTw16);
+    pass16_halves(buf, 256, tw + kTw256);
+#pragma unroll
+    for (int q = 0; q < N / J; ++q) buf[pad(jt + q * J)] = cconj(buf[pad(jt + q * J)]);
+    __syncthreads();
+}
+
+// One pair's interferogram and amplitude samples of one grid line (looks of
+// one line down), from the two images' odd upsampled samples in shared
+// memory and their even ones from the input: the sums of
+// crossmul_looks_kernel with looksdn = 1, in its order.
+__device__ __forceinline__ void form_pair(const float2 *up1, const float2 *up2,
+                                          const float2 *__restrict__ in1,
+                                          const float2 *__restrict__ in2, int na, float scale,
+                                          int nout_cols, int looksac, int mask, float2 *ig_out,
+                                          float2 *am_out) {
+    const float inv = 1.f / 4096.f;  // a power of two: same as the reference's division
+    for (int j = threadIdx.x; j < nout_cols; j += smem_fft::kThreads) {
+        float2 ig = make_float2(0.f, 0.f), am = make_float2(0.f, 0.f);
+        float2 m1 = make_float2(0.f, 0.f), m2 = make_float2(0.f, 0.f);
+        for (int q = 0; q < looksac; ++q) {
+            const int c = j * looksac + q;
+            float2 gd = make_float2(0.f, 0.f), ad = make_float2(0.f, 0.f);
+            float2 s1 = make_float2(0.f, 0.f), s2 = make_float2(0.f, 0.f);
+            float2 a0 = even_sample(in1, c, na, scale), a1 = up1[smem_fft::pad(c)];
+            float2 b0 = even_sample(in2, c, na, scale), b1 = up2[smem_fft::pad(c)];
+            a0 = make_float2(a0.x * inv * 0.5f, a0.y * inv * 0.5f);
+            a1 = make_float2(a1.x * inv * 0.5f, a1.y * inv * 0.5f);
+            b0 = make_float2(b0.x * inv * 0.5f, b0.y * inv * 0.5f);
+            b1 = make_float2(b1.x * inv * 0.5f, b1.y * inv * 0.5f);
+            const float2 g0 = cmul_conj(a0, b0), g1 = cmul_conj(a1, b1);
+            gd.x += g0.x + g1.x;
+            gd.y += g0.y + g1.y;
+            ad.x += (a0.x * a0.x + a0.y * a0.y) + (a1.x * a1.x + a1.y * a1.y);
+            ad.y += (b0.x * b0.x + b0.y * b0.y) + (b1.x * b1.x + b1.y * b1.y);
+            if (mask) {
+                const float2 x1 = __ldg(in1 + c), x2 = __ldg(in2 + c);
+                s1.x += x1.x;
+                s1.y += x1.y;
+                s2.x += x2.x;
+                s2.y += x2.y;
+            }
+            ig.x += gd.x;
+            ig.y += gd.y;
+            am.x += ad.x;
+            am.y += ad.y;
+            m1.x += s1.x;
+            m1.y += s1.y;
+            m2.x += s2.x;
+            m2.y += s2.y;
+        }
+        am = make_float2(sqrtf(am.x), sqrtf(am.y));
+        if (mask && (hypotf(m1.x, m1.y) <= 1.e-6f || hypotf(m2.x, m2.y) <= 1.e-6f)) {
+            ig = make_float2(0.f, 0.f);
+            am = make_float2(0.f, 0.f);
+        }
+        ig_out[j] = ig;
+        am_out[j] = am;
+    }
+}
+
 // The whole stack with looks of one line down and nnn = 4096, fused: per grid
-// line, image k's upsampled line is made in one shared buffer while image
-// k - 1's is still in the other, and the pair's interferogram and amplitude
-// samples of that line are formed from the two (the sums of
-// crossmul_looks_kernel with looksdn = 1, in its order): the images are read
-// once and no upsampled image goes through HBM.  Persistent over lines.
-constexpr int kXmStackSmem = (2 * smem_fft::kBuf + smem_fft::kTw) * (int)sizeof(float2);
+// line, images k and k + 1 are upsampled at once (one per half-CTA) into two
+// of three shared buffers while image k - 1's line is still in the third,
+// and the pairs (k - 1, k) and (k, k + 1) of that line are formed from them:
+// the images are read once and no upsampled image goes through HBM.
+// Persistent over lines.
+constexpr int kXmLine = 4096 + 4096 / 16;  // padded 4,096-point buffer (float2)
+constexpr int kXmStackSmem = (3 * kXmLine + smem_fft::kTw) * (int)sizeof(float2);
 
 __global__ void __launch_bounds__(smem_fft::kThreads, 1)
 crossmul_stack4096_kernel(const float2 *const *__restrict__ imgs, int n, long long ld, int na,
@@ -244,61 +365,26 @@ crossmul_stack4096_kernel(const float2 *const *__restrict__ imgs, int n, long lo
                           float2 *const *__restrict__ amps) {
     using namespace smem_fft;
     extern __shared__ float2 xm_sm[];
-    float2 *tw = xm_sm + 2 * kBuf;
+    float2 *tw = xm_sm + 3 * kXmLine;
     const int t = threadIdx.x;
     for (int i = t; i < kTw; i += kThreads) tw[i] = __ldg(twg + i);
     __syncthreads();
-    const float inv = 1.f / 4096.f;  // a power of two: same as the reference's division
     for (int l = blockIdx.x; l < nlines; l += gridDim.x) {
-        for (int k = 0; k < n; ++k) {
-            float2 *cur = xm_sm + (k & 1) * kBuf;
-            upsample_line(imgs[k] + (long long)l * ld, na, scale, cur, tw);
-            if (k == 0) continue;
-            const float2 *up1 = xm_sm + ((k - 1) & 1) * kBuf, *up2 = cur;
-            const float2 *in1 = imgs[k - 1] + (long long)l * ld, *in2 = imgs[k] + (long long)l * ld;
-            for (int j = t; j < nout_cols; j += kThreads) {
-                float2 ig = make_float2(0.f, 0.f), am = make_float2(0.f, 0.f);
-                float2 m1 = make_float2(0.f, 0.f), m2 = make_float2(0.f, 0.f);
-                for (int q = 0; q < looksac; ++q) {
-                    const int c = j * looksac + q;
-                    float2 gd = make_float2(0.f, 0.f), ad = make_float2(0.f, 0.f);
-                    float2 s1 = make_float2(0.f, 0.f), s2 = make_float2(0.f, 0.f);
-                    float2 a0 = even_sample(in1, c, na, scale), a1 = up1[pad(c)];
-                    float2 b0 = even_sample(in2, c, na, scale), b1 = up2[pad(c)];
-                    a0 = make_float2(a0.x * inv * 0.5f, a0.y * inv * 0.5f);
-                    a1 = make_float2(a1.x * inv * 0.5f, a1.y * inv * 0.5f);
-                    b0 = make_float2(b0.x * inv * 0.5f, b0.y * inv * 0.5f);
-                    b1 = make_float2(b1.x * inv * 0.5f, b1.y * inv * 0.5f);
-                    const float2 g0 = cmul_conj(a0, b0), g1 = cmul_conj(a1, b1);
-                    gd.x += g0.x + g1.x;
-                    gd.y += g0.y + g1.y;
-                    ad.x += (a0.x * a0.x + a0.y * a0.y) + (a1.x * a1.x + a1.y * a1.y);
-                    ad.y += (b0.x * b0.x + b0.y * b0.y) + (b1.x * b1.x + b1.y * b1.y);
-                    if (mask) {
-                        const float2 x1 = __ldg(in1 + c), x2 = __ldg(in2 + c);
-                        s1.x += x1.x;
-                        s1.y += x1.y;
-                        s2.x += x2.x;
-                        s2.y += x2.y;
-                    }
-                    ig.x += gd.x;
-                    ig.y += gd.y;
-                    am.x += ad.x;
-                    am.y += ad.y;
-                    m1.x += s1.x;
-                    m1.y += s1.y;
-                    m2.x += s2.x;
-                    m2.y += s2.y;
-                }
-                am = make_float2(sqrtf(am.x), sqrtf(am.y));
-                if (mask && (hypotf(m1.x, m1.y) <= 1.e-6f || hypotf(m2.x, m2.y) <= 1.e-6f)) {
-                    ig = make_float2(0.f, 0.f);
-                    am = make_float2(0.f, 0.f);
-                }
-                igrams[k - 1][(long long)l * nout_cols + j] = ig;
-                amps[k - 1][(long long)l * nout_cols + j] = am;
-            }
-            __syncthreads();  // the pair's reads are done before the next image overwrites up1
+        const long long row = (long long)l * ld, orow = (long long)l * nout_cols;
+        int prev = -1;  // buffer holding image k - 1's line
+        for (int k = 0; k < n; k += 2) {
+            const int a = prev < 0 ? 0 : (prev + 1) % 3, b = prev < 0 ? 1 : (prev + 2) % 3;
+            float2 *ua = xm_sm + a * kXmLine, *ub = xm_sm + b * kXmLine;
+            const bool two = k + 1 < n;
+            upsample_two(imgs[k] + row, two ? imgs[k + 1] + row : nullptr, na, scale, ua, ub, tw);
+            if (k > 0)
+                form_pair(xm_sm + prev * kXmLine, ua, imgs[k - 1] + row, imgs[k] + row, na, scale,
+                          nout_cols, looksac, mask, igrams[k - 1] + orow, amps[k - 1] + orow);
+            if (two)
+                form_pair(ua, ub, imgs[k] + row, imgs[k + 1] + row, na, scale, nout_cols, looksac,
+                          mask, igrams[k] + orow, amps[k] + orow);
+            __syncthreads();  // the pairs' reads are done before the buffers are written again
+            prev = two ? b : a;
         }
     }
 }
