@@ -29,6 +29,27 @@ def test_upsample_even_samples_are_half_the_input():
     np.testing.assert_allclose(up[:, 0:74:2], x / 2.0, atol=1e-6)
 
 
+def test_upsample_from_odd_samples():
+    """The identity the fused GPU kernels rest on, on the restatement: with
+    the spectrum X spread as the reference spreads it, the unnormalised
+    2nnn-point inverse u has u[2n] = nnn x[n] and u[2n + 1] = the nnn-point
+    inverse of X[k] s_k exp(i pi k / nnn), s_k = -1 for the bins moved to
+    the top (upsample2 returns u / nnn / 2)."""
+    rng = np.random.default_rng(12)
+    for na in (2049, 2600, 4096):
+        x = _img(rng, 2, na).astype(np.complex128)
+        nnn = ox.fft_length(na)
+        up = ox.upsample2(x, nnn) * nnn * 2.0
+        xp = np.zeros((2, nnn), np.complex128)
+        xp[:, :na] = x
+        k = np.arange(nnn)
+        tw = np.where(k < nnn // 2, 1.0, -1.0) * np.exp(1j * np.pi * k / nnn)
+        odd = np.fft.ifft(np.fft.fft(xp, axis=1) * tw, axis=1) * nnn
+        scale = np.abs(up).max()
+        assert np.abs(up[:, 0::2] - nnn * xp).max() / scale < 1e-12
+        assert np.abs(up[:, 1::2] - odd).max() / scale < 1e-12
+
+
 def test_identical_images_give_real_power():
     x = _img(np.random.default_rng(2), 12, 50)
     ig, am = ox.crossmul(x, x, looksac=2, looksdn=3, mask=False)

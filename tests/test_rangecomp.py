@@ -20,6 +20,35 @@ def test_library_replica_matches_restatement():
     assert np.array_equal(rep, want)
 
 
+def test_overlap_save_gives_the_kept_samples():
+    """The identity the fused GPU kernel rests on, checked on the restatement:
+    the kept samples of the 32,768-point circular correlation are a linear
+    correlation (the wrap never reaches n < nvalid), so overlap-save with
+    8,192-point segments of 8,192 - npts + 1 outputs, filter
+    4 conj(DFT_8192(replica)) and the inverse as the conjugate of a forward
+    transform of the conjugate, gives them to FP64 rounding; over segment
+    boundaries and a line's last samples too."""
+    M = 8192
+    rep, npts = orc.replica(**PULSE)
+    rng = np.random.default_rng(11)
+    for nsamps in (9000, 21000, 32768):
+        x = (rng.standard_normal((2, nsamps)) + 1j * rng.standard_normal((2, nsamps))).astype(np.complex64)
+        want = orc.range_compress(x, **PULSE)
+        nvalid, L = nsamps - npts, M - npts + 1
+        H = (orc.RANFFT / M) * np.conj(np.fft.fft(np.concatenate(
+            [rep[:npts].astype(np.complex128), np.zeros(M - npts)])))
+        got = np.zeros((2, nvalid), np.complex128)
+        for s0 in range(0, nvalid, L):
+            seg = np.zeros((2, M), np.complex128)
+            n = min(M, nsamps - s0)
+            seg[:, :n] = x[:, s0:s0 + n]
+            y = np.conj(np.fft.fft(np.conj(np.fft.fft(seg, axis=1) * H), axis=1))
+            m = min(L, nvalid - s0)
+            got[:, s0:s0 + m] = y[:, :m]
+        rms = np.sqrt(np.mean(np.abs(want) ** 2))
+        assert np.abs(got - want).max() / rms < 1e-6
+
+
 def test_point_target_compresses_to_a_peak_of_ranfft():
     # correlation with the replica (sum |chirp|^2 / npts = 1), times 32,768 from
     # the unnormalised inverse transform
