@@ -126,6 +126,9 @@ def test_overlap_option_and_flush_without_a_gpu(monkeypatch):
     o = _lib.default_options()
     assert o.overlap == int(os.environ.get("SRG_DROPIN_OVERLAP", "0") == "1")
     assert _lib.Options.overlap.offset == _lib.Options.scratch_limit.offset + 8
+    # the tile shear follows it and defaults to rectangular tiles
+    assert _lib.Options.tile_shear.offset == _lib.Options.overlap.offset + 4
+    assert o.tile_shear == 0
     assert _lib.lib().srg_dropin_flush(-1) == _lib.SRG_OK
     api.dropin_flush()
 
