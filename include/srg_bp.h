@@ -456,9 +456,10 @@ int srg_forward_project_device(const srg_burst_desc *b, const float *refl,
  * precision, so results agree to FP32 rounding, not bit for bit): for lines
  * of 2,049-4,096 samples (nnn = 4,096) kernels of the library's own that
  * transform each line in shared memory (and, with looksdn = 1, form the
- * pairs there too), otherwise cuFFT.  The device's scratch (upsampled
- * images, twiddle tables, pointer arrays) is shared by every call on it:
- * calls on the same device whose GPU work overlaps (other streams) race. */
+ * pairs there too, with no scratch but read-only tables), otherwise cuFFT.
+ * The device's scratch (upsampled images) is shared by every call on it:
+ * calls on the same device whose GPU work overlaps (other streams) race,
+ * except those that form the pairs in shared memory. */
 int srg_crossmul_device(const float *slc1, const float *slc2, long long ld, int na, int nlines,
                         int looksac, int looksdn, float scale, int mask, float *igram,
                         float *amp, void *stream);

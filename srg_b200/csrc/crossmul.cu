@@ -357,12 +357,21 @@ __device__ __forceinline__ void form_pair(const float2 *up1, const float2 *up2,
 // Persistent over lines.
 constexpr int kXmLine = 4096 + 4096 / 16;  // padded 4,096-point buffer (float2)
 constexpr int kXmStackSmem = (3 * kXmLine + smem_fft::kTw) * (int)sizeof(float2);
+// Images of one launch (its pointers travel as a kernel parameter, 1.5 KB):
+// longer stacks go in launches of up to kXmChunk images overlapping by one.
+constexpr int kXmChunk = 64;
+struct StackPtrs {
+    const float2 *img[kXmChunk];
+    float2 *ig[kXmChunk - 1], *am[kXmChunk - 1];
+};
 
 __global__ void __launch_bounds__(smem_fft::kThreads, 1)
-crossmul_stack4096_kernel(const float2 *const *__restrict__ imgs, int n, long long ld, int na,
+crossmul_stack4096_kernel(const __grid_constant__ StackPtrs p, int n, long long ld, int na,
                           int nlines, int nout_cols, int looksac, float scale, int mask,
-                          const float2 *__restrict__ twg, float2 *const *__restrict__ igrams,
-                          float2 *const *__restrict__ amps) {
+                          const float2 *__restrict__ twg) {
+    const float2 *const *imgs = p.img;
+    float2 *const *igrams = p.ig;
+    float2 *const *amps = p.am;
     using namespace smem_fft;
     extern __shared__ float2 xm_sm[];
     float2 *tw = xm_sm + 3 * kXmLine;
@@ -400,7 +409,6 @@ struct XmCtx {
     Plan fwd, inv;
     DevBuf pad, upA, upB;
     DevBuf tw;          // twiddle tables of the fused kernels (smem_fft)
-    DevBuf ptrs;        // image and output pointers of the fused stack kernel
     bool fused_ready = false;
     int sms = 0;
 };
@@ -494,24 +502,21 @@ int run_stack(const float *const *slcs, int n, long long ld, int na, int nlines,
             CKC(cudaStreamSynchronize(st));  // `tw` is pageable host memory that goes out of scope
             x.fused_ready = true;
         }
-        if (looksdn == 1) {  // the whole stack in one launch
-            std::vector<const void *> ptrs(3 * (size_t)n);
-            for (int k = 0; k < n; ++k) ptrs[k] = slcs[k];
-            for (int k = 0; k + 1 < n; ++k) {
-                ptrs[n + k] = igrams[k];
-                ptrs[2 * n + k] = amps[k];
+        if (looksdn == 1) {  // the whole stack, in launches of up to kXmChunk images
+            for (int k0 = 0; k0 + 1 < n; k0 += kXmChunk - 1) {
+                const int m = std::min(kXmChunk, n - k0);
+                StackPtrs p{};
+                for (int k = 0; k < m; ++k) p.img[k] = reinterpret_cast<const float2 *>(slcs[k0 + k]);
+                for (int k = 0; k + 1 < m; ++k) {
+                    p.ig[k] = reinterpret_cast<float2 *>(igrams[k0 + k]);
+                    p.am[k] = reinterpret_cast<float2 *>(amps[k0 + k]);
+                }
+                crossmul_stack4096_kernel<<<std::min(nout_lines, x.sms), smem_fft::kThreads,
+                                            kXmStackSmem, st>>>(
+                    p, m, ld, na, nout_lines, nout_cols, looksac, scale, mask,
+                    static_cast<const float2 *>(x.tw.p));
+                CKC(cudaGetLastError());
             }
-            // (a copy from pageable memory is staged before the call returns)
-            if ((rc = x.ptrs.ensure(sizeof(void *) * ptrs.size()))) return rc;
-            CKC(cudaMemcpyAsync(x.ptrs.p, ptrs.data(), sizeof(void *) * ptrs.size(),
-                                cudaMemcpyHostToDevice, st));
-            void **vp = static_cast<void **>(x.ptrs.p);
-            crossmul_stack4096_kernel<<<std::min(nout_lines, x.sms), smem_fft::kThreads,
-                                        kXmStackSmem, st>>>(
-                reinterpret_cast<const float2 *const *>(vp), n, ld, na, nout_lines, nout_cols,
-                looksac, scale, mask, static_cast<const float2 *>(x.tw.p),
-                reinterpret_cast<float2 *const *>(vp + n), reinterpret_cast<float2 *const *>(vp + 2 * n));
-            CKC(cudaGetLastError());
             return SRG_OK;
         }
     } else if ((rc = plan_for(x.fwd, nnn, nl)) || (rc = plan_for(x.inv, 2 * nnn, nl)) ||

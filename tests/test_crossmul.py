@@ -171,6 +171,22 @@ def test_gpu_crossmul_stack_equals_pairs(torch_cuda, na, ldn):
 
 
 @gpu
+def test_gpu_crossmul_long_stack_in_launches(torch_cuda):
+    """A stack of 66 images with looks of one line down and 2,100-sample
+    lines: the fused stack kernel takes it in two launches of up to 64
+    images that share one; every pair equals the pair formed alone."""
+    torch = torch_cuda
+    from srg_b200 import api
+    rng = np.random.default_rng(10)
+    imgs = [torch.from_numpy(_img(rng, 6, 2100)).cuda() for _ in range(66)]
+    igs, ams = api.crossmul_stack(imgs, looksac=3, looksdn=1, scale=0.5)
+    assert len(igs) == 65
+    for k in (0, 61, 62, 63, 64):
+        ig, am = api.crossmul(imgs[k], imgs[k + 1], looksac=3, looksdn=1, scale=0.5)
+        assert torch.equal(ig, igs[k]) and torch.equal(am, ams[k]), k
+
+
+@gpu
 def test_gpu_crossmul_files_matches_oracle(torch_cuda):
     from srg_b200 import crossmul as cm
     rng = np.random.default_rng(9)
