@@ -489,7 +489,10 @@ int srg_range_replica(float samplefreq, float startfreq, float ramprate, float p
  * forms those samples by overlap-save (8,192-point transforms in shared
  * memory; the same samples, the 32,768-point correlation never wrapping into
  * them); longer pulses: cuFFT.  FP32 throughout (the reference uses FFTW in
- * single precision: results agree to FP32 rounding, not bit for bit). */
+ * single precision: results agree to FP32 rounding, not bit for bit).  The
+ * device's scratch (the filter spectrum of the last pulse parameters, the
+ * padded line blocks of the cuFFT path) is shared by every call on it: calls
+ * on the same device whose GPU work overlaps (other streams) race. */
 int srg_range_compress_device(const float *lines, long long ld_in, int nlines, int nsamps,
                               float samplefreq, float startfreq, float ramprate,
                               float pulselength, float *out, long long ld_out, int *nvalid_out,
